@@ -1,0 +1,80 @@
+// extern "C" batched-operation entry points (include/gpufhe_b200.h).
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "context.hpp"
+#include "gpufhe_b200.h"
+#include "pipeline.hpp"
+
+gfx::Context* gpufhe_impl(gpufhe_ctx* h);
+
+struct gpufhe_plan {
+    std::unique_ptr<pl::Plan> p;
+};
+
+namespace {
+std::vector<pl::Op> to_ops(uint32_t nops, const gpufhe_op* ops) {
+    std::vector<pl::Op> v(nops);
+    for (uint32_t i = 0; i < nops; ++i) {
+        v[i].L = ops[i].level;
+        v[i].mode = ops[i].mode;
+        v[i].key_id = ops[i].key_id;
+        v[i].galois = ops[i].galois;
+        for (int k = 0; k < 4; ++k) v[i].in[k] = ops[i].in[k];
+        v[i].out[0] = ops[i].out[0];
+        v[i].out[1] = ops[i].out[1];
+    }
+    return v;
+}
+}  // namespace
+
+#define GPUFHE_TRY(...)                                                  \
+    try { __VA_ARGS__ } catch (const std::invalid_argument& e) {         \
+        gfx::set_error(e.what()); return GPUFHE_EINVAL;                  \
+    } catch (const std::length_error& e) {                               \
+        gfx::set_error(e.what()); return GPUFHE_ENOMEM;                  \
+    } catch (const std::exception& e) {                                  \
+        gfx::set_error(e.what()); return GPUFHE_ECUDA;                   \
+    }
+
+extern "C" {
+
+uint64_t gpufhe_op_workspace_bytes(gpufhe_ctx* h, uint32_t level) {
+    gfx::Context* c = gpufhe_impl(h);
+    if (!c || level < 1 || level > c->fullQ()) return 0;
+    return pl::op_workspace_words(*c, level) * 8;
+}
+
+int gpufhe_plan_create(gpufhe_ctx* h, uint32_t nops, const gpufhe_op* ops, uint64_t* d_ws, uint64_t ws_bytes,
+                       gpufhe_plan** out) {
+    gfx::Context* c = gpufhe_impl(h);
+    if (!c || !ops || !out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    GPUFHE_TRY({
+        auto pp = pl::build_plan(*c, to_ops(nops, ops), d_ws, ws_bytes / 8);
+        *out = new gpufhe_plan{std::move(pp)};
+        return GPUFHE_OK;
+    })
+}
+
+int gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t s) {
+    if (!plan) { gfx::set_error("null plan"); return GPUFHE_EINVAL; }
+    cudaError_t e = pl::launch(*plan->p, s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
+}
+
+void gpufhe_plan_destroy(gpufhe_plan* plan) { delete plan; }
+
+int gpufhe_run_ops(gpufhe_ctx* h, uint32_t nops, const gpufhe_op* ops, cudaStream_t s) {
+    gpufhe_plan* p = nullptr;
+    int rc = gpufhe_plan_create(h, nops, ops, nullptr, 0, &p);
+    if (rc) return rc;
+    rc = gpufhe_plan_launch(p, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    gpufhe_plan_destroy(p);
+    if (!rc && e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,211 @@
+#include "context.hpp"
+
+#include <cstring>
+#include <stdexcept>
+
+#include "hostmath.hpp"
+
+namespace gfx {
+
+namespace {
+thread_local std::string g_err;
+
+using hm::u128;
+
+// a*b mod m for m < 2^127 (shift-and-add; setup only).
+u128 mulmod128(u128 a, u128 b, u128 m) {
+    a %= m;
+    u128 r = 0;
+    while (b) {
+        if (b & 1) { r += a; if (r >= m) r -= m; }
+        a <<= 1; if (a >= m) a -= m;
+        b >>= 1;
+    }
+    return r;
+}
+
+// smallest generator-derived primitive 2n-th root (same search as the
+// reference's native_root, params.cpp:42-48)
+u64 native_root(uint32_t n, u64 q) {
+    const u64 M = 2ull * n;
+    for (u64 g = 2; g < q; ++g) {
+        u64 c = hm::powmod(g, (q - 1) / M, q);
+        if (hm::powmod(c, n, q) == q - 1) return c;
+    }
+    throw std::runtime_error("no primitive 2n-th root of unity");
+}
+}  // namespace
+
+std::string last_error() { return g_err; }
+void set_error(const std::string& s) { g_err = s; }
+
+void* Context::dalloc(size_t bytes) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs_.push_back(p);
+    table_bytes_ += bytes;
+    return p;
+}
+
+template <class T>
+T* Context::upload(const std::vector<T>& h) {
+    T* d = (T*)dalloc(h.size() * sizeof(T));
+    cudaError_t e = cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) throw std::runtime_error(std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+    return d;
+}
+
+Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& P, uint32_t alpha,
+                 const std::vector<u64>& roots, int device)
+    : n_(n), alpha_(alpha), device_(device), Q_(Q), P_(P) {
+    if (!hm::is_pow2(n) || n < 512 || n > 65536) throw std::invalid_argument("ring dimension must be 2^9..2^16");
+    if (Q.empty() || Q.size() > (size_t)MAXQ) throw std::invalid_argument("Q tower count out of range");
+    if (P.empty() || P.size() > (size_t)MAXP) throw std::invalid_argument("P tower count out of range");
+    if (alpha == 0 || alpha > Q.size()) throw std::invalid_argument("alpha out of range");
+    logn_ = (uint32_t)hm::ilog2(n);
+    const uint32_t fullQ = (uint32_t)Q.size(), K = (uint32_t)P.size(), QP = fullQ + K;
+    dnum_ = (fullQ + alpha - 1) / alpha;
+    if (dnum_ > (uint32_t)MAXD) throw std::invalid_argument("too many digits");
+    std::vector<u64> QPm(Q);
+    QPm.insert(QPm.end(), P.begin(), P.end());
+    for (u64 q : QPm) {
+        if (q >= (1ull << 61) || (q & 1) == 0 || (q % (2ull * n)) != 1)
+            throw std::invalid_argument("moduli must be odd primes < 2^61 with q = 1 mod 2n");
+    }
+    if (!roots.empty() && roots.size() != QP) throw std::invalid_argument("roots must list Q then P");
+    roots_.resize(QP);
+    for (uint32_t i = 0; i < QP; ++i) roots_[i] = roots.empty() ? native_root(n, QPm[i]) : roots[i];
+    cudaSetDevice(device);
+
+    // per-modulus constants and twiddles
+    std::vector<ModC> mc(QP);
+    std::vector<Tw> twf((size_t)QP * n), twi((size_t)QP * n), f, iv;
+    std::vector<u64> ninv(QP), ninvp(QP);
+    for (uint32_t i = 0; i < QP; ++i) {
+        const u64 q = QPm[i];
+        mc[i] = hm::modc(q);
+        hm::twiddles(n, q, roots_[i], f, iv);
+        std::memcpy(&twf[(size_t)i * n], f.data(), (size_t)n * sizeof(Tw));
+        std::memcpy(&twi[(size_t)i * n], iv.data(), (size_t)n * sizeof(Tw));
+        ninv[i] = hm::invmod(n, q);
+        ninvp[i] = hm::precon(ninv[i], q);
+    }
+
+    // level-independent ModDown constants
+    std::vector<u64> pinv(fullQ), pinvp(fullQ), pdn(K), pdnp(K), phatmodq((size_t)K * fullQ);
+    for (uint32_t i = 0; i < fullQ; ++i) {
+        pinv[i] = hm::invmod(hm::prod_mod(P.data(), K, Q[i]), Q[i]);
+        pinvp[i] = hm::precon(pinv[i], Q[i]);
+    }
+    for (uint32_t j = 0; j < K; ++j) {
+        const u64 p = P[j];
+        u64 phatinv = hm::invmod(hm::prod_mod(P.data(), K, p, (int)j), p);
+        pdn[j] = hm::mulmod(phatinv, hm::invmod(n, p), p);
+        pdnp[j] = hm::precon(pdn[j], p);
+        for (uint32_t i = 0; i < fullQ; ++i) phatmodq[(size_t)j * fullQ + i] = hm::prod_mod(P.data(), K, Q[i], (int)j);
+    }
+
+    // per-level constants
+    lv_host_.assign(fullQ + 1, Level{});
+    std::vector<u64> pool;
+    for (uint32_t L = 1; L <= fullQ; ++L) {
+        Level& lv = lv_host_[L];
+        lv.L = L;
+        lv.nparts = (L + alpha - 1) / alpha;
+        for (uint32_t p = 0; p < lv.nparts; ++p) {
+            lv.part_st[p] = alpha * p;
+            lv.part_sp[p] = (L > alpha * p + alpha) ? alpha : L - alpha * p;
+        }
+        lv.qmp_off = (u32)pool.size();
+        const uint32_t QlP = L + K;
+        for (uint32_t i = 0; i < L; ++i) {
+            const uint32_t p = i / alpha, st = lv.part_st[p], sp = lv.part_sp[p];
+            const u64 q = Q[i];
+            // (partQ / q_i)^-1 mod q_i  (ks_constants.cpp:79-84), times n^-1
+            u64 qhat = hm::prod_mod(Q.data() + st, sp, q, (int)(i - st));
+            lv.up_scale[i] = hm::mulmod(hm::invmod(qhat, q), ninv[i], q);
+            lv.up_scale_p[i] = hm::precon(lv.up_scale[i], q);
+            for (uint32_t j = 0; j < QlP; ++j) {
+                const u64 m = j < L ? Q[j] : P[j - L];
+                pool.push_back(hm::prod_mod(Q.data() + st, sp, m, (int)(i - st)));
+            }
+        }
+        if (L >= 2) {
+            // params.cpp:54-75: s1 = ql^-1 mod q_i, s2 = floor(Ql*u/ql) mod q_i
+            const uint32_t last = L - 1;
+            const u64 ql = Q[last];
+            u64 QlModql = 1 % ql;
+            for (uint32_t t = 0; t < last; ++t) QlModql = hm::mulmod(QlModql, Q[t] % ql, ql);
+            const u64 u = hm::invmod(QlModql, ql);
+            for (uint32_t i = 0; i < last; ++i) {
+                const u64 qi = Q[i];
+                lv.s1[i] = hm::invmod(ql % qi, qi);
+                u128 m2 = (u128)ql * qi, Ql2 = 1 % m2;
+                for (uint32_t t = 0; t < last; ++t) Ql2 = mulmod128(Ql2, Q[t], m2);
+                u128 prod = mulmod128(Ql2, u, m2);
+                u128 pm1 = prod == 0 ? m2 - 1 : prod - 1;
+                lv.s2[i] = (u64)((pm1 / ql) % qi);
+                lv.s1p[i] = hm::precon(lv.s1[i], qi);
+                lv.s2p[i] = hm::precon(lv.s2[i], qi);
+                lv.ps1[i] = hm::mulmod(pinv[i], lv.s1[i], qi);
+                lv.ps1p[i] = hm::precon(lv.ps1[i], qi);
+            }
+        }
+    }
+
+    dc_.n = n; dc_.logn = logn_; dc_.fullQ = fullQ; dc_.K = K; dc_.alpha = alpha; dc_.dnum = dnum_; dc_.QP = QP;
+    dc_.mod = upload(mc);
+    dc_.twf = upload(twf);
+    dc_.twi = upload(twi);
+    dc_.ninv = upload(ninv);
+    dc_.ninvp = upload(ninvp);
+    dc_.lvl = upload(lv_host_);
+    dc_.pool = upload(pool);
+    dc_.pinv = upload(pinv);
+    dc_.pinvp = upload(pinvp);
+    dc_.pdn = upload(pdn);
+    dc_.pdnp = upload(pdnp);
+    dc_.phatmodq = upload(phatmodq);
+}
+
+Context::~Context() {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device_);
+    for (auto& kv : keys_) { cudaFree(kv.second.av); cudaFree(kv.second.bv); }
+    for (void* p : allocs_) cudaFree(p);
+    cudaSetDevice(prev);
+}
+
+void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
+    std::lock_guard<std::mutex> g(mu_);
+    const size_t words = (size_t)dnum_ * (fullQ() + K()) * n_;
+    Key k;
+    auto up = [&](const u64* h) {
+        u64* d = nullptr;
+        cudaError_t e = cudaMalloc(&d, words * 8);
+        if (e != cudaSuccess) throw std::runtime_error(std::string("key cudaMalloc: ") + cudaGetErrorString(e));
+        e = cudaMemcpy(d, h, words * 8, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { cudaFree(d); throw std::runtime_error("key upload failed"); }
+        return d;
+    };
+    k.av = up(av);
+    k.bv = up(bv);
+    auto it = keys_.find(id);
+    if (it != keys_.end()) { cudaFree(it->second.av); cudaFree(it->second.bv); }
+    keys_[id] = k;
+}
+
+const Key* Context::key(uint64_t id) const {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = keys_.find(id);
+    return it == keys_.end() ? nullptr : &it->second;
+}
+
+size_t Context::key_bytes() const {
+    std::lock_guard<std::mutex> g(mu_);
+    return keys_.size() * 2 * (size_t)dnum_ * (fullQ() + K()) * n_ * 8;
+}
+
+}  // namespace gfx

@@ -1,0 +1,105 @@
+// Resident CKKS context: the modulus chain Q (fullQ towers) and special
+// primes P (K towers) with digit width alpha, their twiddle tables, every
+// per-level keyswitch / ModDown / rescale constant, and the resident eval keys.
+// Everything a kernel needs is reachable from the POD `DevCtx`, passed by
+// value to each launch.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gf.cuh"
+
+namespace gfx {
+
+constexpr int MAXQ = 48;     // Q towers
+constexpr int MAXP = 16;     // special primes
+constexpr int MAXQP = MAXQ + MAXP;
+constexpr int MAXD = 48;     // digits
+
+// Constants for one level L (L Q towers, dropping tower L-1 on rescale).
+struct Level {
+    u32 L, nparts;
+    u32 part_st[MAXD], part_sp[MAXD];
+    u32 qmp_off;                       // pool offset of qhatmodp [L][L+K]
+    u64 up_scale[MAXQ], up_scale_p[MAXQ];    // n^-1 * QHatInv_i (i's digit) mod q_i
+    // rescale of tower L-1 onto i < L-1
+    u64 s1[MAXQ], s1p[MAXQ];           // q_l^-1 mod q_i
+    u64 s2[MAXQ], s2p[MAXQ];           // floor(Ql*(Ql^-1 mod q_l)/q_l) mod q_i
+    u64 ps1[MAXQ], ps1p[MAXQ];         // P^-1 * s1 mod q_i
+};
+
+struct DevCtx {
+    u32 n, logn, fullQ, K, alpha, dnum, QP;
+    const ModC* mod;          // [QP]: Q towers then P towers
+    const Tw* twf;            // [QP][n]
+    const Tw* twi;            // [QP][n]
+    const u64* ninv;          // [QP] n^-1 mod q
+    const u64* ninvp;
+    const Level* lvl;         // [fullQ + 1]
+    const u64* pool;          // qhatmodp pools
+    const u64* pinv;          // [fullQ] P^-1 mod q_i
+    const u64* pinvp;
+    const u64* pdn;           // [K] n^-1 * (P/p_j)^-1 mod p_j
+    const u64* pdnp;
+    const u64* phatmodq;      // [K][fullQ] (P/p_j) mod q_i
+};
+
+// A resident eval key: av/bv over full QP for every digit, canonical eval
+// form, layout [dnum][fullQ+K][n].
+struct Key {
+    u64* av = nullptr;
+    u64* bv = nullptr;
+};
+
+class Context {
+public:
+    Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& P, uint32_t alpha,
+            const std::vector<u64>& roots /* empty: native roots */, int device);
+    ~Context();
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+
+    const DevCtx& dev() const { return dc_; }
+    uint32_t n() const { return n_; }
+    uint32_t logn() const { return logn_; }
+    uint32_t fullQ() const { return (uint32_t)Q_.size(); }
+    uint32_t K() const { return (uint32_t)P_.size(); }
+    uint32_t alpha() const { return alpha_; }
+    uint32_t dnum() const { return dnum_; }
+    const std::vector<u64>& Q() const { return Q_; }
+    const std::vector<u64>& P() const { return P_; }
+    const std::vector<u64>& roots() const { return roots_; }
+    const Level& level_host(uint32_t L) const { return lv_host_[L]; }
+    int device() const { return device_; }
+
+    // Upload a key (host [dnum][fullQ+K][n] canonical). id 0 = relinearisation;
+    // rotation keys are stored under their Galois element.
+    void set_key(uint64_t id, const u64* av, const u64* bv);
+    const Key* key(uint64_t id) const;
+    size_t key_bytes() const;
+    size_t resident_bytes() const { return table_bytes_ + key_bytes(); }
+
+private:
+    uint32_t n_, logn_, alpha_, dnum_;
+    int device_;
+    std::vector<u64> Q_, P_, roots_;
+    std::vector<Level> lv_host_;
+    DevCtx dc_{};
+    std::vector<void*> allocs_;
+    size_t table_bytes_ = 0;
+    std::map<uint64_t, Key> keys_;
+    mutable std::mutex mu_;
+    void* dalloc(size_t bytes);
+    template <class T>
+    T* upload(const std::vector<T>& h);
+};
+
+std::string last_error();
+void set_error(const std::string& s);
+
+}  // namespace gfx

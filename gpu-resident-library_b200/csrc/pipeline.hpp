@@ -1,0 +1,41 @@
+// Host interface of the batched pipeline (pipeline.cu).
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "context.hpp"
+#include "pipeline.cuh"
+
+namespace pl {
+
+// One operation of a batch; see Mode for the meaning of in/out.
+struct Op {
+    uint32_t L = 0;
+    uint32_t mode = EMR;
+    uint64_t key_id = 0;      // context key (0 = relinearisation)
+    uint64_t galois = 0;      // ROT: Galois element
+    const u64* in[4] = {nullptr, nullptr, nullptr, nullptr};
+    u64* out[2] = {nullptr, nullptr};
+};
+
+struct Plan {
+    DevCtx dc{};
+    uint32_t logn = 0, nops = 0;
+    PairDesc* d_pairs = nullptr;
+    uint2* d_jobs = nullptr;
+    size_t job_off[7] = {};
+    uint32_t job_cnt[7] = {};
+    u64* ws = nullptr;
+    size_t ws_words = 0;
+    bool own_ws = false;
+    ~Plan();
+};
+
+bool supported_logn(int logn);
+size_t op_workspace_words(const gfx::Context& c, uint32_t L);
+void validate(const gfx::Context& c, const Op& op);
+// ws == nullptr: the plan allocates (and owns) its workspace.
+std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words);
+cudaError_t launch(const Plan& p, cudaStream_t s);
+
+}  // namespace pl

@@ -1,0 +1,122 @@
+// Batched in-place forward / inverse NTT kernels over a list of tower jobs.
+// One launch per pass covers every job (ciphertexts x towers): grid =
+// jobs x tiles-per-job. Used by the reference ABI (LaunchNTT_CT /
+// LaunchINTT_GS, one job) and by the batched transform entry points.
+#pragma once
+#include "ntt.cuh"
+
+namespace xf {
+
+// One tower to transform in place. Twiddles either packed {w, wp} (library
+// tables) or split (two arrays, the reference's table layout).
+struct Job {
+    u64* x;
+    const Tw* tw;        // packed tables, or nullptr when split
+    const u64* w;        // split tables
+    const u64* wp;
+    u64 q;
+    u64 scale, scale_p;  // inverse only: n^-1 (and precon) folded in at the end
+};
+
+template <class F>
+__device__ __forceinline__ auto with_tw(const Job& j, F&& f) {
+    if (j.tw) return f(ntt::TwPacked{j.tw});
+    return f(ntt::TwSplit{j.w, j.wp});
+}
+
+// Jobs come either from a device array (SINGLE = false) or a single by-value
+// kernel parameter (SINGLE = true, the reference ABI's one-tower calls).
+template <bool SINGLE>
+__device__ __forceinline__ Job get_job(const Job* __restrict__ arr, const Job& one, int i) {
+    if constexpr (SINGLE) return one;
+    else return arr[i];
+}
+
+template <int LOGN, bool SINGLE>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
+k_fwd_col(const Job* __restrict__ arr, const Job one) {
+    using G = ntt::Geo<LOGN>;
+    extern __shared__ __align__(16) u64 sm[];
+    const int job = blockIdx.x / G::COL_TILES;
+    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
+    const Job j = get_job<SINGLE>(arr, one, job);
+    const u64 q = j.q, two_q = 2 * q;
+    u64* x = j.x;
+    auto ld = [&](int r, int cl) { return x[r * 256 + c0 + cl]; };
+    auto st = [&](int r, int cl, u64 v) { x[r * 256 + c0 + cl] = v; };
+    with_tw(j, [&](auto tw) {
+        ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0>(sm, tw, q, two_q, ld, st);
+        return 0;
+    });
+}
+
+template <int LOGN, bool SINGLE>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS)
+k_fwd_row(const Job* __restrict__ arr, const Job one) {
+    using G = ntt::Geo<LOGN>;
+    extern __shared__ __align__(16) u64 sm[];
+    const int job = blockIdx.x / G::ROW_TILES;
+    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
+    const Job j = get_job<SINGLE>(arr, one, job);
+    const u64 q = j.q, two_q = 2 * q;
+    u64* x = j.x + (size_t)R0 * 256;
+    auto ld = [&](int rl, int c) { return x[rl * 256 + c]; };
+    with_tw(j, [&](auto tw) {
+        ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0>(sm, tw, R0, q, two_q, ld);
+        return 0;
+    });
+    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
+        u64 v = sm[rl * G::ROW_STRIDE + ntt::rowpad(c)];
+        v = csub(csub(v, two_q), q);
+        x[rl * 256 + c] = v;
+    });
+}
+
+template <int LOGN, bool SINGLE>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS)
+k_inv_row(const Job* __restrict__ arr, const Job one) {
+    using G = ntt::Geo<LOGN>;
+    extern __shared__ __align__(16) u64 sm[];
+    const int job = blockIdx.x / G::ROW_TILES;
+    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
+    const Job j = get_job<SINGLE>(arr, one, job);
+    const u64 q = j.q, two_q = 2 * q;
+    u64* x = j.x + (size_t)R0 * 256;
+    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
+        sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = x[rl * 256 + c];
+    });
+    __syncthreads();
+    auto st = [&](int rl, int c, u64 v) { x[rl * 256 + c] = v; };
+    with_tw(j, [&](auto tw) {
+        ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, tw, R0, q, two_q, st);
+        return 0;
+    });
+}
+
+template <int LOGN, bool SINGLE>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
+k_inv_col(const Job* __restrict__ arr, const Job one) {
+    using G = ntt::Geo<LOGN>;
+    extern __shared__ __align__(16) u64 sm[];
+    const int job = blockIdx.x / G::COL_TILES;
+    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
+    const Job j = get_job<SINGLE>(arr, one, job);
+    const u64 q = j.q, two_q = 2 * q;
+    u64* x = j.x;
+    auto ld = [&](int r, int cl) { return x[r * 256 + c0 + cl]; };
+    const u64 sc = j.scale, scp = j.scale_p;
+    auto st = [&](int r, int cl, u64 v) { x[r * 256 + c0 + cl] = shoup(v, sc, scp, q); };
+    with_tw(j, [&](auto tw) {
+        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, tw, q, two_q, ld, st);
+        return 0;
+    });
+}
+
+}  // namespace xf
+
+// Host-side dispatch (xform.cu). `jobs` is a device array of njobs jobs, or
+// nullptr with `one` used for a single job. Returns cudaErrorInvalidValue for
+// an unsupported ring size.
+cudaError_t xf_launch_ntt(const xf::Job* jobs, const xf::Job* one, int njobs, int logn,
+                          bool inverse, cudaStream_t s);
+bool xf_supported_logn(int logn);

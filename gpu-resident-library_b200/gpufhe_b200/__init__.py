@@ -1,0 +1,190 @@
+"""Python bindings for libgpufhe_b200.so (B200-native resident CKKS path).
+
+The shared library is the product; this module only loads it with ctypes and
+declares the C-ABI signatures from include/*.h. There is no CPU fallback: if
+the library is missing or no CUDA device is present, calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpufhe_b200.so")
+
+VP, U32, U64, I32, DBL = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_double
+
+_lib = None
+
+# reference ABI: include/{ntt,intt,rns_arith,switch_modulus,rescale,basis_convert,
+# ks_fastcore,moddown,tensor,automorph,stage_acc}.h
+_REF_ABI = {
+    "LaunchNTT_CT": [VP, VP, VP, U32, U64, VP],
+    "LaunchINTT_GS": [VP, VP, VP, U32, U64, U64, U64, VP],
+    "LaunchRNSMultTower": [VP, VP, VP, U64, U32, VP],
+    "LaunchSwitchModulus": [VP, U64, U64, U32, VP],
+    "LaunchRescaleFuse": [VP, VP, U64, U64, U64, U32, VP],
+    "LaunchApproxSwitchCRTBasis": [VP, VP, VP, VP, VP, VP, VP, VP, VP, U32, U32, U32, VP],
+    "LaunchKSMultAcc": [VP, VP, VP, VP, VP, U64, U32, VP],
+    "LaunchKSMultAccBatched": [VP, VP, VP, VP, VP, VP, VP, U32, U32, VP],
+    "LaunchModDownCombine": [VP, VP, VP, U64, U64, U32, VP],
+    "LaunchTensor": [VP, VP, VP, VP, VP, VP, VP, VP, U32, U32, VP],
+    "LaunchCombine": [VP, VP, VP, VP, VP, VP, VP, U32, U32, VP],
+    "LaunchAutomorphPermute": [VP, VP, U32, U64, U64, VP],
+    "LaunchPtMulAcc": [VP, VP, VP, VP, VP, U64, U32, VP],
+    "LaunchAddInto": [VP, VP, U64, U32, VP],
+}
+
+CP = C.c_char_p
+_API: dict = {
+    "gpufhe_last_error": (CP, []),
+    "gpufhe_ctx_create": (I32, [U32, VP, U32, VP, U32, U32, VP, I32, C.POINTER(VP)]),
+    "gpufhe_ctx_destroy": (None, [VP]),
+    "gpufhe_ctx_roots": (I32, [VP, VP]),
+    "gpufhe_ctx_set_key": (I32, [VP, U64, VP, VP]),
+    "gpufhe_ctx_resident_bytes": (U64, [VP]),
+    "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
+    "gpufhe_ntt_job_bytes": (U64, []),
+    "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),
+    "gpufhe_op_workspace_bytes": (U64, [VP, U32]),
+    "gpufhe_plan_create": (I32, [VP, U32, VP, VP, U64, C.POINTER(VP)]),
+    "gpufhe_plan_launch": (I32, [VP, VP]),
+    "gpufhe_plan_destroy": (None, [VP]),
+    "gpufhe_run_ops": (I32, [VP, U32, VP, VP]),
+}
+
+EVALMULT_RESCALE, KEYSWITCH, ROTATE, RESCALE = 0, 1, 2, 3
+
+
+class Op(C.Structure):
+    """struct gpufhe_op (include/gpufhe_b200.h)."""
+    _fields_ = [("level", U32), ("mode", U32), ("key_id", U64), ("galois", U64),
+                ("inp", VP * 4), ("out", VP * 2)]
+
+
+
+def lib():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m gpufhe_b200.build` "
+                               "(or __graft_entry__.build()) first")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _REF_ABI.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = None
+        for name, (res, args) in _API.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def ref_abi_symbols():
+    return list(_REF_ABI)
+
+
+class GpuFheError(RuntimeError):
+    pass
+
+
+def check(rc):
+    if rc != 0:
+        raise GpuFheError(f"gpufhe status {rc}: {lib().gpufhe_last_error().decode()}")
+    return rc
+
+
+def api_symbols():
+    return list(_API)
+
+
+def _np_u64(a):
+    import numpy as np
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+class Context:
+    """Owns a gpufhe_ctx handle (chain, tables, constants, resident keys)."""
+
+    def __init__(self, n, Q, P, alpha, roots=None, device=0):
+        self._Q, self._P = _np_u64(Q), _np_u64(P)
+        r = _np_u64(roots) if roots is not None else None
+        h = VP()
+        check(lib().gpufhe_ctx_create(n, self._Q.ctypes.data, len(self._Q), self._P.ctypes.data, len(self._P),
+                                      alpha, r.ctypes.data if r is not None else None, device, C.byref(h)))
+        self.h, self.n, self.alpha = h, n, alpha
+        self.fullQ, self.K = len(self._Q), len(self._P)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpufhe_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_key(self, key_id, av, bv):
+        av, bv = _np_u64(av), _np_u64(bv)
+        check(lib().gpufhe_ctx_set_key(self.h, key_id, av.ctypes.data, bv.ctypes.data))
+
+    def roots(self):
+        import numpy as np
+        r = np.zeros(self.fullQ + self.K, np.uint64)
+        check(lib().gpufhe_ctx_roots(self.h, r.ctypes.data))
+        return r
+
+    def workspace_bytes(self, level):
+        return int(lib().gpufhe_op_workspace_bytes(self.h, level))
+
+    def resident_bytes(self):
+        return int(lib().gpufhe_ctx_resident_bytes(self.h))
+
+
+def make_ops(specs):
+    """specs: iterable of dicts {level, mode, key_id, galois, inp: [ptrs], out: [ptrs]}."""
+    specs = list(specs)
+    arr = (Op * max(1, len(specs)))()
+    for i, s in enumerate(specs):
+        o = arr[i]
+        o.level, o.mode = s["level"], s.get("mode", EVALMULT_RESCALE)
+        o.key_id, o.galois = s.get("key_id", 0), s.get("galois", 0)
+        for k, p in enumerate(s.get("inp", [])):
+            o.inp[k] = p
+        for k, p in enumerate(s.get("out", [])):
+            o.out[k] = p
+    return arr, len(specs)
+
+
+class Plan:
+    """A built batch (job tables + workspace); launch() only enqueues kernels."""
+
+    def __init__(self, ctx, specs, d_ws=None, ws_bytes=0):
+        self.ops, self.nops = make_ops(specs)
+        h = VP()
+        check(lib().gpufhe_plan_create(ctx.h, self.nops, C.cast(self.ops, VP), d_ws, ws_bytes, C.byref(h)))
+        self.h = h
+
+    def launch(self, stream=None):
+        check(lib().gpufhe_plan_launch(self.h, stream))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpufhe_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_ops(ctx, specs, stream=None):
+    ops, n = make_ops(specs)
+    check(lib().gpufhe_run_ops(ctx.h, n, C.cast(ops, VP), stream))

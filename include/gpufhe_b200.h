@@ -1,0 +1,112 @@
+/*
+ * gpufhe_b200 — B200-native resident leveled-CKKS hot path, C ABI.
+ *
+ * The reference (samfrazerdutton/GPU-Resident-Library) exposes its hot path
+ * as 14 extern "C" Launch* kernels (ntt.h, intt.h, rns_arith.h, ...; same
+ * names and semantics are exported by this library, see those headers) and a
+ * C++ API (device_ciphertext.h, ckks_ops.h, keyswitch_resident.h, keygen.h).
+ * This header adds the batched / serving entry points that the reference has
+ * no counterpart for, as plain C: opaque handles, raw pointers, sizes, and an
+ * int status (0 = success, negative = error; gpufhe_last_error() explains).
+ *
+ * Data layout everywhere: tower-major [tower][coeff] uint64 residues in
+ * [0, q), eval form = the reference's bit-reversed NTT order.
+ */
+#ifndef GPUFHE_B200_H
+#define GPUFHE_B200_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPUFHE_OK 0
+#define GPUFHE_EINVAL (-1)   /* bad argument, unsupported size, missing key */
+#define GPUFHE_ECUDA (-2)    /* a CUDA call failed */
+#define GPUFHE_ENOMEM (-3)   /* workspace or HBM budget too small */
+#define GPUFHE_EBUSY (-4)    /* server queue full / request not admitted yet */
+#define GPUFHE_ETIMEOUT (-5) /* bounded wait expired */
+
+typedef struct gpufhe_ctx gpufhe_ctx;
+
+const char* gpufhe_last_error(void);
+
+/* ---------------------------------------------------------------- context
+ * Modulus chain Q[0..fullQ) and special primes P[0..K), digit width alpha
+ * (towers per Hybrid digit, fixed across levels so one full-QP key serves
+ * every level). roots_qp: the 2n-th roots for Q then P, or NULL for the
+ * smallest-generator roots (the reference's native_root). Builds twiddle
+ * tables and every per-level constant on `device`. Replaces the per-call
+ * setup of ks_context_create (reference keyswitch_resident.cpp:32-101). */
+int  gpufhe_ctx_create(uint32_t n, const uint64_t* Q, uint32_t fullQ, const uint64_t* P, uint32_t K,
+                       uint32_t alpha, const uint64_t* roots_qp, int device, gpufhe_ctx** out);
+void gpufhe_ctx_destroy(gpufhe_ctx* ctx);
+int  gpufhe_ctx_roots(const gpufhe_ctx* ctx, uint64_t* roots_qp);
+/* Key over full QP, host [dnum][fullQ+K][n] (dnum = ceil(fullQ/alpha)),
+ * canonical eval form (reference KeySwitchConstants::av/bv, keyswitch.h:35-39).
+ * key_id 0 = relinearisation key; rotation keys use their Galois element. */
+int  gpufhe_ctx_set_key(gpufhe_ctx* ctx, uint64_t key_id, const uint64_t* av, const uint64_t* bv);
+uint64_t gpufhe_ctx_resident_bytes(const gpufhe_ctx* ctx);
+
+/* ---------------------------------------------------------------- transforms
+ * Batched forward/inverse NTT of npolys x towers tower-polys stored
+ * contiguously ([poly][tower][n]); tower t uses modulus first_tower + t in
+ * Q||P order. d_jobs: device scratch of npolys*towers*gpufhe_ntt_job_bytes()
+ * bytes that receives the job list; gpufhe_ntt_run_jobs re-launches a
+ * prepared list (capturable in a CUDA graph). */
+int gpufhe_ntt_batch(gpufhe_ctx* ctx, uint64_t* d_data, uint32_t npolys, uint32_t towers, uint32_t first_tower,
+                     int inverse, uint64_t* d_jobs, cudaStream_t stream);
+uint64_t gpufhe_ntt_job_bytes(void);
+int gpufhe_ntt_run_jobs(gpufhe_ctx* ctx, const uint64_t* d_jobs, uint32_t njobs, int inverse,
+                        cudaStream_t stream);
+
+
+/* ---------------------------------------------------------------- batched ops
+ * One entry per ciphertext operation; a batch may mix levels and modes.
+ *   GPUFHE_EVALMULT_RESCALE: in = {c0a, c1a, c0b, c1b} ([level][n] each),
+ *       out = {r0, r1} ([level-1][n]): tensor -> Hybrid relinearisation ->
+ *       combine -> rescale, the reference's bench_evalmult_resident.cpp:96-100
+ *       chain, bit-exact.
+ *   GPUFHE_KEYSWITCH: in[0] = a, out = {ba0, ba1} (keyswitch_resident,
+ *       keyswitch_resident.cpp:139-225) with key `key_id`.
+ *   GPUFHE_ROTATE: in = {c0, c1}, out = {sigma(c0)+ba0, ba1} with Galois
+ *       element `galois` and the rotation key `key_id` (rotate_ct_device,
+ *       rotate.cpp:118-132). Outputs must not alias inputs.
+ *   GPUFHE_RESCALE: in[0] = comp [level][n] -> out[0] [level-1][n]
+ *       (rescale_resident_raw, keyswitch_resident.cpp:227-244); out may alias in.
+ * Device pointers; ring sizes 2^11..2^16. */
+#define GPUFHE_EVALMULT_RESCALE 0u
+#define GPUFHE_KEYSWITCH 1u
+#define GPUFHE_ROTATE 2u
+#define GPUFHE_RESCALE 3u
+
+typedef struct gpufhe_op {
+    uint32_t level;
+    uint32_t mode;
+    uint64_t key_id;
+    uint64_t galois;
+    const uint64_t* in[4];
+    uint64_t* out[2];
+} gpufhe_op;
+
+typedef struct gpufhe_plan gpufhe_plan;
+
+/* Device workspace one operation at `level` needs (sum over a batch). */
+uint64_t gpufhe_op_workspace_bytes(gpufhe_ctx* ctx, uint32_t level);
+/* Builds the per-phase job tables of a batch (one small device allocation).
+ * d_ws: caller workspace of ws_bytes, or NULL for a plan-owned one. */
+int  gpufhe_plan_create(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, uint64_t* d_ws, uint64_t ws_bytes,
+                        gpufhe_plan** out);
+/* Launches the seven phase kernels for the whole batch on `stream`
+ * (kernel launches only: capturable in a CUDA graph). */
+int  gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t stream);
+void gpufhe_plan_destroy(gpufhe_plan* plan);
+/* create + launch + synchronize + destroy */
+int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUFHE_B200_H */

@@ -1,0 +1,101 @@
+"""Batched pipeline (gpufhe_plan_* C ABI) bit-exact against the CPU oracle:
+EvalMult+Rescale over uneven levels, keyswitch, rotation and rescale."""
+import numpy as np
+import pytest
+
+import oracle as O
+from ckks_setup import Setup
+from gpu_util import dev, empty, host, ptr, sync
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def G():
+    import gpufhe_b200
+    return gpufhe_b200
+
+
+@pytest.fixture(scope="module")
+def S():
+    return Setup(4096, 12, K=3, alpha=3, rot_ks=(5, O.galois_element(-2, 4096)))
+
+
+@pytest.fixture(scope="module")
+def gctx(S):
+    return S.gpu_context()
+
+
+def test_evalmult_rescale_uneven_batch(G, S, gctx):
+    rng = np.random.default_rng(2024)
+    levels = [2, 3, 4, 5, 7, 9, 12, 12, 6]
+    n = S.n
+    keep, specs, want = [], [], []
+    for L in levels:
+        c0a, c1a = S.rand_ct(rng, L)
+        c0b, c1b = S.rand_ct(rng, L)
+        ins = [dev(x) for x in (c0a, c1a, c0b, c1b)]
+        outs = [empty((L - 1) * n), empty((L - 1) * n)]
+        keep += ins + outs
+        specs.append(dict(level=L, mode=G.EVALMULT_RESCALE, inp=[ptr(x) for x in ins], out=[ptr(x) for x in outs]))
+        want.append(S.octx.evalmult_rescale(L, c0a, c1a, c0b, c1b))
+    plan = G.Plan(gctx, specs)
+    for rep in range(2):   # replay: same bits every time, outputs cleared in between
+        for x in keep[4::6] + keep[5::6]:
+            x.zero_()
+        plan.launch()
+        sync()
+        for j, L in enumerate(levels):
+            o0, o1 = host(keep[6 * j + 4]), host(keep[6 * j + 5])
+            assert np.array_equal(o0, want[j][0]), (rep, L)
+            assert np.array_equal(o1, want[j][1]), (rep, L)
+
+
+@pytest.mark.parametrize("L", [1, 3, 8, 12])
+def test_keyswitch(G, S, gctx, L):
+    rng = np.random.default_rng(L)
+    a = S.rand_ct(rng, L)[0]
+    da, b0, b1 = dev(a), empty(L * S.n), empty(L * S.n)
+    G.run_ops(gctx, [dict(level=L, mode=G.KEYSWITCH, inp=[ptr(da)], out=[ptr(b0), ptr(b1)])])
+    e0, e1 = S.octx.keyswitch(L, a)
+    assert np.array_equal(host(b0), e0) and np.array_equal(host(b1), e1)
+
+
+@pytest.mark.parametrize("L", [2, 5, 12])
+def test_rescale(G, S, gctx, L):
+    rng = np.random.default_rng(100 + L)
+    c = S.rand_ct(rng, L)[0]
+    dc = dev(c)
+    G.run_ops(gctx, [dict(level=L, mode=G.RESCALE, inp=[ptr(dc)], out=[ptr(dc)])])
+    assert np.array_equal(host(dc)[: (L - 1) * S.n], S.octx.rescale(L, c))
+
+
+@pytest.mark.parametrize("L", [4, 12])
+def test_rotate(G, S, gctx, L):
+    rng = np.random.default_rng(200 + L)
+    for k in S.rot:
+        c0, c1 = S.rand_ct(rng, L)
+        d0, d1, o0, o1 = dev(c0), dev(c1), empty(L * S.n), empty(L * S.n)
+        G.run_ops(gctx, [dict(level=L, mode=G.ROTATE, key_id=k, galois=k, inp=[ptr(d0), ptr(d1)],
+                              out=[ptr(o0), ptr(o1)])])
+        e0, e1 = S.octx.rotate(L, k, c0, c1, k)
+        assert np.array_equal(host(o0), e0) and np.array_equal(host(o1), e1), k
+
+
+def test_evalmult_rescale_decrypts(G, S, gctx):
+    """Known-answer product (test_evalmult_rescale.cpp:82-93 at scale 2^40)."""
+    n, L = S.n, 12
+    sQ, pkA, pkB = S.octx.keygen(L, seed=101)
+    D = 1 << 40
+    m1 = np.zeros(n, np.int64); m1[0], m1[1] = 3 * D, -2 * D
+    m2 = np.zeros(n, np.int64); m2[0], m2[2] = 4 * D, 5 * D
+    c0a, c1a = S.octx.encrypt(L, m1, pkA, pkB, seed=303)
+    c0b, c1b = S.octx.encrypt(L, m2, pkA, pkB, seed=304)
+    ins = [dev(x) for x in (c0a, c1a, c0b, c1b)]
+    o0, o1 = empty((L - 1) * n), empty((L - 1) * n)
+    G.run_ops(gctx, [dict(level=L, inp=[ptr(x) for x in ins], out=[ptr(o0), ptr(o1)])])
+    sR, _, _ = S.octx.keygen(L - 1, seed=101)
+    dec = S.octx.decrypt_crt(L - 1, host(o0), host(o1), sR)
+    ql = int(S.Q[L - 1])
+    got = [round(v * ql / (D * D)) for v in dec[:6]]
+    assert got == [12, -8, 15, -10, 0, 0]
