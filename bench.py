@@ -1,0 +1,455 @@
+#!/usr/bin/env python
+"""EvalMult+Rescale throughput on B200: batched resident pipeline vs plain form.
+
+Workload (one "step"): 128 independent ciphertext pairs at N = 2^16, chain
+Q = one 60-bit + eleven 50-bit NTT-friendly primes, P = three 60-bit primes,
+dnum = 4 (alpha = 3), pair levels drawn uniformly from 4..12 (seeded). Each
+step runs tensor -> Hybrid relinearisation -> combine -> rescale on every
+pair, bit-exact with the reference's chain (the GPU parity tests check the
+bits; this script measures).
+
+Inputs are seeded uniform residues in [0, q_i) and a seeded uniform full-QP
+relinearisation key (throughput run: the arithmetic is identical for any
+residues). Inputs of one step (about 2 GiB) exceed L2 (126 MB), so no flush
+is needed between timed steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One process per GPU (torchrun for N > 1): every rank serves its own 128
+pairs (weak scaling, no data-path collective); the barrier and the max of
+the per-rank device times are the only cross-rank steps. Rank 0 prints one
+JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-resident-library_b200"))
+
+N_LOG = 16
+FULLQ, K_SPECIAL, ALPHA = 12, 3, 3
+PAIRS = 128
+LEVEL_RANGE = (4, 12)
+SEED = 20260725
+METRIC = "EvalMult+Rescale ops/s at N=2^16 (bit-exact), served vs plain; p50/p99 latency"
+WORKLOAD = ("batched EvalMult+Rescale, 128 independent ciphertext pairs, N=2^16, "
+            "Q=1x60+11x50-bit, P=3x60-bit, dnum=4, levels U{4..12}")
+
+
+def peaks():
+    p = {"hbm_gbs": 6650.0, "source": "fallback"}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        p = {"hbm_gbs": float(m["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        pass
+    return p
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def workload_levels(seed):
+    rng = np.random.default_rng(seed)
+    return [int(x) for x in rng.integers(LEVEL_RANGE[0], LEVEL_RANGE[1] + 1, PAIRS)]
+
+
+def chain(primes_fn, n):
+    q0 = primes_fn(1, 60, n)
+    qs = primes_fn(FULLQ - 1, 50, n, avoid=list(q0))
+    Q = np.concatenate([q0, qs])
+    P = primes_fn(K_SPECIAL, 60, n, avoid=list(Q))
+    return Q, P
+
+
+def algorithmic_bytes(levels, n):
+    """8N[4L + 2(L-1)] per op + the evk once per launch at the max level."""
+    ct = sum(8 * n * (4 * L + 2 * (L - 1)) for L in levels)
+    Lm = max(levels)
+    beta = -(-Lm // ALPHA)
+    return ct + 8 * n * 2 * beta * (Lm + K_SPECIAL)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.lines = []
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU oracle
+def cpu_port_rate(levels, n, nthreads, budget_s=20.0):
+    """Oracle (CPU restatement of the reference path) on a bounded sample."""
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    Q, P = chain(O.native_primes, n)
+    ctx = O.Ctx(n, Q, P, ALPHA)
+    rng = np.random.default_rng(SEED + 7)
+    rows = ctx.dnum * (FULLQ + K_SPECIAL)
+    QP = ctx.QP
+    av = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+    bv = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+    ctx.set_key(0, av, bv)
+    threads = nthreads or O.num_threads()
+    sample = levels[:max(1, min(len(levels), threads))]
+    ins = [[np.concatenate([rng.integers(0, int(q), n, dtype=np.uint64) for q in Q[:L]]) for L in sample]
+           for _ in range(4)]
+    reps, t_total = 0, 0.0
+    while True:
+        t0 = time.perf_counter()
+        ctx.evalmult_rescale_batch(sample, *ins, nthreads=threads)
+        t_total += time.perf_counter() - t0
+        reps += 1
+        if t_total > budget_s / 4 or reps >= 3:
+            break
+    return {"value": reps * len(sample) / t_total, "unit": "ops/s", "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} pairs (levels {sample}) x {reps} reps of the same N=2^16 workload, "
+                      f"OpenMP over pairs"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    n = 1 << N_LOG
+    levels = workload_levels(SEED)
+    Q, P = chain(O.native_primes, n)
+    ctx = O.Ctx(n, Q, P, ALPHA)
+    rng = np.random.default_rng(SEED + 7)
+    QP = ctx.QP
+    rows = ctx.dnum * (FULLQ + K_SPECIAL)
+    av = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+    bv = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+    ctx.set_key(0, av, bv)
+    threads = O.num_threads()
+    sample = levels[:max(1, min(len(levels), threads))]
+    ins = [[np.concatenate([rng.integers(0, int(q), n, dtype=np.uint64) for q in Q[:L]]) for L in sample]
+           for _ in range(4)]
+    for _ in range(args.warmup):
+        ctx.evalmult_rescale_batch(sample, *ins, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.evalmult_rescale_batch(sample, *ins, nthreads=threads)
+    dt = time.perf_counter() - t0
+    value = args.steps * len(sample) / dt
+    desc = (f"{len(sample)} pairs (levels {sample}) of the N=2^16 workload per step, OpenMP over pairs "
+            f"on {threads} host threads; the reference's CPU path restated (oracle/)")
+    line = {"metric": METRIC, "value": value, "unit": "ops/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "n": n, "pairs_per_step": len(sample), "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": "ops/s", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "ops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_gpu(args):
+    import torch
+    import gpufhe_b200 as G
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    n = 1 << N_LOG
+    Q, P = chain(G.native_primes, n)
+    ctx = G.Context(n, Q, P, ALPHA, device=local)
+    rng = np.random.default_rng(SEED + rank)
+    QP = np.concatenate([Q, P])
+    rows = -(-FULLQ // ALPHA) * len(QP)
+    av = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+    bv = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+    ctx.set_key(0, av, bv)
+    levels = workload_levels(SEED + rank)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + rank)
+
+    def residues(L):
+        t = torch.empty((L, n), dtype=torch.int64, device=dev)
+        for i in range(L):
+            t[i].random_(0, int(Q[i]), generator=gen)
+        return t
+
+    ins, outs, specs = [], [], []
+    for L in levels:
+        x = [residues(L) for _ in range(4)]
+        o = [torch.empty(((L - 1), n), dtype=torch.int64, device=dev) for _ in range(2)]
+        ins.append(x)
+        outs.append(o)
+        specs.append(dict(level=L, mode=G.EVALMULT_RESCALE, inp=[t.data_ptr() for t in x],
+                          out=[t.data_ptr() for t in o]))
+    ws_bytes = sum(ctx.workspace_bytes(L) for L in levels)
+    ws = torch.empty(ws_bytes // 8, dtype=torch.int64, device=dev)
+    plan = G.Plan(ctx, specs, ws.data_ptr(), ws_bytes)
+    kernels_per_step = plan.kernel_count()
+
+    stream = torch.cuda.Stream(device=dev)
+    graph = torch.cuda.CUDAGraph()
+    plan.launch(stream.cuda_stream)   # first launch outside capture (sets kernel attributes)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph, stream=stream):
+        plan.launch(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * PAIRS * args.steps / (ms * 1e-3)
+
+    # per-phase device times (outside the timed region)
+    cur = torch.cuda.current_stream().cuda_stream
+    phases = []
+    for k in range(7):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(3):
+            plan.launch_phase(k, cur)
+        b.record()
+        torch.cuda.synchronize()
+        phases.append(a.elapsed_time(b) / 3)
+
+    # e2e through the C-ABI host-buffer entry (pinned host memory)
+    h_in, h_out, keep = [], [], []
+    bi = bo = 0
+    for j, L in enumerate(levels):
+        for x in ins[j]:
+            hx = x.cpu().pin_memory()
+            keep.append(hx)
+            h_in.append(hx.data_ptr())
+            bi += hx.numel() * 8
+        for o in outs[j]:
+            ho = torch.empty(o.shape, dtype=torch.int64).pin_memory()
+            keep.append(ho)
+            h_out.append(ho.data_ptr())
+            bo += ho.numel() * 8
+    e2e_steps = max(1, min(args.steps, 5))
+    plan.launch_host(h_in, h_out, stream.cuda_stream)   # warm
+    barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(e2e_steps):
+        plan.launch_host(h_in, h_out, stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * PAIRS / (e2e_ms * 1e-3)
+
+    # plain per-chain form: one pair per plan, graph per chain, 16 streams
+    plain = None
+    if not args.no_plain:
+        nst = 16
+        streams = [torch.cuda.Stream(device=dev) for _ in range(nst)]
+        pplans, pgraphs = [], []
+        off = 0
+        for j, L in enumerate(levels):
+            wb = ctx.workspace_bytes(L)
+            pp = G.Plan(ctx, [specs[j]], ws.data_ptr() + off, wb)
+            off += wb
+            g = torch.cuda.CUDAGraph()
+            s = streams[j % nst]
+            with torch.cuda.graph(g, stream=s):
+                pp.launch(torch.cuda.current_stream().cuda_stream)
+            pplans.append(pp)
+            pgraphs.append((g, s))
+        torch.cuda.synchronize()
+        def plain_step():
+            for g, s in pgraphs:
+                with torch.cuda.stream(s):
+                    g.replay()
+        plain_step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(1, min(args.steps, 3))
+        a.record()
+        for _ in range(reps):
+            plain_step()
+        for s in streams:
+            torch.cuda.current_stream().wait_stream(s)
+        b.record()
+        torch.cuda.synchronize()
+        pms = a.elapsed_time(b) / reps
+        plain = {"value": PAIRS / (pms * 1e-3), "unit": "ops/s", "ms_per_step": pms,
+                 "form": "one pair per launch set (7 kernels), CUDA graph per chain, 16 streams"}
+        del pgraphs, pplans
+
+    # config-2 NTT kernel isolation: 64 polys x 12 towers x 2^16
+    ntt = None
+    if not args.no_ntt:
+        npol, tw = 64, 12
+        data = torch.empty(npol * tw * n, dtype=torch.int64, device=dev)
+        for t_ in range(tw):
+            data.view(npol, tw, n)[:, t_, :].random_(0, int(Q[t_]), generator=gen)
+        jb = int(G.lib().gpufhe_ntt_job_bytes())
+        jf = torch.empty(npol * tw * jb // 8, dtype=torch.int64, device=dev)
+        ji = torch.empty_like(jf)
+        G.check(G.lib().gpufhe_ntt_batch(ctx.h, data.data_ptr(), npol, tw, 0, 0, jf.data_ptr(), cur))
+        G.check(G.lib().gpufhe_ntt_batch(ctx.h, data.data_ptr(), npol, tw, 0, 1, ji.data_ptr(), cur))
+        torch.cuda.synchronize()
+        res = {}
+        for name, inv, jt in (("fwd", 0, jf), ("inv", 1, ji)):
+            for _ in range(3):
+                G.lib().gpufhe_ntt_run_jobs(ctx.h, jt.data_ptr(), npol * tw, inv, cur)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(10):
+                G.lib().gpufhe_ntt_run_jobs(ctx.h, jt.data_ptr(), npol * tw, inv, cur)
+            b.record()
+            torch.cuda.synchronize()
+            t_ms = a.elapsed_time(b) / 10
+            gbs = 2 * 8 * n * npol * tw / (t_ms * 1e-3) / 1e9
+            res[name] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"]}
+        ntt = {"workload": "64 polys x 12 towers x 2^16, 50-bit primes", "bytes_per_tower": 2 * 8 * n, **res}
+        del data
+
+    # CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_port_rate(levels, n, 0)
+
+    if dist is not None:
+        dist.barrier()
+        del graph
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    pk = peaks()
+    alg = algorithmic_bytes(levels, n)
+    achieved = alg / (ms_step * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "ops/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues and key)",
+        "config": {"workload": WORKLOAD, "n": n, "pairs_per_gpu": PAIRS, "levels": "U{4..12} seeded",
+                   "mean_level": float(np.mean(levels)), "l2": "inputs larger than L2 (no flush)",
+                   "graph": "7 kernels per step, one CUDA graph"},
+        "roofline": {"bound": "hbm", "kernel": "fused EvalMult+Rescale step (K1..K7)", "achieved": achieved,
+                     "peak": pk["hbm_gbs"], "peak_source": pk["source"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "algorithmic_bytes_per_launch": alg, "traffic": None},
+        "phases_ms": {f"K{k + 1}": p for k, p in enumerate(phases)},
+        "e2e": {"value": e2e_value, "unit": "ops/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
+                "ms_per_step": e2e_ms},
+        "plain": plain,
+        "served_vs_plain": (value / world / plain["value"]) if plain else None,
+        "latency_ms": {"p50": ms_step, "p99": ms_step, "mode": "whole batch per step"},
+        "ntt_kernel_isolation": ntt,
+        "gpu_launches": kernels_per_step * args.steps,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpufhe", choices=["gpufhe", "reference"])
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-ntt", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -64,6 +64,51 @@ int gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t s) {
     return GPUFHE_OK;
 }
 
+int gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t s) {
+    if (!plan || phase >= 7) { gfx::set_error("bad plan or phase"); return GPUFHE_EINVAL; }
+    cudaError_t e = pl::launch(*plan->p, s, 1u << phase);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
+}
+
+uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
+    if (!plan) return 0;
+    uint32_t k = 0;
+    for (int i = 0; i < 7; ++i) k += plan->p->job_cnt[i] ? 1 : 0;
+    return k;
+}
+
+int gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
+                            cudaStream_t s) {
+    if (!plan || !h_in || !h_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    const pl::Plan& p = *plan->p;
+    const size_t n = (size_t)1 << p.logn;
+    for (size_t i = 0; i < p.ops.size(); ++i) {
+        const pl::Op& op = p.ops[i];
+        for (int k = 0; k < pl::input_count(op.mode); ++k) {
+            const uint64_t* src = h_in[4 * i + k];
+            if (!src) continue;
+            cudaError_t e = cudaMemcpyAsync((void*)op.in[k], src, op.L * n * 8, cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+        }
+    }
+    cudaError_t e = pl::launch(p, s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    for (size_t i = 0; i < p.ops.size(); ++i) {
+        const pl::Op& op = p.ops[i];
+        const int nout = op.mode == pl::RESCALE ? 1 : 2;
+        for (int k = 0; k < nout; ++k) {
+            uint64_t* dst = h_out[2 * i + k];
+            if (!dst) continue;
+            e = cudaMemcpyAsync(dst, op.out[k], pl::output_towers(op) * n * 8, cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+        }
+    }
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
+}
+
 void gpufhe_plan_destroy(gpufhe_plan* plan) { delete plan; }
 
 int gpufhe_run_ops(gpufhe_ctx* h, uint32_t nops, const gpufhe_op* ops, cudaStream_t s) {

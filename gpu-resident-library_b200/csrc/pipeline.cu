@@ -27,7 +27,7 @@ struct Launcher {
         cudaFuncSetAttribute(k7_final_fwd_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
         done = true;
     }
-    static void launch(const Plan& p, cudaStream_t s) {
+    static void launch(const Plan& p, cudaStream_t s, unsigned mask) {
         using G = ntt::Geo<LOGN>;
         using PGL = PG<LOGN>;
         attrs();
@@ -35,19 +35,22 @@ struct Launcher {
         const PairDesc* pd = p.d_pairs;
         auto J = [&](int k) { return p.d_jobs + p.job_off[k]; };
         auto cnt = [&](int k) { return p.job_cnt[k]; };
-        if (cnt(0)) k1_inv_row<LOGN><<<cnt(0) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(0));
-        if (cnt(1)) k2_inv_col<LOGN><<<cnt(1) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(1));
-        if (cnt(2)) k3_modup_fwd_col<LOGN><<<cnt(2) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(2));
-        if (cnt(3)) k4_mac_fwd_row<LOGN><<<cnt(3) * PGL::MAC_TILES, PGL::MAC_THREADS, PGL::MAC_SMEM, s>>>(D, pd, J(3));
-        if (cnt(4)) k5_moddown_inv_col<LOGN><<<cnt(4) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(4));
-        if (cnt(5)) k6_moddown_fwd_col<LOGN><<<cnt(5) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(5));
-        if (cnt(6)) k7_final_fwd_row<LOGN><<<cnt(6) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(6));
+        if ((mask >> 0 & 1) && cnt(0)) k1_inv_row<LOGN><<<cnt(0) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(0));
+        if ((mask >> 1 & 1) && cnt(1)) k2_inv_col<LOGN><<<cnt(1) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(1));
+        if ((mask >> 2 & 1) && cnt(2)) k3_modup_fwd_col<LOGN><<<cnt(2) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(2));
+        if ((mask >> 3 & 1) && cnt(3)) k4_mac_fwd_row<LOGN><<<cnt(3) * PGL::MAC_TILES, PGL::MAC_THREADS, PGL::MAC_SMEM, s>>>(D, pd, J(3));
+        if ((mask >> 4 & 1) && cnt(4)) k5_moddown_inv_col<LOGN><<<cnt(4) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(4));
+        if ((mask >> 5 & 1) && cnt(5)) k6_moddown_fwd_col<LOGN><<<cnt(5) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(5));
+        if ((mask >> 6 & 1) && cnt(6)) k7_final_fwd_row<LOGN><<<cnt(6) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(6));
     }
 };
 
 }  // namespace
 
 bool supported_logn(int logn) { return logn >= 11 && logn <= 16; }
+
+int input_count(uint32_t mode) { return mode == EMR ? 4 : mode == ROT ? 2 : 1; }
+uint32_t output_towers(const Op& op) { return (op.mode == EMR || op.mode == RESCALE) ? op.L - 1 : op.L; }
 
 size_t op_workspace_words(const gfx::Context& c, uint32_t L) {
     return (size_t)ws_layout(L, c.K(), c.alpha()).total * c.n();
@@ -142,17 +145,18 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
     cudaMemcpy(plan->d_pairs, pairs.data(), pairs.size() * sizeof(PairDesc), cudaMemcpyHostToDevice);
     cudaMemcpy(plan->d_jobs, all.data(), total * sizeof(uint2), cudaMemcpyHostToDevice);
     plan->nops = (uint32_t)ops.size();
+    plan->ops = ops;
     return plan;
 }
 
-cudaError_t launch(const Plan& p, cudaStream_t s) {
+cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask) {
     switch (p.logn) {
-        case 11: Launcher<11>::launch(p, s); break;
-        case 12: Launcher<12>::launch(p, s); break;
-        case 13: Launcher<13>::launch(p, s); break;
-        case 14: Launcher<14>::launch(p, s); break;
-        case 15: Launcher<15>::launch(p, s); break;
-        case 16: Launcher<16>::launch(p, s); break;
+        case 11: Launcher<11>::launch(p, s, mask); break;
+        case 12: Launcher<12>::launch(p, s, mask); break;
+        case 13: Launcher<13>::launch(p, s, mask); break;
+        case 14: Launcher<14>::launch(p, s, mask); break;
+        case 15: Launcher<15>::launch(p, s, mask); break;
+        case 16: Launcher<16>::launch(p, s, mask); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

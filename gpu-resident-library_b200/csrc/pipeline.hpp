@@ -28,6 +28,7 @@ struct Plan {
     u64* ws = nullptr;
     size_t ws_words = 0;
     bool own_ws = false;
+    std::vector<Op> ops;      // host copy (device pointers and levels)
     ~Plan();
 };
 
@@ -36,6 +37,9 @@ size_t op_workspace_words(const gfx::Context& c, uint32_t L);
 void validate(const gfx::Context& c, const Op& op);
 // ws == nullptr: the plan allocates (and owns) its workspace.
 std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words);
-cudaError_t launch(const Plan& p, cudaStream_t s);
+// mask selects phases K1..K7 (bit k = phase k+1); 0x7f runs the whole batch.
+cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x7f);
+int input_count(uint32_t mode);
+uint32_t output_towers(const Op& op);
 
 }  // namespace pl

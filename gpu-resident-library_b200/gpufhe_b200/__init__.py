@@ -51,6 +51,12 @@ _API: dict = {
     "gpufhe_plan_launch": (I32, [VP, VP]),
     "gpufhe_plan_destroy": (None, [VP]),
     "gpufhe_run_ops": (I32, [VP, U32, VP, VP]),
+    "gpufhe_plan_launch_phase": (I32, [VP, U32, VP]),
+    "gpufhe_plan_kernel_count": (U32, [VP]),
+    "gpufhe_plan_launch_host": (I32, [VP, VP, VP, VP]),
+    "gpufhe_native_primes": (I32, [VP, U32, U32, U32, VP, U32]),
+    "gpufhe_native_root": (U64, [U32, U64]),
+    "gpufhe_rescale_consts": (I32, [VP, VP, VP, U32]),
 }
 
 EVALMULT_RESCALE, KEYSWITCH, ROTATE, RESCALE = 0, 1, 2, 3
@@ -173,6 +179,18 @@ class Plan:
     def launch(self, stream=None):
         check(lib().gpufhe_plan_launch(self.h, stream))
 
+    def launch_phase(self, phase, stream=None):
+        check(lib().gpufhe_plan_launch_phase(self.h, phase, stream))
+
+    def kernel_count(self):
+        return int(lib().gpufhe_plan_kernel_count(self.h))
+
+    def launch_host(self, h_in, h_out, stream=None):
+        """h_in: list of 4 host pointers per op (0 for unused); h_out: 2 per op."""
+        ai = (VP * len(h_in))(*h_in)
+        ao = (VP * len(h_out))(*h_out)
+        check(lib().gpufhe_plan_launch_host(self.h, ai, ao, stream))
+
     def close(self):
         if getattr(self, "h", None):
             lib().gpufhe_plan_destroy(self.h)
@@ -188,3 +206,15 @@ class Plan:
 def run_ops(ctx, specs, stream=None):
     ops, n = make_ops(specs)
     check(lib().gpufhe_run_ops(ctx.h, n, C.cast(ops, VP), stream))
+
+
+def native_primes(count, bits, n, avoid=()):
+    import numpy as np
+    out = np.zeros(count, np.uint64)
+    av = np.ascontiguousarray(list(avoid), np.uint64)
+    check(lib().gpufhe_native_primes(out.ctypes.data, count, bits, n, av.ctypes.data if len(av) else None, len(av)))
+    return out
+
+
+def native_root(n, q):
+    return int(lib().gpufhe_native_root(n, int(q)))

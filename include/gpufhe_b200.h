@@ -50,6 +50,14 @@ int  gpufhe_ctx_roots(const gpufhe_ctx* ctx, uint64_t* roots_qp);
 int  gpufhe_ctx_set_key(gpufhe_ctx* ctx, uint64_t key_id, const uint64_t* av, const uint64_t* bv);
 uint64_t gpufhe_ctx_resident_bytes(const gpufhe_ctx* ctx);
 
+/* ---------------------------------------------------------------- parameters
+ * C forms of the reference's native parameter routines (include/params.h;
+ * reference src/params.cpp:29-75). */
+int      gpufhe_native_primes(uint64_t* out, uint32_t count, uint32_t bits, uint32_t n, const uint64_t* avoid,
+                              uint32_t navoid);
+uint64_t gpufhe_native_root(uint32_t n, uint64_t q);
+int      gpufhe_rescale_consts(uint64_t* s1, uint64_t* s2, const uint64_t* mod, uint32_t last);
+
 /* ---------------------------------------------------------------- transforms
  * Batched forward/inverse NTT of npolys x towers tower-polys stored
  * contiguously ([poly][tower][n]); tower t uses modulus first_tower + t in
@@ -103,6 +111,16 @@ int  gpufhe_plan_create(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, ui
  * (kernel launches only: capturable in a CUDA graph). */
 int  gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t stream);
 void gpufhe_plan_destroy(gpufhe_plan* plan);
+/* One phase (0..6 = K1..K7) only, for per-kernel timing. */
+int  gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t stream);
+/* Number of kernels one gpufhe_plan_launch enqueues. */
+uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
+/* Host-buffer form: copies h_in[4*i+k] (host, level*n words) into op i's
+ * device inputs, launches the batch and copies each op's outputs back into
+ * h_out[2*i+k]; synchronizes `stream`. NULL entries are skipped. Pinned host
+ * memory gives full PCIe bandwidth. */
+int  gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
+                             cudaStream_t stream);
 /* create + launch + synchronize + destroy */
 int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaStream_t stream);
 
