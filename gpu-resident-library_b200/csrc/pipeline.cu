@@ -146,7 +146,36 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
     cudaMemcpy(plan->d_jobs, all.data(), total * sizeof(uint2), cudaMemcpyHostToDevice);
     plan->nops = (uint32_t)ops.size();
     plan->ops = ops;
+    plan->pairs_host = pairs;
     return plan;
+}
+
+namespace {
+__global__ void k_set_pair(PairDesc* dst, PairDesc v) { *dst = v; }
+}  // namespace
+
+void rebind(Plan& p, uint32_t idx, const Op& op, const gfx::Context& c, cudaStream_t s) {
+    if (idx >= p.pairs_host.size()) throw std::invalid_argument("rebind: index");
+    validate(c, op);
+    const Op& old = p.ops[idx];
+    const bool same_shape = old.L == op.L && (old.mode == op.mode ||
+                            ((old.mode == KS || old.mode == ROT) && (op.mode == KS || op.mode == ROT)));
+    if (!same_shape) throw std::invalid_argument("rebind: level or job shape differs");
+    PairDesc P = p.pairs_host[idx];
+    P.mode = op.mode;
+    P.galois = op.galois;
+    for (int k = 0; k < 4; ++k) P.in[k] = op.in[k];
+    P.out[0] = op.out[0];
+    P.out[1] = op.out[1];
+    if (op.mode != RESCALE) {
+        const gfx::Key* key = c.key(op.key_id);
+        if (!key) throw std::invalid_argument("missing eval key");
+        P.kav = key->av;
+        P.kbv = key->bv;
+    }
+    p.pairs_host[idx] = P;
+    p.ops[idx] = op;
+    k_set_pair<<<1, 1, 0, s>>>(p.d_pairs + idx, P);
 }
 
 cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask) {

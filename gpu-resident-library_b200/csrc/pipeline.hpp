@@ -29,6 +29,7 @@ struct Plan {
     size_t ws_words = 0;
     bool own_ws = false;
     std::vector<Op> ops;      // host copy (device pointers and levels)
+    std::vector<PairDesc> pairs_host;
     ~Plan();
 };
 
@@ -40,6 +41,12 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
 // mask selects phases K1..K7 (bit k = phase k+1); 0x7f runs the whole batch.
 cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x7f);
 int input_count(uint32_t mode);
+// Rebinds operation `idx` of a built plan to new buffers / mode (same level
+// and job shape) by a one-thread kernel on `s`: no allocation and no host
+// transfer, so it can be recorded in a CUDA graph together with launch().
+// KS and ROT plans share one job shape, so a keyswitch plan also serves
+// rotations at the same level.
+void rebind(Plan& p, uint32_t idx, const Op& op, const gfx::Context& c, cudaStream_t s);
 uint32_t output_towers(const Op& op);
 
 }  // namespace pl

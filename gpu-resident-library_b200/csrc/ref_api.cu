@@ -1,0 +1,655 @@
+// The reference's C++ API (namespace gpufhe) on this library's kernels:
+// DeviceCiphertext, DeviceTables / mul_resident / rescale_resident,
+// KeySwitchConstants / compute_keyswitch_constants / keyswitch_core_resident,
+// DeviceKSContext / DeviceKSWork / keyswitch_resident / rescale_resident_raw,
+// rotation, and the host keygen / evalkeygen / encrypt / decrypt harness.
+// Same names, arguments, results and error behaviour (std::runtime_error on
+// CUDA failures and unknown moduli) as the reference headers they replace.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "ckks_ops.h"
+#include "context.hpp"
+#include "device_ciphertext.h"
+#include "hostmath.hpp"
+#include "keygen.h"
+#include "keyswitch.h"
+#include "keyswitch_resident.h"
+#include "params.h"
+#include "pipeline.hpp"
+#include "rescale.h"
+#include "rns_arith.h"
+#include "xform.cuh"
+
+namespace {
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string("gpufhe: ") + what + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+T* dup_to_device(const std::vector<T>& h) {
+    T* d = nullptr;
+    ck(cudaMalloc(&d, std::max<size_t>(h.size(), 1) * sizeof(T)), "cudaMalloc");
+    ck(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy");
+    return d;
+}
+
+constexpr int MAXT = gfx::MAXQ;
+struct TowerMods { ModC m[MAXT]; };
+
+__global__ void k_mul_towers(u64* __restrict__ a0, u64* __restrict__ a1, const u64* __restrict__ b0,
+                             const u64* __restrict__ b1, TowerMods tm, uint32_t n) {
+    const uint32_t t = blockIdx.y;
+    const ModC m = tm.m[t];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const size_t x = (size_t)t * n + k;
+        a0[x] = mulmod(a0[x], b0[x], m);
+        a1[x] = mulmod(a1[x], b1[x], m);
+    }
+}
+
+// dst = SwitchModulus(src, q_old -> q_new) (switch_modulus.cu:11-42 semantics)
+__global__ void k_switch_copy(u64* __restrict__ dst, const u64* __restrict__ src, u64 half, u64 diff, int larger,
+                              ModC mnew, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const u64 x = src[i];
+        const u64 d = x > half ? diff : 0;
+        if (larger) { dst[i] = x + d; continue; }
+        const u64 xm = reduce64(x, mnew);
+        dst[i] = xm >= d ? xm - d : xm + mnew.q - d;
+    }
+}
+
+// out[j] = in[sigma slot] for one eval-form tower
+__global__ void k_galois_gather(u64* __restrict__ out, const u64* __restrict__ in, uint32_t logn, u64 k) {
+    const uint32_t n = 1u << logn;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t e = 2 * (__brev(j) >> (32 - logn)) + 1;
+        const uint32_t t = (uint32_t)(((u64)e * k) & (2ull * n - 1));
+        out[j] = in[__brev((t - 1) >> 1) >> (32 - logn)];
+    }
+}
+
+unsigned grid_for(uint32_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 4096); }
+
+// Switch-modulus values of one component's dropped tower into a survivor.
+void switch_params(u64 q_old, u64 q_new, u64& half, u64& diff, int& larger) {
+    half = q_old >> 1;
+    larger = q_new > q_old;
+    diff = larger ? q_new - q_old : (q_old - q_new) % q_new;
+}
+
+// Drops the last of `towers` towers of one eval-form component, tower by
+// tower through n-word scratch buffers (the reference's rescale contract).
+// fwd(t)/inv(t) give the transform job for modulus t.
+template <class FJ, class IJ>
+void rescale_component(u64* base, uint32_t towers, uint32_t n, const std::vector<u64>& q,
+                       const std::vector<u64>& s1, const std::vector<u64>& s2, u64* scratch, u64* drop,
+                       cudaStream_t s, FJ fwd, IJ inv) {
+    if (towers < 2) return;
+    const uint32_t last = towers - 1;
+    const int logn = hm::ilog2(n);
+    ck(cudaMemcpyAsync(drop, base + (size_t)last * n, (size_t)n * 8, cudaMemcpyDeviceToDevice, s), "copy");
+    xf::Job ji = inv(last);
+    ji.x = drop;
+    ck(xf_launch_ntt(nullptr, &ji, 1, logn, true, s), "intt");
+    for (uint32_t t = 0; t < last; ++t) {
+        u64 half, diff;
+        int larger;
+        switch_params(q[last], q[t], half, diff, larger);
+        k_switch_copy<<<grid_for(n), 256, 0, s>>>(scratch, drop, half, diff, larger, hm::modc(q[t]), n);
+        xf::Job jf = fwd(t);
+        jf.x = scratch;
+        ck(xf_launch_ntt(nullptr, &jf, 1, logn, false, s), "ntt");
+        LaunchRescaleFuse(base + (size_t)t * n, scratch, s1[t], s2[t], q[t], n, s);
+    }
+}
+
+// Process-wide cache of packed twiddle tables for host-orchestrated helpers.
+struct TabEntry { Tw* f; Tw* i; u64 ninv, ninvp; };
+std::mutex g_tab_mu;
+std::map<std::tuple<int, uint32_t, u64, u64>, TabEntry> g_tabs;
+
+TabEntry tables_for(uint32_t n, u64 q, u64 root) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(g_tab_mu);
+    auto key = std::make_tuple(dev, n, q, root);
+    auto it = g_tabs.find(key);
+    if (it != g_tabs.end()) return it->second;
+    std::vector<Tw> f, iv;
+    hm::twiddles(n, q, root, f, iv);
+    TabEntry e{dup_to_device(f), dup_to_device(iv), hm::invmod(n, q), 0};
+    e.ninvp = hm::precon(e.ninv, q);
+    g_tabs.emplace(key, e);
+    return e;
+}
+
+// Transforms every tower of a host [towers][n] array (tower t mod[t]).
+void host_xform(std::vector<u64>& h, uint32_t towers, uint32_t n, const std::vector<u64>& mod,
+                const std::vector<u64>& root, bool inverse) {
+    u64* d = dup_to_device(h);
+    std::vector<xf::Job> jobs(towers);
+    for (uint32_t t = 0; t < towers; ++t) {
+        TabEntry e = tables_for(n, mod[t], root[t]);
+        jobs[t] = xf::Job{d + (size_t)t * n, inverse ? e.i : e.f, nullptr, nullptr, mod[t], e.ninv, e.ninvp};
+    }
+    xf::Job* dj = dup_to_device(jobs);
+    ck(xf_launch_ntt(dj, nullptr, (int)towers, hm::ilog2(n), inverse, 0), "transform");
+    ck(cudaDeviceSynchronize(), "sync");
+    ck(cudaMemcpy(h.data(), d, h.size() * 8, cudaMemcpyDeviceToHost), "download");
+    cudaFree(dj);
+    cudaFree(d);
+}
+
+inline u64 emb(long v, u64 q) { return (u64)((v % (long)q + (long)q) % (long)q); }
+uint32_t g_hw = 0;
+
+struct WorkImpl {
+    std::unique_ptr<pl::Plan> plan;
+    gfx::Context* ctx = nullptr;
+};
+
+}  // namespace
+
+namespace gpufhe {
+
+// ---------------------------------------------------------------- DeviceCiphertext
+DeviceCiphertext::DeviceCiphertext(Scheme scheme, uint32_t n, uint32_t num_towers)
+    : scheme_(scheme), n_(n), towers_(num_towers) {
+    const size_t bytes = (size_t)n_ * towers_ * sizeof(uint64_t);
+    ck(cudaMalloc(&d_c0_, bytes), "DeviceCiphertext: cudaMalloc c0");
+    cudaError_t e = cudaMalloc(&d_c1_, bytes);
+    if (e != cudaSuccess) { cudaFree(d_c0_); d_c0_ = nullptr; ck(e, "DeviceCiphertext: cudaMalloc c1"); }
+}
+DeviceCiphertext::~DeviceCiphertext() {
+    if (d_c0_) cudaFree(d_c0_);
+    if (d_c1_) cudaFree(d_c1_);
+}
+DeviceCiphertext::DeviceCiphertext(DeviceCiphertext&& o) noexcept
+    : scheme_(o.scheme_), format_(o.format_), n_(o.n_), towers_(o.towers_), d_c0_(o.d_c0_), d_c1_(o.d_c1_) {
+    o.d_c0_ = o.d_c1_ = nullptr;
+}
+DeviceCiphertext& DeviceCiphertext::operator=(DeviceCiphertext&& o) noexcept {
+    if (this != &o) {
+        if (d_c0_) cudaFree(d_c0_);
+        if (d_c1_) cudaFree(d_c1_);
+        scheme_ = o.scheme_; format_ = o.format_; n_ = o.n_; towers_ = o.towers_;
+        d_c0_ = o.d_c0_; d_c1_ = o.d_c1_;
+        o.d_c0_ = o.d_c1_ = nullptr;
+    }
+    return *this;
+}
+void DeviceCiphertext::upload(const std::vector<uint64_t>& c0, const std::vector<uint64_t>& c1) {
+    const size_t need = (size_t)n_ * towers_;
+    if (c0.size() != need || c1.size() != need) throw std::runtime_error("DeviceCiphertext::upload size mismatch");
+    ck(cudaMemcpy(d_c0_, c0.data(), need * 8, cudaMemcpyHostToDevice), "DeviceCiphertext: upload c0");
+    ck(cudaMemcpy(d_c1_, c1.data(), need * 8, cudaMemcpyHostToDevice), "DeviceCiphertext: upload c1");
+}
+void DeviceCiphertext::to_host(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1) const {
+    const size_t need = (size_t)n_ * towers_;
+    c0.resize(need);
+    c1.resize(need);
+    ck(cudaMemcpy(c0.data(), d_c0_, need * 8, cudaMemcpyDeviceToHost), "DeviceCiphertext: to_host c0");
+    ck(cudaMemcpy(c1.data(), d_c1_, need * 8, cudaMemcpyDeviceToHost), "DeviceCiphertext: to_host c1");
+}
+
+// ---------------------------------------------------------------- DeviceTables
+void build_device_tables(DeviceTables& T, uint32_t n, const std::vector<uint64_t>& moduli) {
+    T.n = n;
+    T.q = moduli;
+    const uint32_t towers = (uint32_t)moduli.size();
+    T.d_froots.assign(towers, nullptr); T.d_fprecon.assign(towers, nullptr);
+    T.d_iroots.assign(towers, nullptr); T.d_iprecon.assign(towers, nullptr);
+    T.ninv.resize(towers); T.ninv_precon.resize(towers);
+    for (uint32_t t = 0; t < towers; ++t) {
+        const u64 q = moduli[t];
+        const u64 root = native_root(n, q);   // smallest-generator root, as ckks_ops.cpp:25-38
+        std::vector<Tw> f, iv;
+        hm::twiddles(n, q, root, f, iv);
+        std::vector<u64> fr(n), fp(n), ir(n), ip(n);
+        for (uint32_t i = 0; i < n; ++i) { fr[i] = f[i].w; fp[i] = f[i].wp; ir[i] = iv[i].w; ip[i] = iv[i].wp; }
+        T.d_froots[t] = dup_to_device(fr); T.d_fprecon[t] = dup_to_device(fp);
+        T.d_iroots[t] = dup_to_device(ir); T.d_iprecon[t] = dup_to_device(ip);
+        T.ninv[t] = hm::invmod(n, q);
+        T.ninv_precon[t] = hm::precon(T.ninv[t], q);
+    }
+}
+
+DeviceTables::~DeviceTables() {
+    for (auto* v : {&d_froots, &d_fprecon, &d_iroots, &d_iprecon})
+        for (auto p : *v) if (p) cudaFree(p);
+}
+
+void mul_resident(DeviceCiphertext& a, const DeviceCiphertext& b, const DeviceTables& T, cudaStream_t stream) {
+    const uint32_t n = a.n(), towers = a.num_towers();
+    if (!towers) return;
+    for (uint32_t t0 = 0; t0 < towers; t0 += MAXT) {
+        const uint32_t cnt = std::min<uint32_t>(MAXT, towers - t0);
+        TowerMods tm;
+        for (uint32_t t = 0; t < cnt; ++t) tm.m[t] = hm::modc(T.q[t0 + t]);
+        dim3 g(std::max(1u, std::min(grid_for(n), 64u)), cnt);
+        DeviceCiphertext& bb = const_cast<DeviceCiphertext&>(b);
+        k_mul_towers<<<g, 256, 0, stream>>>(a.c0() + (size_t)t0 * n, a.c1() + (size_t)t0 * n,
+                                            bb.c0() + (size_t)t0 * n, bb.c1() + (size_t)t0 * n, tm, n);
+    }
+}
+
+void rescale_resident(DeviceCiphertext& ct, const DeviceTables& T, const std::vector<uint64_t>& s1,
+                      const std::vector<uint64_t>& s2, cudaStream_t stream, uint64_t* scratch, uint64_t* dropCoeff) {
+    const uint32_t n = ct.n(), towers = ct.num_towers();
+    if (towers < 2) return;
+    auto fwd = [&](uint32_t t) { return xf::Job{nullptr, nullptr, T.d_froots[t], T.d_fprecon[t], T.q[t], 0, 0}; };
+    auto inv = [&](uint32_t t) {
+        return xf::Job{nullptr, nullptr, T.d_iroots[t], T.d_iprecon[t], T.q[t], T.ninv[t], T.ninv_precon[t]};
+    };
+    rescale_component(ct.c0(), towers, n, T.q, s1, s2, scratch, dropCoeff, stream, fwd, inv);
+    rescale_component(ct.c1(), towers, n, T.q, s1, s2, scratch, dropCoeff, stream, fwd, inv);
+    ct.drop_tower();
+}
+
+// ---------------------------------------------------------------- constants
+void compute_keyswitch_constants(KeySwitchConstants& K, const std::vector<uint64_t>& moduliQ,
+                                 const std::vector<uint64_t>& moduliP, uint32_t numPart) {
+    const uint32_t sizeQ = (uint32_t)moduliQ.size(), sizeP = (uint32_t)moduliP.size();
+    if (!numPart) throw std::invalid_argument("numPart must be >= 1");
+    const uint32_t alpha = (uint32_t)std::ceil((double)sizeQ / numPart);
+    K.sizeQl = sizeQ; K.sizeP = sizeP; K.numPart = numPart; K.alpha = alpha; K.fullQ = sizeQ;
+    K.qMod = moduliQ; K.pMod = moduliP;
+    K.pInvModq.resize(sizeQ);
+    for (uint32_t i = 0; i < sizeQ; ++i)
+        K.pInvModq[i] = hm::invmod(hm::prod_mod(moduliP.data(), sizeP, moduliQ[i]), moduliQ[i]);
+    K.pHatInv.resize(sizeP); K.pHatInvPrec.resize(sizeP); K.pHatModq.resize((size_t)sizeP * sizeQ);
+    for (uint32_t j = 0; j < sizeP; ++j) {
+        const u64 pj = moduliP[j];
+        K.pHatInv[j] = hm::invmod(hm::prod_mod(moduliP.data(), sizeP, pj, (int)j), pj);
+        K.pHatInvPrec[j] = hm::precon(K.pHatInv[j], pj);
+        for (uint32_t i = 0; i < sizeQ; ++i)
+            K.pHatModq[(size_t)j * sizeQ + i] = hm::prod_mod(moduliP.data(), sizeP, moduliQ[i], (int)j);
+    }
+    K.mdBMuLo.resize(sizeQ); K.mdBMuHi.resize(sizeQ);
+    for (uint32_t i = 0; i < sizeQ; ++i) {
+        const ModC m = hm::modc(moduliQ[i]);
+        K.mdBMuLo[i] = m.mu_lo; K.mdBMuHi[i] = m.mu_hi;
+    }
+    for (auto* v : {&K.partQHatInv, &K.partQHatInvPrec, &K.partSrcMod, &K.partQHatModp, &K.partComplMod,
+                    &K.partBMuLo, &K.partBMuHi}) v->assign(numPart, {});
+    K.sizePart.resize(numPart); K.sizeCompl.resize(numPart); K.startIdx.resize(numPart);
+    for (uint32_t part = 0; part < numPart; ++part) {
+        const uint32_t st = alpha * part;
+        const uint32_t sp = (sizeQ > st + alpha) ? alpha : (sizeQ > st ? sizeQ - st : 0);
+        K.startIdx[part] = st; K.sizePart[part] = sp;
+        std::vector<u64> src(moduliQ.begin() + st, moduliQ.begin() + st + sp);
+        K.partSrcMod[part] = src;
+        K.partQHatInv[part].resize(sp); K.partQHatInvPrec[part].resize(sp);
+        for (uint32_t i = 0; i < sp; ++i) {
+            K.partQHatInv[part][i] = hm::invmod(hm::prod_mod(src.data(), sp, src[i], (int)i), src[i]);
+            K.partQHatInvPrec[part][i] = hm::precon(K.partQHatInv[part][i], src[i]);
+        }
+        std::vector<u64> compl_;
+        for (uint32_t i = 0; i < sizeQ; ++i) if (i < st || i >= st + sp) compl_.push_back(moduliQ[i]);
+        for (uint32_t j = 0; j < sizeP; ++j) compl_.push_back(moduliP[j]);
+        const uint32_t sc = (uint32_t)compl_.size();
+        K.sizeCompl[part] = sc; K.partComplMod[part] = compl_;
+        K.partQHatModp[part].resize((size_t)sp * sc);
+        for (uint32_t i = 0; i < sp; ++i)
+            for (uint32_t j = 0; j < sc; ++j)
+                K.partQHatModp[part][(size_t)i * sc + j] = hm::prod_mod(src.data(), sp, compl_[j], (int)i);
+        K.partBMuLo[part].resize(sc); K.partBMuHi[part].resize(sc);
+        for (uint32_t j = 0; j < sc; ++j) {
+            const ModC m = hm::modc(compl_[j]);
+            K.partBMuLo[part][j] = m.mu_lo; K.partBMuHi[part][j] = m.mu_hi;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- resident keyswitch
+DeviceKSContext ks_context_create(const KeySwitchConstants& K) {
+    DeviceKSContext C;
+    C.n = K.n; C.sizeQl = K.sizeQl; C.sizeP = K.sizeP; C.sizeQlP = K.sizeQl + K.sizeP;
+    C.numPart = K.numPart; C.fullQ = K.fullQ ? K.fullQ : K.sizeQl;
+    C.sizePart = K.sizePart; C.sizeCompl = K.sizeCompl; C.startIdx = K.startIdx;
+    C.qModHost = K.qMod; C.pModHost = K.pMod; C.pInvModqHost = K.pInvModq;
+    std::vector<u64> roots;
+    auto root_of = [&](u64 q) {
+        for (size_t r = 0; r < K.rootModList.size(); ++r) if (K.rootModList[r] == q) return K.rootValList[r];
+        throw std::runtime_error("no root table for modulus");
+    };
+    for (u64 q : K.qMod) { roots.push_back(root_of(q)); C.modList.push_back(q); }
+    for (u64 p : K.pMod) { roots.push_back(root_of(p)); C.modList.push_back(p); }
+    const uint32_t alpha = K.alpha ? K.alpha : (K.sizeQl + K.numPart - 1) / K.numPart;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    auto* ctx = new gfx::Context(K.n, K.qMod, K.pMod, alpha, roots, dev);
+    C.impl = ctx;
+    if (!K.av.empty()) {
+        // repack the full-QP key rows for this level into [dnum][sizeQl+sizeP][n]
+        const uint32_t dnum = ctx->dnum(), QlP = C.sizeQlP, n = K.n;
+        if (K.av.size() < dnum || K.bv.size() < dnum) {
+            delete ctx;
+            throw std::runtime_error("eval key has fewer digits than the partition");
+        }
+        const uint32_t delta = C.fullQ - K.sizeQl;
+        std::vector<u64> av((size_t)dnum * QlP * n), bv(av.size());
+        for (uint32_t p = 0; p < dnum; ++p)
+            for (uint32_t i = 0; i < QlP; ++i) {
+                const uint32_t row = i >= K.sizeQl ? i + delta : i;
+                std::memcpy(&av[((size_t)p * QlP + i) * n], &K.av[p][(size_t)row * n], (size_t)n * 8);
+                std::memcpy(&bv[((size_t)p * QlP + i) * n], &K.bv[p][(size_t)row * n], (size_t)n * 8);
+            }
+        ctx->set_key(0, av.data(), bv.data());
+    }
+    return C;
+}
+
+void ks_context_destroy(DeviceKSContext& C) {
+    delete static_cast<gfx::Context*>(C.impl);
+    C.impl = nullptr;
+}
+
+DeviceKSWork ks_work_create(const DeviceKSContext& C) {
+    auto* ctx = static_cast<gfx::Context*>(C.impl);
+    if (!ctx) throw std::runtime_error("ks_work_create: empty context");
+    DeviceKSWork W;
+    const uint32_t L = C.sizeQl;
+    const size_t words = pl::op_workspace_words(*ctx, L);
+    ck(cudaMalloc(&W.d_ws, words * 8), "ks_work_create: workspace");
+    auto* wi = new WorkImpl();
+    wi->ctx = ctx;
+    if (ctx->key(0)) {
+        pl::Op op;
+        op.L = L;
+        op.mode = pl::KS;
+        static u64 dummy[2];
+        op.in[0] = dummy;   // rebound on every call
+        op.out[0] = op.out[1] = dummy;
+        wi->plan = pl::build_plan(*ctx, {op}, W.d_ws, words);
+    }
+    W.impl = wi;
+    return W;
+}
+
+void ks_work_destroy(DeviceKSWork& W) {
+    delete static_cast<WorkImpl*>(W.impl);
+    W.impl = nullptr;
+    if (W.d_ws) cudaFree(W.d_ws);
+    W.d_ws = nullptr;
+}
+
+void keyswitch_resident(const uint64_t* d_a, uint64_t* d_ba0, uint64_t* d_ba1, const DeviceKSContext& C,
+                        DeviceKSWork& W, cudaStream_t s) {
+    auto* wi = static_cast<WorkImpl*>(W.impl);
+    if (!wi || !wi->plan) throw std::runtime_error("keyswitch_resident: context has no eval key");
+    pl::Op op;
+    op.L = C.sizeQl;
+    op.mode = pl::KS;
+    op.in[0] = d_a;
+    op.out[0] = d_ba0;
+    op.out[1] = d_ba1;
+    pl::rebind(*wi->plan, 0, op, *wi->ctx, s);
+    ck(pl::launch(*wi->plan, s), "keyswitch_resident");
+}
+
+void rescale_resident_raw(uint64_t* d_c, uint32_t towers, const DeviceKSContext& C, const std::vector<uint64_t>& s1,
+                          const std::vector<uint64_t>& s2, uint64_t* d_scratch, uint64_t* d_drop, cudaStream_t s) {
+    auto* ctx = static_cast<gfx::Context*>(C.impl);
+    if (!ctx) throw std::runtime_error("rescale_resident_raw: empty context");
+    if (towers < 2) return;
+    if (towers > ctx->fullQ()) throw std::runtime_error("rescale_resident_raw: more towers than the context");
+    const auto& D = ctx->dev();
+    const uint32_t n = C.n;
+    std::vector<u64> ninv(towers), ninvp(towers);
+    ck(cudaMemcpy(ninv.data(), D.ninv, towers * 8, cudaMemcpyDeviceToHost), "ninv");
+    ck(cudaMemcpy(ninvp.data(), D.ninvp, towers * 8, cudaMemcpyDeviceToHost), "ninvp");
+    const std::vector<u64>& q = ctx->Q();
+    auto fwd = [&](uint32_t t) { return xf::Job{nullptr, D.twf + (size_t)t * n, nullptr, nullptr, q[t], 0, 0}; };
+    auto inv = [&](uint32_t t) { return xf::Job{nullptr, D.twi + (size_t)t * n, nullptr, nullptr, q[t], ninv[t], ninvp[t]}; };
+    rescale_component(d_c, towers, n, q, s1, s2, d_scratch, d_drop, s, fwd, inv);
+}
+
+KeySwitchResult keyswitch_core_resident(const std::vector<uint64_t>& aTowers, const KeySwitchConstants& K) {
+    DeviceKSContext C = ks_context_create(K);
+    DeviceKSWork W = ks_work_create(C);
+    const size_t T = (size_t)K.sizeQl * K.n;
+    u64* da = dup_to_device(aTowers);
+    u64 *d0 = nullptr, *d1 = nullptr;
+    ck(cudaMalloc(&d0, T * 8), "cudaMalloc");
+    ck(cudaMalloc(&d1, T * 8), "cudaMalloc");
+    keyswitch_resident(da, d0, d1, C, W, 0);
+    ck(cudaDeviceSynchronize(), "keyswitch");
+    KeySwitchResult R;
+    R.ba0.resize(T);
+    R.ba1.resize(T);
+    ck(cudaMemcpy(R.ba0.data(), d0, T * 8, cudaMemcpyDeviceToHost), "download");
+    ck(cudaMemcpy(R.ba1.data(), d1, T * 8, cudaMemcpyDeviceToHost), "download");
+    cudaFree(da); cudaFree(d0); cudaFree(d1);
+    ks_work_destroy(W);
+    ks_context_destroy(C);
+    return R;
+}
+
+// ---------------------------------------------------------------- rotation
+void automorphism_eval_device(uint64_t* d_v, uint32_t towers, uint32_t n, uint32_t k, const std::vector<uint64_t>&,
+                              const std::vector<uint64_t>&, uint64_t* d_scratch, cudaStream_t s) {
+    const uint32_t logn = (uint32_t)hm::ilog2(n);
+    for (uint32_t t = 0; t < towers; ++t) {
+        uint64_t* col = d_v + (size_t)t * n;
+        k_galois_gather<<<grid_for(n), 256, 0, s>>>(d_scratch, col, logn, k);
+        ck(cudaMemcpyAsync(col, d_scratch, (size_t)n * 8, cudaMemcpyDeviceToDevice, s), "automorphism copy");
+    }
+}
+
+void rotate_ct_device(uint64_t* d_c0, uint64_t* d_c1, uint32_t k, const DeviceKSContext& C, DeviceKSWork& W,
+                      uint32_t towers, uint32_t n, const std::vector<uint64_t>&, const std::vector<uint64_t>&,
+                      uint64_t*, uint64_t* d_b0, uint64_t* d_b1, cudaStream_t s) {
+    auto* wi = static_cast<WorkImpl*>(W.impl);
+    if (!wi || !wi->plan) throw std::runtime_error("rotate_ct_device: context has no rotation key");
+    if (towers != C.sizeQl) throw std::runtime_error("rotate_ct_device: tower count differs from the context");
+    pl::Op op;
+    op.L = towers;
+    op.mode = pl::ROT;
+    op.galois = k;
+    op.in[0] = d_c0;
+    op.in[1] = d_c1;
+    op.out[0] = d_b0;
+    op.out[1] = d_b1;
+    pl::rebind(*wi->plan, 0, op, *wi->ctx, s);
+    ck(pl::launch(*wi->plan, s), "rotate_ct_device");
+    const size_t bytes = (size_t)towers * n * 8;
+    ck(cudaMemcpyAsync(d_c0, d_b0, bytes, cudaMemcpyDeviceToDevice, s), "rotate copy");
+    ck(cudaMemcpyAsync(d_c1, d_b1, bytes, cudaMemcpyDeviceToDevice, s), "rotate copy");
+}
+
+void rotate_ct_resident(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, uint32_t k,
+                        const KeySwitchConstants& Krot, uint32_t towers, uint32_t n, const std::vector<uint64_t>& mod,
+                        const std::vector<uint64_t>& root) {
+    DeviceKSContext C = ks_context_create(Krot);
+    DeviceKSWork W = ks_work_create(C);
+    const size_t T = (size_t)towers * n;
+    u64 *d0 = dup_to_device(c0), *d1 = dup_to_device(c1), *b0 = nullptr, *b1 = nullptr;
+    ck(cudaMalloc(&b0, T * 8), "cudaMalloc");
+    ck(cudaMalloc(&b1, T * 8), "cudaMalloc");
+    rotate_ct_device(d0, d1, k, C, W, towers, n, mod, root, nullptr, b0, b1, 0);
+    ck(cudaDeviceSynchronize(), "rotate");
+    ck(cudaMemcpy(c0.data(), d0, T * 8, cudaMemcpyDeviceToHost), "download");
+    ck(cudaMemcpy(c1.data(), d1, T * 8, cudaMemcpyDeviceToHost), "download");
+    cudaFree(d0); cudaFree(d1); cudaFree(b0); cudaFree(b1);
+    ks_work_destroy(W);
+    ks_context_destroy(C);
+}
+
+// ---------------------------------------------------------------- host harness
+void set_secret_hamming_weight(uint32_t h) { g_hw = h; }
+
+KeyPairHost keygen_host(uint32_t n, const std::vector<uint64_t>& moduli, const std::vector<uint64_t>& roots,
+                        uint64_t ns, double sigma, uint64_t seed) {
+    const uint32_t sizeQ = (uint32_t)moduli.size();
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<double> gauss(0.0, sigma);
+    std::vector<int> sc(n), ec(n);
+    if (g_hw == 0) {
+        for (uint32_t k = 0; k < n; ++k) sc[k] = (int)(rng() % 3) - 1;
+    } else {
+        std::vector<uint32_t> idx(n);
+        for (uint32_t k = 0; k < n; ++k) idx[k] = k;
+        for (uint32_t k = n - 1; k > 0; --k) { uint32_t j = (uint32_t)(rng() % (k + 1)); std::swap(idx[k], idx[j]); }
+        const uint32_t h = g_hw < n ? g_hw : n;
+        for (uint32_t k = 0; k < h; ++k) sc[idx[k]] = (rng() & 1ull) ? 1 : -1;
+    }
+    for (uint32_t k = 0; k < n; ++k) ec[k] = (int)std::lround(gauss(rng));
+    KeyPairHost K;
+    const size_t T = (size_t)sizeQ * n;
+    K.s.resize(T); K.pkA.resize(T); K.pkB.resize(T);
+    std::vector<u64> eT(T);
+    for (uint32_t t = 0; t < sizeQ; ++t) {
+        const u64 q = moduli[t];
+        for (uint32_t k = 0; k < n; ++k) {
+            const size_t x = (size_t)t * n + k;
+            K.s[x] = emb(sc[k], q);
+            eT[x] = emb(ec[k], q);
+            K.pkA[x] = rng() % q;
+        }
+    }
+    host_xform(K.s, sizeQ, n, moduli, roots, false);
+    host_xform(eT, sizeQ, n, moduli, roots, false);
+    for (uint32_t t = 0; t < sizeQ; ++t) {
+        const u64 q = moduli[t];
+        for (uint32_t k = 0; k < n; ++k) {
+            const size_t x = (size_t)t * n + k;
+            const u64 as = hm::mulmod(K.pkA[x], K.s[x], q);
+            const u64 nse = hm::mulmod(ns % q, eT[x], q);
+            K.pkB[x] = nse >= as ? nse - as : nse + q - as;
+        }
+    }
+    return K;
+}
+
+void evalkeygen_host_sold(KeySwitchConstants& K, const std::vector<uint64_t>& /*sQP*/,
+                          const std::vector<uint64_t>& sOld, const std::vector<uint64_t>& pkA_QP,
+                          const std::vector<uint64_t>& pkB_QP, const std::vector<uint64_t>& PModq_QP,
+                          const std::vector<uint64_t>& modQP, const std::vector<uint64_t>& rootQP, uint64_t ns,
+                          double sigma, uint64_t seed) {
+    const uint32_t n = K.n, sizeQlP = (uint32_t)modQP.size();
+    const uint32_t sizeQl = K.sizeQl, alpha = K.alpha, numPart = K.numPart;
+    K.evalKeyTowers = sizeQlP;
+    K.av.assign(numPart, {});
+    K.bv.assign(numPart, {});
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<double> gauss(0.0, sigma);
+    const size_t T = (size_t)sizeQlP * n;
+    for (uint32_t part = 0; part < numPart; ++part) {
+        const uint32_t st = alpha * part;
+        const uint32_t sp = (sizeQl > st + alpha) ? alpha : (sizeQl - st);
+        const uint32_t en = st + sp;
+        std::vector<int> uc(n), e0c(n), e1c(n);
+        for (uint32_t k = 0; k < n; ++k) {
+            uc[k] = (int)(rng() % 3) - 1;
+            e0c[k] = (int)std::lround(gauss(rng));
+            e1c[k] = (int)std::lround(gauss(rng));
+        }
+        std::vector<u64> uT(T), e0T(T), e1T(T);
+        for (uint32_t t = 0; t < sizeQlP; ++t)
+            for (uint32_t k = 0; k < n; ++k) {
+                const size_t x = (size_t)t * n + k;
+                uT[x] = emb(uc[k], modQP[t]); e0T[x] = emb(e0c[k], modQP[t]); e1T[x] = emb(e1c[k], modQP[t]);
+            }
+        host_xform(uT, sizeQlP, n, modQP, rootQP, false);
+        host_xform(e0T, sizeQlP, n, modQP, rootQP, false);
+        host_xform(e1T, sizeQlP, n, modQP, rootQP, false);
+        K.av[part].resize(T);
+        K.bv[part].resize(T);
+        for (uint32_t t = 0; t < sizeQlP; ++t) {
+            const u64 q = modQP[t];
+            for (uint32_t k = 0; k < n; ++k) {
+                const size_t x = (size_t)t * n + k;
+                u64 a = hm::mulmod(pkA_QP[x], uT[x], q) + hm::mulmod(ns % q, e1T[x], q);
+                u64 b = hm::mulmod(pkB_QP[x], uT[x], q) + hm::mulmod(ns % q, e0T[x], q);
+                a = a >= q ? a - q : a;
+                b = b >= q ? b - q : b;
+                if (t >= st && t < en) {
+                    b += hm::mulmod(PModq_QP[t] % q, sOld[x], q);
+                    b = b >= q ? b - q : b;
+                }
+                K.av[part][x] = a;
+                K.bv[part][x] = b;
+            }
+        }
+    }
+}
+
+void evalkeygen_host(KeySwitchConstants& K, const std::vector<uint64_t>& sQP, const std::vector<uint64_t>& pkA_QP,
+                     const std::vector<uint64_t>& pkB_QP, const std::vector<uint64_t>& PModq_QP,
+                     const std::vector<uint64_t>& modQP, const std::vector<uint64_t>& rootQP, uint64_t ns,
+                     double sigma, uint64_t seed) {
+    const uint32_t n = K.n, sizeQlP = (uint32_t)modQP.size();
+    std::vector<u64> s2(sQP.size());
+    for (uint32_t t = 0; t < sizeQlP; ++t)
+        for (uint32_t k = 0; k < n; ++k) {
+            const size_t x = (size_t)t * n + k;
+            s2[x] = hm::mulmod(sQP[x], sQP[x], modQP[t]);
+        }
+    evalkeygen_host_sold(K, sQP, s2, pkA_QP, pkB_QP, PModq_QP, modQP, rootQP, ns, sigma, seed);
+}
+
+void encrypt_host(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, const std::vector<int64_t>& m,
+                  const std::vector<uint64_t>& pkA, const std::vector<uint64_t>& pkB, uint32_t n,
+                  const std::vector<uint64_t>& mod, const std::vector<uint64_t>& root, uint64_t ns, double sigma,
+                  uint64_t seed) {
+    const uint32_t sizeQ = (uint32_t)mod.size();
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<double> g(0.0, sigma);
+    std::vector<int> vc(n), e0c(n), e1c(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        vc[k] = (int)(rng() % 3) - 1;
+        e0c[k] = (int)std::lround(g(rng));
+        e1c[k] = (int)std::lround(g(rng));
+    }
+    const size_t T = (size_t)sizeQ * n;
+    std::vector<u64> vT(T), e0T(T), e1T(T), mT(T);
+    for (uint32_t t = 0; t < sizeQ; ++t)
+        for (uint32_t k = 0; k < n; ++k) {
+            const size_t x = (size_t)t * n + k;
+            const u64 q = mod[t];
+            vT[x] = emb(vc[k], q); e0T[x] = emb(e0c[k], q); e1T[x] = emb(e1c[k], q); mT[x] = emb((long)m[k], q);
+        }
+    for (auto* v : {&vT, &e0T, &e1T, &mT}) host_xform(*v, sizeQ, n, mod, root, false);
+    c0.resize(T);
+    c1.resize(T);
+    for (uint32_t t = 0; t < sizeQ; ++t) {
+        const u64 q = mod[t];
+        for (uint32_t k = 0; k < n; ++k) {
+            const size_t x = (size_t)t * n + k;
+            u64 b = hm::mulmod(pkB[x], vT[x], q) + hm::mulmod(ns % q, e0T[x], q);
+            b = b >= q ? b - q : b;
+            u64 a = hm::mulmod(pkA[x], vT[x], q) + hm::mulmod(ns % q, e1T[x], q);
+            a = a >= q ? a - q : a;
+            b += mT[x];
+            c0[x] = b >= q ? b - q : b;
+            c1[x] = a;
+        }
+    }
+}
+
+void decrypt_host(std::vector<int64_t>& mout, const std::vector<uint64_t>& c0, const std::vector<uint64_t>& c1,
+                  const std::vector<uint64_t>& s, uint32_t n, const std::vector<uint64_t>& mod,
+                  const std::vector<uint64_t>& root) {
+    const u64 q = mod[0];
+    std::vector<u64> ph(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        u64 v = c0[k] + hm::mulmod(c1[k], s[k], q);
+        ph[k] = v >= q ? v - q : v;
+    }
+    host_xform(ph, 1, n, {q}, {root[0]}, true);
+    mout.resize(n);
+    for (uint32_t k = 0; k < n; ++k) mout[k] = ph[k] > q / 2 ? (int64_t)ph[k] - (int64_t)q : (int64_t)ph[k];
+}
+
+}  // namespace gpufhe

@@ -46,6 +46,10 @@ static gpufhe::KeySwitchConstants level_consts(const RefH* h, uint32_t L, uint32
     gpufhe::compute_keyswitch_constants(C, q, h->P, numPart);
     for (uint32_t i = 0; i < L; ++i) { C.rootModList.push_back(h->Q[i]); C.rootValList.push_back(h->rQ[i]); }
     for (uint32_t j = 0; j < h->K; ++j) { C.rootModList.push_back(h->P[j]); C.rootValList.push_back(h->rP[j]); }
+    /* ks_context_create (keyswitch_resident.cpp:73-84) reads av/bv[part] for
+     * every part: give it empty per-part vectors until a key is attached. */
+    C.av.assign(C.numPart, {});
+    C.bv.assign(C.numPart, {});
     return C;
 }
 
