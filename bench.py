@@ -289,7 +289,7 @@ def run_gpu(args):
     # per-phase device times (outside the timed region)
     cur = torch.cuda.current_stream().cuda_stream
     phases = []
-    for k in range(7):
+    for k in range(9):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         for _ in range(3):
@@ -363,7 +363,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         pms = a.elapsed_time(b) / reps
         plain = {"value": PAIRS / (pms * 1e-3), "unit": "ops/s", "ms_per_step": pms,
-                 "form": "one pair per launch set (7 kernels), CUDA graph per chain, 16 streams"}
+                 "form": "one pair per launch set (9 kernels), CUDA graph per chain, 16 streams"}
         del pgraphs, pplans
 
     # config-2 NTT kernel isolation: 64 polys x 12 towers x 2^16
@@ -415,11 +415,11 @@ def run_gpu(args):
         "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues and key)",
         "config": {"workload": WORKLOAD, "n": n, "pairs_per_gpu": PAIRS, "levels": "U{4..12} seeded",
                    "mean_level": float(np.mean(levels)), "l2": "inputs larger than L2 (no flush)",
-                   "graph": "7 kernels per step, one CUDA graph"},
-        "roofline": {"bound": "hbm", "kernel": "fused EvalMult+Rescale step (K1..K7)", "achieved": achieved,
+                   "graph": f"{kernels_per_step} kernels per step, one CUDA graph"},
+        "roofline": {"bound": "hbm", "kernel": "fused EvalMult+Rescale step (phases P1..P9)", "achieved": achieved,
                      "peak": pk["hbm_gbs"], "peak_source": pk["source"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "algorithmic_bytes_per_launch": alg, "traffic": None},
-        "phases_ms": {f"K{k + 1}": p for k, p in enumerate(phases)},
+        "phases_ms": {f"P{k + 1}": p for k, p in enumerate(phases)},
         "e2e": {"value": e2e_value, "unit": "ops/s", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo,
                 "ms_per_step": e2e_ms},
         "plain": plain,

@@ -65,7 +65,7 @@ int gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t s) {
 }
 
 int gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t s) {
-    if (!plan || phase >= 7) { gfx::set_error("bad plan or phase"); return GPUFHE_EINVAL; }
+    if (!plan || phase >= (uint32_t)pl::NPHASE) { gfx::set_error("bad plan or phase"); return GPUFHE_EINVAL; }
     cudaError_t e = pl::launch(*plan->p, s, 1u << phase);
     if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
     return GPUFHE_OK;
@@ -74,7 +74,7 @@ int gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t s) 
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     if (!plan) return 0;
     uint32_t k = 0;
-    for (int i = 0; i < 7; ++i) k += plan->p->job_cnt[i] ? 1 : 0;
+    for (int i = 0; i < pl::NPHASE; ++i) k += plan->p->job_cnt[i] ? 1 : 0;
     return k;
 }
 

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <stdexcept>
 
 namespace pl {
@@ -14,34 +15,44 @@ namespace {
 
 template <int LOGN>
 struct Launcher {
-    static void attrs() {
+    static void attrs(uint32_t dnum) {
         using G = ntt::Geo<LOGN>;
         static bool done = false;
-        if (done) return;
-        cudaFuncSetAttribute(k1_inv_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-        cudaFuncSetAttribute(k2_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-        cudaFuncSetAttribute(k3_modup_fwd_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-        cudaFuncSetAttribute(k4_mac_fwd_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, PG<LOGN>::MAC_SMEM);
-        cudaFuncSetAttribute(k5_moddown_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-        cudaFuncSetAttribute(k6_moddown_fwd_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-        cudaFuncSetAttribute(k7_final_fwd_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-        done = true;
+        static uint32_t mac_dnum = 0;
+        if (!done) {
+            cudaFuncSetAttribute(p1_inv_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+            cudaFuncSetAttribute(p2_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+            cudaFuncSetAttribute(p3_modup_fwd_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+            cudaFuncSetAttribute(p4_modup_fwd_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+            cudaFuncSetAttribute(p6_moddown_inv_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+            cudaFuncSetAttribute(p7_moddown_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+            cudaFuncSetAttribute(p8_moddown_fwd_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+            cudaFuncSetAttribute(p9_final_fwd_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+            done = true;
+        }
+        if (dnum > mac_dnum) {
+            cudaFuncSetAttribute(p5_mac<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(dnum));
+            mac_dnum = dnum;
+        }
     }
     static void launch(const Plan& p, cudaStream_t s, unsigned mask) {
         using G = ntt::Geo<LOGN>;
-        using PGL = PG<LOGN>;
-        attrs();
+        constexpr int MAC_TILES = (1 << LOGN) / MAC_TILE;
+        attrs(p.dc.dnum);
         const DevCtx& D = p.dc;
         const PairDesc* pd = p.d_pairs;
         auto J = [&](int k) { return p.d_jobs + p.job_off[k]; };
         auto cnt = [&](int k) { return p.job_cnt[k]; };
-        if ((mask >> 0 & 1) && cnt(0)) k1_inv_row<LOGN><<<cnt(0) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(0));
-        if ((mask >> 1 & 1) && cnt(1)) k2_inv_col<LOGN><<<cnt(1) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(1));
-        if ((mask >> 2 & 1) && cnt(2)) k3_modup_fwd_col<LOGN><<<cnt(2) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(2));
-        if ((mask >> 3 & 1) && cnt(3)) k4_mac_fwd_row<LOGN><<<cnt(3) * PGL::MAC_TILES, PGL::MAC_THREADS, PGL::MAC_SMEM, s>>>(D, pd, J(3));
-        if ((mask >> 4 & 1) && cnt(4)) k5_moddown_inv_col<LOGN><<<cnt(4) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(4));
-        if ((mask >> 5 & 1) && cnt(5)) k6_moddown_fwd_col<LOGN><<<cnt(5) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(5));
-        if ((mask >> 6 & 1) && cnt(6)) k7_final_fwd_row<LOGN><<<cnt(6) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(6));
+        auto on = [&](int k) { return (mask >> k & 1) && cnt(k); };
+        if (on(0)) p1_inv_row<LOGN><<<cnt(0) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(0));
+        if (on(1)) p2_inv_col<LOGN><<<cnt(1) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(1));
+        if (on(2)) p3_modup_fwd_col<LOGN><<<cnt(2) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(2));
+        if (on(3)) p4_modup_fwd_row<LOGN><<<cnt(3) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(3));
+        if (on(4)) p5_mac<LOGN><<<cnt(4) * MAC_TILES, MAC_NT, mac_smem(D.dnum), s>>>(D, pd, p.d_mac_jobs, p.d_plist);
+        if (on(5)) p6_moddown_inv_row<LOGN><<<cnt(5) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(5));
+        if (on(6)) p7_moddown_inv_col<LOGN><<<cnt(6) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(6));
+        if (on(7)) p8_moddown_fwd_col<LOGN><<<cnt(7) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(7));
+        if (on(8)) p9_final_fwd_row<LOGN><<<cnt(8) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(8));
     }
 };
 
@@ -60,6 +71,7 @@ void validate(const gfx::Context& c, const Op& op) {
     if (op.L < 1 || op.L > c.fullQ()) throw std::invalid_argument("level out of range");
     if ((op.mode == EMR || op.mode == RESCALE) && op.L < 2) throw std::invalid_argument("rescale needs L >= 2");
     if (c.alpha() > (uint32_t)MAXA) throw std::invalid_argument("digit width above the fused limit");
+    if (c.dnum() > (uint32_t)MAC_MAX_DNUM) throw std::invalid_argument("too many digits for the key-stationary MAC");
     if (op.mode > RESCALE) throw std::invalid_argument("unknown mode");
     const int nin = op.mode == EMR ? 4 : op.mode == ROT ? 2 : 1;
     for (int k = 0; k < nin; ++k) if (!op.in[k]) throw std::invalid_argument("null input");
@@ -70,6 +82,8 @@ void validate(const gfx::Context& c, const Op& op) {
 Plan::~Plan() {
     if (d_pairs) cudaFree(d_pairs);
     if (d_jobs) cudaFree(d_jobs);
+    if (d_mac_jobs) cudaFree(d_mac_jobs);
+    if (d_plist) cudaFree(d_plist);
     if (own_ws && ws) cudaFree(ws);
 }
 
@@ -78,7 +92,7 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
     auto plan = std::make_unique<Plan>();
     plan->dc = c.dev();
     plan->logn = c.logn();
-    const uint32_t n = c.n(), K = c.K();
+    const uint32_t K = c.K();
     size_t need = 0;
     for (const Op& op : ops) { validate(c, op); need += op_workspace_words(c, op.L); }
     if (!ws) {
@@ -91,7 +105,9 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
     }
     plan->ws_words = need;
     std::vector<PairDesc> pairs(ops.size());
-    std::vector<uint2> jobs[7];
+    std::vector<uint2> jobs[NPHASE];
+    // P5: pairs per (key, QP row), streamed in groups of MAC_GROUP
+    std::map<std::pair<uint64_t, uint32_t>, std::vector<uint32_t>> rows;
     size_t off = 0;
     for (size_t pi = 0; pi < ops.size(); ++pi) {
         const Op& op = ops[pi];
@@ -116,34 +132,54 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
         if (op.mode == RESCALE) {
             jobs[0].push_back({pu, L - 1});
             jobs[1].push_back({pu, L - 1});
-            for (uint32_t i = 0; i + 1 < L; ++i) { jobs[5].push_back({pu, i}); jobs[6].push_back({pu, i}); }
+            for (uint32_t i = 0; i + 1 < L; ++i) { jobs[7].push_back({pu, i}); jobs[8].push_back({pu, i}); }
             continue;
         }
         for (uint32_t i = 0; i < L; ++i) { jobs[0].push_back({pu, i}); jobs[1].push_back({pu, i}); }
         for (uint32_t p = 0; p < nparts; ++p) {
             const uint32_t st = c.alpha() * p, sp = std::min(c.alpha(), L - st);
             for (uint32_t i = 0; i < QlP; ++i)
-                if (i < st || i >= st + sp) jobs[2].push_back({pu, p * QlP + i});
+                if (i < st || i >= st + sp) { jobs[2].push_back({pu, p * QlP + i}); jobs[3].push_back({pu, p * QlP + i}); }
         }
-        for (uint32_t i = 0; i < QlP; ++i) jobs[3].push_back({pu, i});
+        for (uint32_t i = 0; i < QlP; ++i) rows[{op.key_id, qp_of(i, L, c.fullQ())}].push_back(pu);
         const bool emr = op.mode == EMR;
-        for (uint32_t cc = 0; cc < 2; ++cc)
-            for (uint32_t t = emr ? 0 : 1; t <= K; ++t) jobs[4].push_back({pu, cc * (K + 1) + t});
+        for (uint32_t cc = 0; cc < 2; ++cc) {
+            for (uint32_t t = emr ? 0 : 1; t <= K; ++t) jobs[5].push_back({pu, cc * (K + 1) + t});
+            jobs[6].push_back({pu, cc});
+        }
         const uint32_t outL = emr ? L - 1 : L;
         for (uint32_t cc = 0; cc < 2; ++cc)
-            for (uint32_t i = 0; i < outL; ++i) { jobs[5].push_back({pu, cc * L + i}); jobs[6].push_back({pu, cc * L + i}); }
+            for (uint32_t i = 0; i < outL; ++i) { jobs[7].push_back({pu, cc * L + i}); jobs[8].push_back({pu, cc * L + i}); }
     }
-    (void)n;
+    std::vector<uint4> mac_jobs;
+    std::vector<uint32_t> plist;
+    for (auto& kv : rows) {
+        const auto& v = kv.second;
+        for (size_t g = 0; g < v.size(); g += MAC_GROUP) {
+            const uint32_t cnt = (uint32_t)std::min<size_t>(MAC_GROUP, v.size() - g);
+            mac_jobs.push_back({kv.first.second, (uint32_t)plist.size(), cnt, 0});
+            plist.insert(plist.end(), v.begin() + g, v.begin() + g + cnt);
+        }
+    }
     size_t total = 0;
-    for (int k = 0; k < 7; ++k) { plan->job_off[k] = total; plan->job_cnt[k] = (uint32_t)jobs[k].size(); total += jobs[k].size(); }
+    for (int k = 0; k < NPHASE; ++k) {
+        plan->job_off[k] = total;
+        plan->job_cnt[k] = (uint32_t)jobs[k].size();
+        total += jobs[k].size();
+    }
+    plan->job_cnt[4] = (uint32_t)mac_jobs.size();
     std::vector<uint2> all;
     all.reserve(total);
-    for (int k = 0; k < 7; ++k) all.insert(all.end(), jobs[k].begin(), jobs[k].end());
+    for (int k = 0; k < NPHASE; ++k) all.insert(all.end(), jobs[k].begin(), jobs[k].end());
     if (cudaMalloc(&plan->d_pairs, std::max<size_t>(pairs.size(), 1) * sizeof(PairDesc)) != cudaSuccess ||
-        cudaMalloc(&plan->d_jobs, std::max<size_t>(total, 1) * sizeof(uint2)) != cudaSuccess)
+        cudaMalloc(&plan->d_jobs, std::max<size_t>(total, 1) * sizeof(uint2)) != cudaSuccess ||
+        cudaMalloc(&plan->d_mac_jobs, std::max<size_t>(mac_jobs.size(), 1) * sizeof(uint4)) != cudaSuccess ||
+        cudaMalloc(&plan->d_plist, std::max<size_t>(plist.size(), 1) * sizeof(uint32_t)) != cudaSuccess)
         throw std::runtime_error("plan allocation failed");
     cudaMemcpy(plan->d_pairs, pairs.data(), pairs.size() * sizeof(PairDesc), cudaMemcpyHostToDevice);
     cudaMemcpy(plan->d_jobs, all.data(), total * sizeof(uint2), cudaMemcpyHostToDevice);
+    cudaMemcpy(plan->d_mac_jobs, mac_jobs.data(), mac_jobs.size() * sizeof(uint4), cudaMemcpyHostToDevice);
+    cudaMemcpy(plan->d_plist, plist.data(), plist.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
     plan->nops = (uint32_t)ops.size();
     plan->ops = ops;
     plan->pairs_host = pairs;
@@ -161,6 +197,8 @@ void rebind(Plan& p, uint32_t idx, const Op& op, const gfx::Context& c, cudaStre
     const bool same_shape = old.L == op.L && (old.mode == op.mode ||
                             ((old.mode == KS || old.mode == ROT) && (op.mode == KS || op.mode == ROT)));
     if (!same_shape) throw std::invalid_argument("rebind: level or job shape differs");
+    if (op.key_id != old.key_id && p.ops.size() > 1)
+        throw std::invalid_argument("rebind: changing the key of one operation of a shared batch");
     PairDesc P = p.pairs_host[idx];
     P.mode = op.mode;
     P.galois = op.galois;

@@ -15,14 +15,18 @@
 // SwitchModulus(q_l -> q_i). Every step is an exact residue computation, so
 // each output equals the reference's bit for bit.
 //
-// Kernels (one launch each over all jobs of the batch; jobs are (pair, sub)):
-//   K1 inv-row  (pair,i)        tensor / gather prologue, INTT row stages  -> X
-//   K2 inv-col  (pair,i)        INTT column stages, * n^-1 QHatInv         -> X
-//   K3 fwd-col  (pair,p,i)      ModUp conversion prologue, NTT columns     -> Y
-//   K4 fwd-row  (pair,i<L+K)    NTT rows per digit + key MAC, epilogue     -> W / U / RP
-//   K5 inv-col  (pair,c,t<=K)   INTT columns of U and RP, scaled           -> U / RP
-//   K6 fwd-col  (pair,c,i)      ModDown + SwitchModulus prologue           -> Z
-//   K7 fwd-row  (pair,c,i)      NTT rows, final combine                    -> out
+// Phases (one launch each; jobs are (pair, sub) unless noted):
+//   P1 inv-row  (pair,i)       tensor / gather prologue, INTT row stages     -> X
+//   P2 inv-col  (pair,i)       INTT column stages, * n^-1 QHatInv            -> X
+//   P3 fwd-col  (pair,p,i)     ModUp conversion prologue, NTT column stages  -> Y
+//   P4 fwd-row  (pair,p,i)     NTT row stages                               -> Y (eval digit)
+//   P5 MAC      (row,group)    key-stationary inner product over the batch:
+//                              one CTA keeps a key-row tile of every digit in
+//                              shared memory and streams all pairs using it -> W / U / RP
+//   P6 inv-row  (pair,c,t)     INTT row stages of U (dropped tower) and RP   -> U / RP
+//   P7 inv-col  (pair,c)       INTT columns of RP then U, scaled; r_l        -> RP / U
+//   P8 fwd-col  (pair,c,i)     ModDown conversion + SwitchModulus prologue   -> Z
+//   P9 fwd-row  (pair,c,i)     NTT row stages, final combine                -> out
 #pragma once
 #include "context.hpp"
 #include "ntt.cuh"
@@ -32,7 +36,11 @@ namespace pl {
 using gfx::DevCtx;
 using gfx::Level;
 
-constexpr int MAXA = 16;   // digit width supported by the fused ModUp prologue
+constexpr int NPHASE = 9;
+constexpr int MAXA = 16;       // digit width supported by the fused ModUp prologue
+constexpr int MAC_TILE = 512;  // P5 elements per CTA
+constexpr int MAC_NT = 128;    // P5 threads (4 elements each)
+constexpr int MAC_GROUP = 16;  // P5 pairs streamed per CTA
 
 enum Mode : u32 {
     EMR = 0,       // EvalMult + Rescale: in = c0a,c1a,c0b,c1b [L]; out0,out1 [L-1]
@@ -82,17 +90,7 @@ __device__ __forceinline__ u32 galois_slot(u32 j, u64 k) {
     return __brev((t - 1) >> 1) >> (32 - LOGN);
 }
 
-template <int LOGN>
-struct PG {
-    using G = ntt::Geo<LOGN>;
-    static constexpr int MAC_RB = ntt::cmin(G::R1, 8);          // K4 row tile rows
-    static constexpr int MAC_TILE = MAC_RB * 256;
-    static constexpr int MAC_THREADS = MAC_TILE / 8;            // 8 values per thread
-    static constexpr int MAC_TILES = G::R1 / MAC_RB;
-    static constexpr int MAC_SMEM = MAC_RB * G::ROW_STRIDE * 8;
-};
-
-// Digit source value at element e of tower i (eval form, canonical).
+// Digit source value at element e of Q tower i (eval form, canonical).
 template <int LOGN>
 __device__ __forceinline__ u64 digit_src(const PairDesc& P, u32 i, u32 e, const ModC& m) {
     const size_t o = ((size_t)i << LOGN);
@@ -101,10 +99,14 @@ __device__ __forceinline__ u64 digit_src(const PairDesc& P, u32 i, u32 e, const 
     return P.in[0][o + e];
 }
 
-// ------------------------------------------------------------------ K1
+__device__ __forceinline__ u64* slot_ptr(const PairDesc& P, u32 slot, int logn) {
+    return P.ws + ((size_t)slot << logn);
+}
+
+// ------------------------------------------------------------------ P1
 template <int LOGN>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS)
-k1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
     const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
@@ -113,7 +115,7 @@ k1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
     const u32 i = jb.y;
     const ModC m = D.mod[i];
     const WsLayout w = ws_layout(P.L, D.K, D.alpha);
-    u64* X = P.ws + ((size_t)(w.X + i) << LOGN) + (size_t)R0 * 256;
+    u64* X = slot_ptr(P, w.X + i, LOGN) + (size_t)R0 * 256;
     ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
         sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = digit_src<LOGN>(P, i, (R0 + rl) * 256 + c, m);
     });
@@ -123,10 +125,10 @@ k1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
                                                            m.q, m.two_q, st);
 }
 
-// ------------------------------------------------------------------ K2
+// ------------------------------------------------------------------ P2
 template <int LOGN>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
-k2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
     const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
@@ -138,257 +140,332 @@ k2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
     const u64 sc = P.mode == RESCALE ? D.ninv[i] : lv.up_scale[i];
     const u64 scp = P.mode == RESCALE ? D.ninvp[i] : lv.up_scale_p[i];
     const WsLayout w = ws_layout(P.L, D.K, D.alpha);
-    u64* X = P.ws + ((size_t)(w.X + i) << LOGN) + c0;
+    u64* X = slot_ptr(P, w.X + i, LOGN) + c0;
     auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
     auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
     ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)i << LOGN)}, m.q,
                                                           m.two_q, ld, st);
 }
 
-// ------------------------------------------------------------------ K3
-template <int LOGN>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
-k3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+// ------------------------------------------------------------------ P3
+template <int LOGN, int SP>
+__device__ __forceinline__ void p3_body(const DevCtx& D, const PairDesc& P, u32 p, u32 i, int c0, u64* sm) {
     using G = ntt::Geo<LOGN>;
-    extern __shared__ __align__(16) u64 sm[];
-    __shared__ u64 cst[MAXA];
-    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
-    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
-    const PairDesc& P = pairs[jb.x];
     const u32 L = P.L, K = D.K, QlP = L + K;
-    const u32 p = jb.y / QlP, i = jb.y % QlP;
     const Level& lv = D.lvl[L];
-    const u32 st0 = lv.part_st[p], sp = lv.part_sp[p];
+    const u32 st0 = lv.part_st[p];
+    const u32 sp = SP > 0 ? (u32)SP : lv.part_sp[p];
     const u32 qp = qp_of(i, L, D.fullQ);
     const ModC m = D.mod[qp];
-    if (threadIdx.x < sp) cst[threadIdx.x] = D.pool[lv.qmp_off + (st0 + threadIdx.x) * QlP + i];
-    __syncthreads();
     const WsLayout w = ws_layout(L, K, D.alpha);
-    const u64* X = P.ws + ((size_t)(w.X + st0) << LOGN) + c0;
-    u64* Y = P.ws + ((size_t)(w.Y + p * QlP + i) << LOGN) + c0;
+    const u64* X = slot_ptr(P, w.X + st0, LOGN) + c0;
+    u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + c0;
+    const u64* pool = D.pool + lv.qmp_off + (size_t)st0 * QlP + i;
+    __shared__ u64 cst[MAXA];
+    if (threadIdx.x < sp) cst[threadIdx.x] = pool[(size_t)threadIdx.x * QlP];
+    __syncthreads();
     auto ld = [&](int r, int cl) {
         const u64* x = X + r * 256 + cl;
         u64 lo = 0, hi = 0;
-#pragma unroll 4
-        for (u32 s = 0; s < sp; ++s) mac_wide(lo, hi, x[(size_t)s << LOGN], cst[s]);
+        if constexpr (SP > 0) {
+#pragma unroll
+            for (int s = 0; s < SP; ++s) mac_wide(lo, hi, x[(size_t)s << LOGN], cst[s]);
+        } else {
+            for (u32 s = 0; s < sp; ++s) mac_wide(lo, hi, x[(size_t)s << LOGN], cst[s]);
+        }
         return barrett_lazy(lo, hi, m.q, m.mu_lo, m.mu_hi);
     };
-    auto st = [&](int r, int cl, u64 v) { Y[r * 256 + cl] = v; };
+    auto stf = [&](int r, int cl, u64 v) { Y[r * 256 + cl] = v; };
     ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0>(sm, ntt::TwPacked{D.twf + ((size_t)qp << LOGN)}, m.q,
-                                                       m.two_q, ld, st);
+                                                       m.two_q, ld, stf);
 }
 
-// ------------------------------------------------------------------ K4
 template <int LOGN>
-__global__ void __launch_bounds__(PG<LOGN>::MAC_THREADS)
-k4_mac_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
-    using PGL = PG<LOGN>;
-    constexpr int NT = PGL::MAC_THREADS, RB = PGL::MAC_RB;
     extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / PGL::MAC_TILES];
-    const u32 R0 = (blockIdx.x % PGL::MAC_TILES) * RB;
+    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
+    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
     const PairDesc& P = pairs[jb.x];
-    const u32 L = P.L, K = D.K, QlP = L + K, i = jb.y;
-    const Level& lv = D.lvl[L];
+    const u32 QlP = P.L + D.K;
+    const u32 p = jb.y / QlP, i = jb.y % QlP;
+    switch (D.lvl[P.L].part_sp[p]) {
+        case 1: p3_body<LOGN, 1>(D, P, p, i, c0, sm); break;
+        case 2: p3_body<LOGN, 2>(D, P, p, i, c0, sm); break;
+        case 3: p3_body<LOGN, 3>(D, P, p, i, c0, sm); break;
+        case 4: p3_body<LOGN, 4>(D, P, p, i, c0, sm); break;
+        default: p3_body<LOGN, 0>(D, P, p, i, c0, sm); break;
+    }
+}
+
+// ------------------------------------------------------------------ P4
+// NTT row stages of one digit tower; output reduced to [0, 2q).
+template <int LOGN>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    using G = ntt::Geo<LOGN>;
+    extern __shared__ __align__(16) u64 sm[];
+    const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
+    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
+    const PairDesc& P = pairs[jb.x];
+    const u32 L = P.L, QlP = L + D.K;
+    const u32 p = jb.y / QlP, i = jb.y % QlP;
     const u32 qp = qp_of(i, L, D.fullQ);
     const ModC m = D.mod[qp];
-    const WsLayout w = ws_layout(L, K, D.alpha);
-    const size_t tile0 = (size_t)R0 * 256;
-    const ntt::TwPacked twf{D.twf + ((size_t)qp << LOGN)};
-    const size_t krow = (size_t)qp;   // full-QP key row of QlP position i
+    const WsLayout w = ws_layout(L, D.K, D.alpha);
+    u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + (size_t)R0 * 256;
+    auto ld = [&](int rl, int c) { return Y[rl * 256 + c]; };
+    ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0>(sm, ntt::TwPacked{D.twf + ((size_t)qp << LOGN)}, R0,
+                                                           m.q, m.two_q, ld);
+    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
+        Y[rl * 256 + c] = csub(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)], m.two_q);
+    });
+}
 
-    u64 a0l[8], a0h[8], a1l[8], a1h[8];
+// ------------------------------------------------------------------ P5
+// Job: {key row r (QP index), offset into the pair-index list, pair count}.
+// The CTA loads the key tile of row r for every digit (av and bv) into
+// shared memory once, then for each listed pair accumulates
+//   res_c = sum_p digit_p * key_p   (128-bit, one Barrett at the end)
+// over that pair's digits and writes the epilogue for its QlP position.
+template <int LOGN>
+__global__ void __launch_bounds__(MAC_NT)
+p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
+       const u32* __restrict__ plist) {
+    constexpr int TILES = (1 << LOGN) / MAC_TILE;
+    constexpr int EPT = MAC_TILE / MAC_NT;
+    extern __shared__ __align__(16) u64 sm[];     // [dnum][2][MAC_TILE]
+    const uint4 jb = jobs[blockIdx.x / TILES];
+    const u32 tile0 = (blockIdx.x % TILES) * MAC_TILE;
+    const u32 r = jb.x;
+    const ModC m = D.mod[r];
+    const u32 dnum = D.dnum;
+    // every listed pair uses the same key (checked on the host)
+    const PairDesc& P0 = pairs[plist[jb.y]];
+    for (u32 k = threadIdx.x; k < dnum * MAC_TILE; k += MAC_NT) {
+        const u32 p = k / MAC_TILE, e = k % MAC_TILE;
+        const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0 + e;
+        sm[(2 * p) * MAC_TILE + e] = P0.kbv[off];
+        sm[(2 * p + 1) * MAC_TILE + e] = P0.kav[off];
+    }
+    __syncthreads();
+    const bool is_p = r >= D.fullQ;
+    for (u32 g = 0; g < jb.z; ++g) {
+        const PairDesc& P = pairs[plist[jb.y + g]];
+        const u32 L = P.L, K = D.K, QlP = L + K;
+        const u32 i = is_p ? L + (r - D.fullQ) : r;       // QlP position of row r
+        const Level& lv = D.lvl[L];
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        u64 a0l[EPT], a0h[EPT], a1l[EPT], a1h[EPT];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) a0l[k] = a0h[k] = a1l[k] = a1h[k] = 0;
-
-    for (u32 p = 0; p < lv.nparts; ++p) {
-        const u32 st0 = lv.part_st[p], sp = lv.part_sp[p];
-        const bool in_range = i >= st0 && i < st0 + sp;
-        const size_t kofs = (((size_t)p * D.QP + krow) << LOGN) + tile0;
-        const u64* kb = P.kbv + kofs;
-        const u64* ka = P.kav + kofs;
-        if (in_range) {
+        for (int k = 0; k < EPT; ++k) a0l[k] = a0h[k] = a1l[k] = a1h[k] = 0;
+        for (u32 p = 0; p < lv.nparts; ++p) {
+            const u32 st0 = lv.part_st[p], sp = lv.part_sp[p];
+            const bool in_range = !is_p && i >= st0 && i < st0 + sp;
+            const u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + tile0;
+            const u64* kb = sm + (2 * p) * MAC_TILE;
+            const u64* ka = sm + (2 * p + 1) * MAC_TILE;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const u32 e = threadIdx.x + k * NT;
-                const u64 v = digit_src<LOGN>(P, i, (u32)tile0 + e, m);
+            for (int k = 0; k < EPT; ++k) {
+                const u32 e = threadIdx.x + k * MAC_NT;
+                const u64 v = in_range ? digit_src<LOGN>(P, i, tile0 + e, m) : Y[e];
                 mac_wide(a0l[k], a0h[k], v, kb[e]);
                 mac_wide(a1l[k], a1h[k], v, ka[e]);
             }
-        } else {
-            const u64* Y = P.ws + ((size_t)(w.Y + p * QlP + i) << LOGN) + tile0;
-            auto ld = [&](int rl, int c) { return Y[rl * 256 + c]; };
-            ntt::fwd_row_rounds<G::A, RB, NT, 3, 0>(sm, twf, R0, m.q, m.two_q, ld);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const u32 e = threadIdx.x + k * NT;
-                const u64 v = csub(sm[(e >> 8) * G::ROW_STRIDE + ntt::rowpad(e & 255)], m.two_q);
-                mac_wide(a0l[k], a0h[k], v, kb[e]);
-                mac_wide(a1l[k], a1h[k], v, ka[e]);
-            }
-            __syncthreads();
         }
-    }
-    u64 r0[8], r1[8];
+        u64 r0[EPT], r1[EPT];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        r0[k] = barrett(a0l[k], a0h[k], m);
-        r1[k] = barrett(a1l[k], a1h[k], m);
-    }
-
-    const bool is_q = i < L;
-    const bool drop = P.mode == EMR && i == L - 1;
-    if (is_q && !drop) {
-        // W = (t + res*P^-1)*s1 (EvalMult+Rescale) or res*P^-1 (keyswitch)
-        u64* W0 = P.ws + ((size_t)(w.W + i) << LOGN) + tile0;
-        u64* W1 = P.ws + ((size_t)(w.W + L + i) << LOGN) + tile0;
+        for (int k = 0; k < EPT; ++k) {
+            r0[k] = barrett(a0l[k], a0h[k], m);
+            r1[k] = barrett(a1l[k], a1h[k], m);
+        }
         const u64 q = m.q;
-        if (P.mode == EMR) {
-            const u64 s1 = lv.s1[i], s1p = lv.s1p[i], ps1 = lv.ps1[i], ps1p = lv.ps1p[i];
-            const size_t o = ((size_t)i << LOGN) + tile0;
+        u64 *d0, *d1;
+        if (is_p) {
+            d0 = slot_ptr(P, w.RP + (i - L), LOGN) + tile0;
+            d1 = slot_ptr(P, w.RP + K + (i - L), LOGN) + tile0;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const u32 e = threadIdx.x + k * NT;
-                const u64 x0 = P.in[0][o + e], x1 = P.in[1][o + e], y0 = P.in[2][o + e], y1 = P.in[3][o + e];
-                const u64 t0 = mulmod(x0, y0, m);
-                u64 lo, hi;
-                mul_wide(x0, y1, lo, hi);
-                mac_wide(lo, hi, x1, y0);
-                const u64 t1 = barrett(lo, hi, m);
-                W0[e] = csub(csub(shoup_lazy(t0, s1, s1p, q) + shoup_lazy(r0[k], ps1, ps1p, q), m.two_q), q);
-                W1[e] = csub(csub(shoup_lazy(t1, s1, s1p, q) + shoup_lazy(r1[k], ps1, ps1p, q), m.two_q), q);
+            for (int k = 0; k < EPT; ++k) {
+                const u32 e = threadIdx.x + k * MAC_NT;
+                d0[e] = r0[k];
+                d1[e] = r1[k];
             }
-        } else {
-            const u64 pv = D.pinv[i], pvp = D.pinvp[i];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const u32 e = threadIdx.x + k * NT;
-                W0[e] = shoup(r0[k], pv, pvp, q);
-                W1[e] = shoup(r1[k], pv, pvp, q);
-            }
+            continue;
         }
-        return;
-    }
-    // dropped tower (u = t + res*P^-1) or P tower (res): INTT row stages
-    if (drop) {
         const u64 pv = D.pinv[i], pvp = D.pinvp[i];
-        const size_t o = ((size_t)i << LOGN) + tile0;
+        if (P.mode != EMR) {   // keyswitch / rotation: W = res * P^-1
+            d0 = slot_ptr(P, w.W + i, LOGN) + tile0;
+            d1 = slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const u32 e = threadIdx.x + k * NT;
+            for (int k = 0; k < EPT; ++k) {
+                const u32 e = threadIdx.x + k * MAC_NT;
+                d0[e] = shoup(r0[k], pv, pvp, q);
+                d1[e] = shoup(r1[k], pv, pvp, q);
+            }
+            continue;
+        }
+        const size_t o = ((size_t)i << LOGN) + tile0;
+        const bool drop = i == L - 1;
+        const u64 s1 = lv.s1[i], s1p = lv.s1p[i], ps1 = lv.ps1[i], ps1p = lv.ps1p[i];
+        d0 = drop ? slot_ptr(P, w.U, LOGN) + tile0 : slot_ptr(P, w.W + i, LOGN) + tile0;
+        d1 = drop ? slot_ptr(P, w.U + 1, LOGN) + tile0 : slot_ptr(P, w.W + L + i, LOGN) + tile0;
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+            const u32 e = threadIdx.x + k * MAC_NT;
             const u64 x0 = P.in[0][o + e], x1 = P.in[1][o + e], y0 = P.in[2][o + e], y1 = P.in[3][o + e];
             const u64 t0 = mulmod(x0, y0, m);
             u64 lo, hi;
             mul_wide(x0, y1, lo, hi);
             mac_wide(lo, hi, x1, y0);
             const u64 t1 = barrett(lo, hi, m);
-            r0[k] = csub(t0 + shoup(r0[k], pv, pvp, m.q), m.q);
-            r1[k] = csub(t1 + shoup(r1[k], pv, pvp, m.q), m.q);
+            if (drop) {   // u = t + res * P^-1 (eval), INTT'd in P6/P7
+                d0[e] = csub(t0 + shoup(r0[k], pv, pvp, q), q);
+                d1[e] = csub(t1 + shoup(r1[k], pv, pvp, q), q);
+            } else {      // W = t*s1 + res*P^-1*s1
+                d0[e] = csub(csub(shoup_lazy(t0, s1, s1p, q) + shoup_lazy(r0[k], ps1, ps1p, q), m.two_q), q);
+                d1[e] = csub(csub(shoup_lazy(t1, s1, s1p, q) + shoup_lazy(r1[k], ps1, ps1p, q), m.two_q), q);
+            }
         }
-    }
-    const ntt::TwPacked twi{D.twi + ((size_t)qp << LOGN)};
-    for (int c = 0; c < 2; ++c) {
-        u64* dst = drop ? P.ws + ((size_t)(w.U + c) << LOGN) + tile0
-                        : P.ws + ((size_t)(w.RP + c * K + (i - L)) << LOGN) + tile0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const u32 e = threadIdx.x + k * NT;
-            sm[(e >> 8) * G::ROW_STRIDE + ntt::rowpad(e & 255)] = c ? r1[k] : r0[k];
-        }
-        __syncthreads();
-        auto st = [&](int rl, int cc, u64 v) { dst[rl * 256 + cc] = v; };
-        ntt::inv_row_rounds<G::A, RB, NT, 3, 8>(sm, twi, R0, m.q, m.two_q, st);
-        __syncthreads();
     }
 }
 
-// ------------------------------------------------------------------ K5
+// ------------------------------------------------------------------ P6
+// INTT row stages of U[c] (t = 0, EvalMult+Rescale only) and RP[c][t-1].
 template <int LOGN>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
-k5_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
-    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
+    const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
+    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
     const PairDesc& P = pairs[jb.x];
     const u32 L = P.L, K = D.K;
     const u32 c = jb.y / (K + 1), t = jb.y % (K + 1);
     const WsLayout w = ws_layout(L, K, D.alpha);
-    u32 qp, slot;
-    u64 sc, scp;
-    if (t == 0) { qp = L - 1; slot = w.U + c; sc = D.ninv[qp]; scp = D.ninvp[qp]; }
-    else { qp = D.fullQ + t - 1; slot = w.RP + c * K + (t - 1); sc = D.pdn[t - 1]; scp = D.pdnp[t - 1]; }
+    const u32 qp = t == 0 ? L - 1 : D.fullQ + t - 1;
+    const u32 slot = t == 0 ? w.U + c : w.RP + c * K + (t - 1);
     const ModC m = D.mod[qp];
-    u64* X = P.ws + ((size_t)slot << LOGN) + c0;
-    auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
-    auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
-    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)qp << LOGN)}, m.q,
-                                                          m.two_q, ld, st);
+    u64* X = slot_ptr(P, slot, LOGN) + (size_t)R0 * 256;
+    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int cc) {
+        sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)] = X[rl * 256 + cc];
+    });
+    __syncthreads();
+    auto st = [&](int rl, int cc, u64 v) { X[rl * 256 + cc] = v; };
+    ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, ntt::TwPacked{D.twi + ((size_t)qp << LOGN)}, R0,
+                                                           m.q, m.two_q, st);
 }
 
-// ------------------------------------------------------------------ K6
+// ------------------------------------------------------------------ P7
+// One CTA per (pair, component, column tile): INTT columns of the K P towers
+// (scaled by n^-1 * PHatInv), then of U[c] (scaled by n^-1) followed by
+// r_l = u - conv'_l * P^-1 mod q_l, written back into U[c]. The thread that
+// stores an element of each P tower is the one that reads it back for r_l.
 template <int LOGN>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
-k6_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+p7_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
-    __shared__ u64 ci[gfx::MAXP], cl_[gfx::MAXP];
+    __shared__ u64 cl_[gfx::MAXP];
     const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
     const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
     const PairDesc& P = pairs[jb.x];
-    const u32 L = P.L, K = D.K, mode = P.mode;
-    const u32 c = jb.y / L, i = jb.y % L;
-    const u32 l = L - 1;
+    const u32 L = P.L, K = D.K, c = jb.y, l = L - 1;
+    const WsLayout w = ws_layout(L, K, D.alpha);
+    if (threadIdx.x < K) cl_[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + l];
+    for (u32 t = 1; t <= K; ++t) {
+        const u32 qp = D.fullQ + t - 1;
+        const ModC m = D.mod[qp];
+        const u64 sc = D.pdn[t - 1], scp = D.pdnp[t - 1];
+        u64* X = slot_ptr(P, w.RP + c * K + (t - 1), LOGN) + c0;
+        auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
+        auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
+        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)qp << LOGN)}, m.q,
+                                                              m.two_q, ld, st);
+        __syncthreads();
+    }
+    if (P.mode != EMR) return;
+    const ModC m = D.mod[l];
+    const u64 ni = D.ninv[l], nip = D.ninvp[l], pv = D.pinv[l], pvp = D.pinvp[l];
+    u64* U = slot_ptr(P, w.U + c, LOGN) + c0;
+    const u64* XP = slot_ptr(P, w.RP + c * K, LOGN) + c0;
+    auto ld = [&](int r, int cl) { return U[r * 256 + cl]; };
+    auto st = [&](int r, int cl, u64 v) {
+        const int e = r * 256 + cl;
+        const u64 u = shoup(v, ni, nip, m.q);
+        u64 lo = 0, hi = 0;
+        for (u32 j = 0; j < K; ++j) mac_wide(lo, hi, XP[((size_t)j << LOGN) + e], cl_[j]);
+        const u64 tmp = shoup(barrett_lazy(lo, hi, m.q, m.mu_lo, m.mu_hi), pv, pvp, m.q);
+        U[e] = u >= tmp ? u - tmp : u + m.q - tmp;
+    };
+    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)l << LOGN)}, m.q,
+                                                          m.two_q, ld, st);
+}
+
+// ------------------------------------------------------------------ P8
+template <int LOGN, u32 MODE>
+__device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 c, u32 i, int c0, u64* sm,
+                                        const u64* ci) {
+    using G = ntt::Geo<LOGN>;
+    const u32 L = P.L, K = D.K, l = L - 1;
     const WsLayout w = ws_layout(L, K, D.alpha);
     const Level& lv = D.lvl[L];
     const ModC m = D.mod[i];
-    const ModC ml = D.mod[l];
-    if (threadIdx.x < K) {
-        ci[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + i];
-        cl_[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + l];
-    }
-    __syncthreads();
-    const u64* XP = P.ws + ((size_t)(w.RP + c * K) << LOGN) + c0;
-    const u64* UC = mode == RESCALE ? P.ws + ((size_t)(w.X + l) << LOGN) + c0
-                                    : P.ws + ((size_t)(w.U + c) << LOGN) + c0;
-    u64* Z = P.ws + ((size_t)(w.Z + c * L + i) << LOGN) + c0;
     const u64 q = m.q;
+    const u64* XP = slot_ptr(P, w.RP + c * K, LOGN) + c0;
+    const u64* R = MODE == RESCALE ? slot_ptr(P, w.X + l, LOGN) + c0 : slot_ptr(P, w.U + c, LOGN) + c0;
+    u64* Z = slot_ptr(P, w.Z + c * L + i, LOGN) + c0;
     // SwitchModulus q_l -> q_i (switch_modulus.cu:11-27)
-    const u64 half = ml.q >> 1;
-    const bool larger = q > ml.q;
-    const u64 diff = larger ? q - ml.q : (ml.q - q) % q;
-    auto swm = [&](u64 r) -> u64 {
-        const u64 d = r > half ? diff : 0;
-        if (larger) return r + d;
-        const u64 xm = reduce64(r, m);
-        return xm >= d ? xm - d : xm + q - d;
-    };
-    auto conv = [&](const u64* x, const u64* cst, const ModC& mm) {
-        u64 lo = 0, hi = 0;
-        for (u32 j = 0; j < K; ++j) mac_wide(lo, hi, x[(size_t)j << LOGN], cst[j]);
-        return barrett_lazy(lo, hi, mm.q, mm.mu_lo, mm.mu_hi);
-    };
+    const u64 ql = D.mod[l].q;
+    const u64 half = ql >> 1;
+    const bool larger = q > ql;
+    const u64 diff = larger ? q - ql : (ql - q) % q;
+    const u64 s2 = lv.s2[i], s2p = lv.s2p[i];
+    const u64 cm = MODE == EMR ? lv.ps1[i] : D.pinv[i];
+    const u64 cmp = MODE == EMR ? lv.ps1p[i] : D.pinvp[i];
     auto ld = [&](int r, int cl) -> u64 {
         const int e = r * 256 + cl;
-        if (mode == RESCALE) return shoup_lazy(swm(UC[e]), lv.s2[i], lv.s2p[i], q);
-        const u64 cvi = conv(XP + e, ci, m);
-        if (mode != EMR) return 2 * q - shoup_lazy(cvi, D.pinv[i], D.pinvp[i], q);
-        const u64 cvl = conv(XP + e, cl_, ml);
-        const u64 tmp = shoup(cvl, D.pinv[l], D.pinvp[l], ml.q);
-        const u64 u = UC[e];
-        const u64 rl = u >= tmp ? u - tmp : u + ml.q - tmp;
-        return shoup_lazy(swm(rl), lv.s2[i], lv.s2p[i], q) + 2 * q - shoup_lazy(cvi, lv.ps1[i], lv.ps1p[i], q);
+        u64 v = 0;
+        if constexpr (MODE == EMR || MODE == RESCALE) {
+            const u64 x = R[e];
+            const u64 d = x > half ? diff : 0;
+            u64 sw;
+            if (larger) sw = x + d;
+            else { const u64 xm = reduce64(x, m); sw = xm >= d ? xm - d : xm + q - d; }
+            v = shoup_lazy(sw, s2, s2p, q);
+        }
+        if constexpr (MODE != RESCALE) {
+            u64 lo = 0, hi = 0;
+            for (u32 j = 0; j < K; ++j) mac_wide(lo, hi, XP[((size_t)j << LOGN) + e], ci[j]);
+            v += 2 * q - shoup_lazy(barrett_lazy(lo, hi, q, m.mu_lo, m.mu_hi), cm, cmp, q);
+        }
+        return v;
     };
     auto st = [&](int r, int cl, u64 v) { Z[r * 256 + cl] = v; };
-    ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0>(sm, ntt::TwPacked{D.twf + ((size_t)i << LOGN)}, q,
-                                                       m.two_q, ld, st);
+    ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0>(sm, ntt::TwPacked{D.twf + ((size_t)i << LOGN)}, q, m.two_q,
+                                                       ld, st);
 }
 
-// ------------------------------------------------------------------ K7
 template <int LOGN>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS)
-k7_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    extern __shared__ __align__(16) u64 sm[];
+    __shared__ u64 ci[gfx::MAXP];
+    const uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
+    const int c0 = (blockIdx.x % ntt::Geo<LOGN>::COL_TILES) * ntt::Geo<LOGN>::C;
+    const PairDesc& P = pairs[jb.x];
+    const u32 c = jb.y / P.L, i = jb.y % P.L;
+    if (threadIdx.x < D.K) ci[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + i];
+    __syncthreads();
+    if (P.mode == EMR) p8_body<LOGN, EMR>(D, P, c, i, c0, sm, ci);
+    else if (P.mode == RESCALE) p8_body<LOGN, RESCALE>(D, P, c, i, c0, sm, ci);
+    else p8_body<LOGN, KS>(D, P, c, i, c0, sm, ci);
+}
+
+// ------------------------------------------------------------------ P9
+template <int LOGN>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
     const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
@@ -399,13 +476,13 @@ k7_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     const WsLayout w = ws_layout(L, K, D.alpha);
     const ModC m = D.mod[i];
     const size_t tile0 = (size_t)R0 * 256;
-    const u64* Z = P.ws + ((size_t)(w.Z + c * L + i) << LOGN) + tile0;
+    const u64* Z = slot_ptr(P, w.Z + c * L + i, LOGN) + tile0;
     auto ld = [&](int rl, int cc) { return Z[rl * 256 + cc]; };
     ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0>(sm, ntt::TwPacked{D.twf + ((size_t)i << LOGN)}, R0, m.q,
                                                            m.two_q, ld);
     const size_t o = ((size_t)i << LOGN) + tile0;
     u64* out = P.out[c] + o;
-    const u64* Wt = P.ws + ((size_t)(w.W + c * L + i) << LOGN) + tile0;
+    const u64* Wt = slot_ptr(P, w.W + c * L + i, LOGN) + tile0;
     const Level& lv = D.lvl[L];
     const u64 s1 = lv.s1[i], s1p = lv.s1p[i];
     ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int cc) {

@@ -23,8 +23,10 @@ struct Plan {
     uint32_t logn = 0, nops = 0;
     PairDesc* d_pairs = nullptr;
     uint2* d_jobs = nullptr;
-    size_t job_off[7] = {};
-    uint32_t job_cnt[7] = {};
+    size_t job_off[NPHASE] = {};
+    uint32_t job_cnt[NPHASE] = {};
+    uint4* d_mac_jobs = nullptr;
+    uint32_t* d_plist = nullptr;
     u64* ws = nullptr;
     size_t ws_words = 0;
     bool own_ws = false;
@@ -38,8 +40,10 @@ size_t op_workspace_words(const gfx::Context& c, uint32_t L);
 void validate(const gfx::Context& c, const Op& op);
 // ws == nullptr: the plan allocates (and owns) its workspace.
 std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words);
-// mask selects phases K1..K7 (bit k = phase k+1); 0x7f runs the whole batch.
-cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x7f);
+// mask selects phases P1..P9 (bit k = phase k+1); 0x1ff runs the whole batch.
+cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
+constexpr int MAC_MAX_DNUM = 16;
+inline int mac_smem(uint32_t dnum) { return (int)(dnum * 2 * MAC_TILE * sizeof(u64)); }
 int input_count(uint32_t mode);
 // Rebinds operation `idx` of a built plan to new buffers / mode (same level
 // and job shape) by a one-thread kernel on `s`: no allocation and no host
