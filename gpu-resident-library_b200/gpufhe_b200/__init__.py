@@ -57,6 +57,8 @@ _API: dict = {
     "gpufhe_native_primes": (I32, [VP, U32, U32, U32, VP, U32]),
     "gpufhe_native_root": (U64, [U32, U64]),
     "gpufhe_rescale_consts": (I32, [VP, VP, VP, U32]),
+    "gpufhe_rescale_noalloc": (I32, [VP, U32, VP, VP]),
+    "gpufhe_rescale_noalloc_max_words": (U64, []),
 }
 
 EVALMULT_RESCALE, KEYSWITCH, ROTATE, RESCALE = 0, 1, 2, 3

@@ -124,6 +124,23 @@ int  gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uin
 /* create + launch + synchronize + destroy */
 int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- no allocation
+ * No counterpart in the reference. Rescale of one eval-form component
+ * d_comp ([level][n], in place: the first level-1 towers receive the result)
+ * that calls no cudaMalloc / cudaFree: for hosts that own the device-memory
+ * budget through their own pool and forbid a library from allocating
+ * (cudaMalloc can fail under a fixed budget, cudaFree synchronizes the
+ * device), and for serving threads that must not block on an allocation.
+ * Same result, bit for bit, as GPUFHE_RESCALE and rescale_resident_raw.
+ * Its scratch is a static device array of gpufhe_rescale_noalloc_max_words()
+ * uint64 words (8 MiB, held by every GPU that loads the library until the
+ * process exits); level * n above that returns GPUFHE_ENOMEM. The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make it before any stream capture. All calls share the array: calls that
+ * overlap on the GPU race. */
+int      gpufhe_rescale_noalloc(gpufhe_ctx* ctx, uint32_t level, uint64_t* d_comp, cudaStream_t stream);
+uint64_t gpufhe_rescale_noalloc_max_words(void);
+
 #ifdef __cplusplus
 }
 #endif
