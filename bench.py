@@ -136,6 +136,144 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ---------------------------------------------------------------- serving trace
+SERVE_LOGNS = (14, 15, 16)
+SERVE_TOWERS, SERVE_K, SERVE_ALPHA = 24, 8, 8          # dnum = 3 at 24 towers
+SERVE_RATE = 2000.0                                     # Poisson arrivals, requests/s
+SERVE_ROT_STEPS = (1, 2, 4, 8, -1, -2, -4, -8)
+SERVE_WORKLOAD = ("serving trace: Poisson arrivals at 2000 req/s (seeded); per request N in {2^14,2^15,2^16}, "
+                  "towers U[4,24], depth U[1,10] of EvalMult+Rescale (capped at towers-1) with U[0,8] rotations "
+                  "by +-{1,2,4,8} interleaved; Q=1x60+23x50-bit, P=8x60-bit, alpha=8 (dnum=3)")
+
+
+def galois_element(r, n):
+    M = 2 * n
+    return pow(5, r, M) if r >= 0 else pow(pow(5, -r, M), -1, M)
+
+
+def serving_contexts(G, device):
+    """One context per ring size with a relinearisation key and one key per rotation step."""
+    ctxs = []
+    for lg in SERVE_LOGNS:
+        n = 1 << lg
+        q0 = G.native_primes(1, 60, n)
+        qs = G.native_primes(SERVE_TOWERS - 1, 50, n, avoid=list(q0))
+        Q = np.concatenate([q0, qs])
+        P = G.native_primes(SERVE_K, 60, n, avoid=list(Q))
+        c = G.Context(n, Q, P, SERVE_ALPHA, device=device)
+        rows = -(-SERVE_TOWERS // SERVE_ALPHA) * (SERVE_TOWERS + SERVE_K)
+        rng = np.random.default_rng(SEED + lg)
+        pool = rng.integers(0, 1 << 49, 2 * rows * n, dtype=np.uint64)   # below every prime of the chain
+        for j, k in enumerate([0] + [galois_element(r, n) for r in SERVE_ROT_STEPS]):
+            key = np.roll(pool, 7919 * j)                                  # distinct material per key
+            c.set_key(k, key[: rows * n], key[rows * n:])
+        ctxs.append(c)
+    return ctxs
+
+
+def serving_trace(count, seed):
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, count))
+    reqs = []
+    for i in range(count):
+        c = int(rng.integers(0, len(SERVE_LOGNS)))
+        n = 1 << SERVE_LOGNS[c]
+        L = int(rng.integers(4, SERVE_TOWERS + 1))
+        d = min(int(rng.integers(1, 11)), L - 1)
+        rots = [galois_element(int(r), n) for r in rng.choice(SERVE_ROT_STEPS, int(rng.integers(0, 9)))]
+        ops = [(0, 0)] * d + [(2, k) for k in rots]
+        ops = [ops[j] for j in rng.permutation(len(ops))]
+        reqs.append((c, L, ops, float(arrivals[i])))
+    return reqs
+
+
+def serve(G, ctxs, reqs, budget, plain):
+    srv = G.Server(ctxs, budget, plain=plain)
+    for i, (c, L, ops, t) in enumerate(reqs):
+        srv.submit(c, L, ops, arrival_s=t, seed=SEED + i)
+    srv.start()
+    srv.drain(900.0)
+    st, rec = srv.stats(), srv.records()
+    srv.close()
+    lat = np.array([r["t_finish"] - r["t_arrival"] for r in rec]) * 1e3
+    lat_admit = np.array([r["t_finish"] - r["t_admit"] for r in rec]) * 1e3
+    span = max(r["t_finish"] for r in rec) - min(r["t_arrival"] for r in rec)
+    return {
+        "ops_per_s": st["ops"] / st["busy_s"], "evalmult_rescale_ops_per_s": st["emr_ops"] / st["busy_s"],
+        "requests_per_s": st["completed"] / st["busy_s"], "busy_s": st["busy_s"], "trace_span_s": span,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "from": "arrival to result (queueing included)"},
+        "service_latency_ms": {"p50": float(np.percentile(lat_admit, 50)),
+                               "p99": float(np.percentile(lat_admit, 99)), "from": "admission to result"},
+        "steps": st["steps"], "ops": st["ops"], "evalmult_rescale_ops": st["emr_ops"],
+        "completed": st["completed"], "peak_active": st["peak_active"], "max_batch": st["max_batch"],
+        "peak_arena_bytes": st["peak_bytes"], "arena_bytes": st["arena_bytes"],
+        "resident_bytes": st["resident_bytes"],
+    }
+
+
+def run_serving(G, device, count, free_bytes, dist=None, dev=None):
+    """The trace on this rank's share of requests (all of it at N=1)."""
+    ctxs = serving_contexts(G, device)
+    reqs = serving_trace(count, SEED + 5)
+    resident = sum(c.resident_bytes() for c in ctxs)
+    arena = min(int(free_bytes * 0.6), 80 << 30)
+    if dist is not None:
+        budgets = [None] * dist.get_world_size()
+        dist.all_gather_object(budgets, arena)
+        owner = shard_requests(len(reqs), budgets)
+        reqs = [r for r, o in zip(reqs, owner) if o == dist.get_rank()]
+    budget = resident + arena
+    served = serve(G, ctxs, reqs, budget, plain=False)
+    plain = serve(G, ctxs, reqs, budget, plain=True)
+    for c in ctxs:
+        c.close()
+    out = {"workload": SERVE_WORKLOAD, "requests": count, "requests_this_rank": len(reqs),
+           "hbm_budget_bytes": budget, "inputs": "seeded residues generated on the device at admission",
+           "served": served, "plain": plain, "served_vs_plain_ops": served["ops_per_s"] / plain["ops_per_s"]}
+    if dist is not None:
+        # whole-job rates: all ranks' operations over the slowest rank's busy time
+        for form in ("served", "plain"):
+            busy = max_over_ranks(out[form]["busy_s"], dist, dev)
+            ops = sum_over_ranks(out[form]["ops"], dist, dev)
+            emr = sum_over_ranks(out[form]["evalmult_rescale_ops"], dist, dev)
+            out[form]["job_ops_per_s"] = ops / busy
+            out[form]["job_evalmult_rescale_ops_per_s"] = emr / busy
+    return out
+
+
+def shard_requests(count, budgets):
+    """Owner rank of each request: smooth weighted round robin, weights = free HBM budget per rank."""
+    w = [max(1, int(b)) for b in budgets]
+    total = sum(w)
+    cur = [0] * len(w)
+    owner = []
+    for _ in range(count):
+        for k in range(len(w)):
+            cur[k] += w[k]
+        best = max(range(len(w)), key=lambda k: (cur[k], -k))
+        cur[best] -= total
+        owner.append(best)
+    return owner
+
+
+def _reduce(x, dist, dev, op):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def max_over_ranks(x, dist, dev):
+    return _reduce(x, dist, dev, dist.ReduceOp.MAX if dist is not None else None)
+
+
+def sum_over_ranks(x, dist, dev):
+    return _reduce(x, dist, dev, dist.ReduceOp.SUM if dist is not None else None)
+
+
 # ---------------------------------------------------------------- CPU oracle
 def cpu_port_rate(levels, n, nthreads, budget_s=20.0):
     """Oracle (CPU restatement of the reference path) on a bounded sample."""
@@ -278,11 +416,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     ms_step = ms / args.steps
     value = world * PAIRS * args.steps / (ms * 1e-3)
 
@@ -321,11 +455,7 @@ def run_gpu(args):
         plan.launch_host(h_in, h_out, stream.cuda_stream)
     b.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = a.elapsed_time(b) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(a.elapsed_time(b) / e2e_steps, dist, dev)
     e2e_value = world * PAIRS / (e2e_ms * 1e-3)
 
     # plain per-chain form: one pair per plan, graph per chain, 16 streams
@@ -395,6 +525,15 @@ def run_gpu(args):
         ntt = {"workload": "64 polys x 12 towers x 2^16, 50-bit primes", "bytes_per_tower": 2 * 8 * n, **res}
         del data
 
+    # serving trace (continuous batching vs one request at a time)
+    serving = None
+    if not args.no_serve:
+        del plan, ws, ins, outs, keep
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        free_b, _ = torch.cuda.mem_get_info(dev)
+        serving = run_serving(G, local, args.serve_requests, free_b, dist, dev)
+
     # CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -424,8 +563,10 @@ def run_gpu(args):
                 "ms_per_step": e2e_ms},
         "plain": plain,
         "served_vs_plain": (value / world / plain["value"]) if plain else None,
-        "latency_ms": {"p50": ms_step, "p99": ms_step, "mode": "whole batch per step"},
+        "latency_ms": (dict(serving["served"]["latency_ms"], source="serving trace, served form") if serving
+                       else {"p50": ms_step, "p99": ms_step, "source": "whole batch per step"}),
         "ntt_kernel_isolation": ntt,
+        "serving": serving,
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
@@ -443,6 +584,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

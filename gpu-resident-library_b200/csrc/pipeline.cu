@@ -79,39 +79,25 @@ void validate(const gfx::Context& c, const Op& op) {
     if (op.mode == ROT && (op.galois % 2 == 0 || op.galois >= 2ull * c.n())) throw std::invalid_argument("bad Galois element");
 }
 
-Plan::~Plan() {
-    if (d_pairs) cudaFree(d_pairs);
-    if (d_jobs) cudaFree(d_jobs);
-    if (d_mac_jobs) cudaFree(d_mac_jobs);
-    if (d_plist) cudaFree(d_plist);
-    if (own_ws && ws) cudaFree(ws);
-}
+// Host tables of a batch: pair descriptors, per-phase jobs and P5 groups.
+struct HostTables {
+    std::vector<PairDesc> pairs;
+    std::vector<uint2> jobs;       // all phases, concatenated
+    std::vector<uint4> mac_jobs;
+    std::vector<uint32_t> plist;
+    size_t job_off[NPHASE] = {};
+    uint32_t job_cnt[NPHASE] = {};
+};
 
-std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words) {
-    if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
-    auto plan = std::make_unique<Plan>();
-    plan->dc = c.dev();
-    plan->logn = c.logn();
+static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const std::vector<u64*>& ws_ptrs,
+                        HostTables& T) {
     const uint32_t K = c.K();
-    size_t need = 0;
-    for (const Op& op : ops) { validate(c, op); need += op_workspace_words(c, op.L); }
-    if (!ws) {
-        if (cudaMalloc(&plan->ws, std::max<size_t>(need, 1) * 8) != cudaSuccess)
-            throw std::runtime_error("workspace allocation failed");
-        plan->own_ws = true;
-        ws = plan->ws;
-    } else if (ws_words < need) {
-        throw std::length_error("workspace too small");
-    }
-    plan->ws_words = need;
-    std::vector<PairDesc> pairs(ops.size());
+    T.pairs.assign(ops.size(), PairDesc{});
     std::vector<uint2> jobs[NPHASE];
-    // P5: pairs per (key, QP row), streamed in groups of MAC_GROUP
     std::map<std::pair<uint64_t, uint32_t>, std::vector<uint32_t>> rows;
-    size_t off = 0;
     for (size_t pi = 0; pi < ops.size(); ++pi) {
         const Op& op = ops[pi];
-        PairDesc& P = pairs[pi];
+        PairDesc& P = T.pairs[pi];
         std::memset(&P, 0, sizeof(P));
         P.L = op.L;
         P.mode = op.mode;
@@ -119,8 +105,7 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
         for (int k = 0; k < 4; ++k) P.in[k] = op.in[k];
         P.out[0] = op.out[0];
         P.out[1] = op.out[1];
-        P.ws = ws + off;
-        off += op_workspace_words(c, op.L);
+        P.ws = ws_ptrs[pi];
         if (op.mode != RESCALE) {
             const gfx::Key* key = c.key(op.key_id);
             if (!key) throw std::invalid_argument("missing eval key");
@@ -151,39 +136,114 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
         for (uint32_t cc = 0; cc < 2; ++cc)
             for (uint32_t i = 0; i < outL; ++i) { jobs[7].push_back({pu, cc * L + i}); jobs[8].push_back({pu, cc * L + i}); }
     }
-    std::vector<uint4> mac_jobs;
-    std::vector<uint32_t> plist;
+    T.mac_jobs.clear();
+    T.plist.clear();
     for (auto& kv : rows) {
         const auto& v = kv.second;
         for (size_t g = 0; g < v.size(); g += MAC_GROUP) {
             const uint32_t cnt = (uint32_t)std::min<size_t>(MAC_GROUP, v.size() - g);
-            mac_jobs.push_back({kv.first.second, (uint32_t)plist.size(), cnt, 0});
-            plist.insert(plist.end(), v.begin() + g, v.begin() + g + cnt);
+            T.mac_jobs.push_back({kv.first.second, (uint32_t)T.plist.size(), cnt, 0});
+            T.plist.insert(T.plist.end(), v.begin() + g, v.begin() + g + cnt);
         }
     }
     size_t total = 0;
     for (int k = 0; k < NPHASE; ++k) {
-        plan->job_off[k] = total;
-        plan->job_cnt[k] = (uint32_t)jobs[k].size();
+        T.job_off[k] = total;
+        T.job_cnt[k] = (uint32_t)jobs[k].size();
         total += jobs[k].size();
     }
-    plan->job_cnt[4] = (uint32_t)mac_jobs.size();
-    std::vector<uint2> all;
-    all.reserve(total);
-    for (int k = 0; k < NPHASE; ++k) all.insert(all.end(), jobs[k].begin(), jobs[k].end());
-    if (cudaMalloc(&plan->d_pairs, std::max<size_t>(pairs.size(), 1) * sizeof(PairDesc)) != cudaSuccess ||
-        cudaMalloc(&plan->d_jobs, std::max<size_t>(total, 1) * sizeof(uint2)) != cudaSuccess ||
-        cudaMalloc(&plan->d_mac_jobs, std::max<size_t>(mac_jobs.size(), 1) * sizeof(uint4)) != cudaSuccess ||
-        cudaMalloc(&plan->d_plist, std::max<size_t>(plist.size(), 1) * sizeof(uint32_t)) != cudaSuccess)
-        throw std::runtime_error("plan allocation failed");
-    cudaMemcpy(plan->d_pairs, pairs.data(), pairs.size() * sizeof(PairDesc), cudaMemcpyHostToDevice);
-    cudaMemcpy(plan->d_jobs, all.data(), total * sizeof(uint2), cudaMemcpyHostToDevice);
-    cudaMemcpy(plan->d_mac_jobs, mac_jobs.data(), mac_jobs.size() * sizeof(uint4), cudaMemcpyHostToDevice);
-    cudaMemcpy(plan->d_plist, plist.data(), plist.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
-    plan->nops = (uint32_t)ops.size();
-    plan->ops = ops;
-    plan->pairs_host = pairs;
+    T.job_cnt[4] = (uint32_t)T.mac_jobs.size();
+    T.jobs.clear();
+    T.jobs.reserve(total);
+    for (int k = 0; k < NPHASE; ++k) T.jobs.insert(T.jobs.end(), jobs[k].begin(), jobs[k].end());
+}
+
+Plan::Plan() : staging(std::make_unique<HostTables>()) {}
+
+Plan::~Plan() {
+    if (d_blob) cudaFree(d_blob);
+    if (h_blob) cudaFreeHost(h_blob);
+    if (own_ws && ws) cudaFree(ws);
+}
+
+// All tables of a plan live in one device blob (pairs, jobs, P5 groups, pair
+// lists at 256-byte aligned offsets), uploaded by one copy from a pinned host
+// mirror, so an asynchronous rebuild does not wait for the stream.
+static void commit(Plan& p, const HostTables& T, const std::vector<Op>& ops, cudaStream_t s, bool async) {
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t b_pairs = al(T.pairs.size() * sizeof(PairDesc));
+    const size_t b_jobs = al(T.jobs.size() * sizeof(uint2));
+    const size_t b_mac = al(T.mac_jobs.size() * sizeof(uint4));
+    const size_t b_plist = al(T.plist.size() * sizeof(uint32_t));
+    const size_t total = std::max<size_t>(b_pairs + b_jobs + b_mac + b_plist, 256);
+    if (total > p.blob_cap) {
+        if (p.d_blob) cudaFree(p.d_blob);
+        if (p.h_blob) cudaFreeHost(p.h_blob);
+        p.d_blob = nullptr;
+        p.h_blob = nullptr;
+        p.blob_cap = 0;
+        const size_t cap = total + total / 2;
+        if (cudaMalloc(&p.d_blob, cap) != cudaSuccess) throw std::runtime_error("plan allocation failed");
+        if (cudaMallocHost(&p.h_blob, cap) != cudaSuccess) throw std::runtime_error("plan host allocation failed");
+        p.blob_cap = cap;
+    }
+    char* h = static_cast<char*>(p.h_blob);
+    char* d = static_cast<char*>(p.d_blob);
+    std::memcpy(h, T.pairs.data(), T.pairs.size() * sizeof(PairDesc));
+    std::memcpy(h + b_pairs, T.jobs.data(), T.jobs.size() * sizeof(uint2));
+    std::memcpy(h + b_pairs + b_jobs, T.mac_jobs.data(), T.mac_jobs.size() * sizeof(uint4));
+    std::memcpy(h + b_pairs + b_jobs + b_mac, T.plist.data(), T.plist.size() * sizeof(uint32_t));
+    const size_t used = b_pairs + b_jobs + b_mac + b_plist;
+    if (used) {
+        cudaError_t e = async ? cudaMemcpyAsync(d, h, used, cudaMemcpyHostToDevice, s)
+                              : cudaMemcpy(d, h, used, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) throw std::runtime_error(std::string("plan upload: ") + cudaGetErrorString(e));
+    }
+    p.d_pairs = reinterpret_cast<PairDesc*>(d);
+    p.d_jobs = reinterpret_cast<uint2*>(d + b_pairs);
+    p.d_mac_jobs = reinterpret_cast<uint4*>(d + b_pairs + b_jobs);
+    p.d_plist = reinterpret_cast<uint32_t*>(d + b_pairs + b_jobs + b_mac);
+    for (int k = 0; k < NPHASE; ++k) { p.job_off[k] = T.job_off[k]; p.job_cnt[k] = T.job_cnt[k]; }
+    p.nops = (uint32_t)ops.size();
+    p.ops = ops;
+    p.pairs_host = T.pairs;
+}
+
+std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words) {
+    if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
+    auto plan = std::make_unique<Plan>();
+    plan->dc = c.dev();
+    plan->logn = c.logn();
+    size_t need = 0;
+    for (const Op& op : ops) { validate(c, op); need += op_workspace_words(c, op.L); }
+    if (!ws) {
+        if (cudaMalloc(&plan->ws, std::max<size_t>(need, 1) * 8) != cudaSuccess)
+            throw std::runtime_error("workspace allocation failed");
+        plan->own_ws = true;
+        ws = plan->ws;
+    } else if (ws_words < need) {
+        throw std::length_error("workspace too small");
+    }
+    plan->ws_words = need;
+    std::vector<u64*> wsp(ops.size());
+    size_t off = 0;
+    for (size_t i = 0; i < ops.size(); ++i) { wsp[i] = ws + off; off += op_workspace_words(c, ops[i].L); }
+    HostTables T;
+    fill_tables(c, ops, wsp, T);
+    commit(*plan, T, ops, 0, false);
     return plan;
+}
+
+void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops, const std::vector<u64*>& ws_ptrs,
+                     cudaStream_t s) {
+    if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
+    if (ws_ptrs.size() != ops.size()) throw std::invalid_argument("one workspace per operation");
+    for (const Op& op : ops) validate(c, op);
+    p.dc = c.dev();
+    p.logn = c.logn();
+    HostTables& T = *p.staging;
+    fill_tables(c, ops, ws_ptrs, T);
+    commit(p, T, ops, s, true);
 }
 
 namespace {

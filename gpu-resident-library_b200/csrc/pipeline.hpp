@@ -18,7 +18,10 @@ struct Op {
     u64* out[2] = {nullptr, nullptr};
 };
 
+struct HostTables;
+
 struct Plan {
+    Plan();
     DevCtx dc{};
     uint32_t logn = 0, nops = 0;
     PairDesc* d_pairs = nullptr;
@@ -32,6 +35,10 @@ struct Plan {
     bool own_ws = false;
     std::vector<Op> ops;      // host copy (device pointers and levels)
     std::vector<PairDesc> pairs_host;
+    void* d_blob = nullptr;            // device tables (pairs, jobs, P5 groups, pair lists)
+    void* h_blob = nullptr;            // pinned host mirror of d_blob
+    size_t blob_cap = 0;
+    std::unique_ptr<HostTables> staging;
     ~Plan();
 };
 
@@ -40,6 +47,12 @@ size_t op_workspace_words(const gfx::Context& c, uint32_t L);
 void validate(const gfx::Context& c, const Op& op);
 // ws == nullptr: the plan allocates (and owns) its workspace.
 std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words);
+// Rebuilds `p` in place for a new batch (one workspace pointer per op),
+// reusing its buffers when large enough; the tables are uploaded with one
+// cudaMemcpyAsync on `s` from the plan's pinned mirror, so the host must not
+// rebuild `p` again before work queued on `s` has consumed them.
+void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops, const std::vector<u64*>& ws_ptrs,
+                     cudaStream_t s);
 // mask selects phases P1..P9 (bit k = phase k+1); 0x1ff runs the whole batch.
 cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
 constexpr int MAC_MAX_DNUM = 16;

@@ -59,6 +59,16 @@ _API: dict = {
     "gpufhe_rescale_consts": (I32, [VP, VP, VP, U32]),
     "gpufhe_rescale_noalloc": (I32, [VP, U32, VP, VP]),
     "gpufhe_rescale_noalloc_max_words": (U64, []),
+    "gpufhe_server_create": (I32, [VP, U32, U64, U32, U32, I32, C.POINTER(VP)]),
+    "gpufhe_server_destroy": (None, [VP]),
+    "gpufhe_server_request_bytes": (U64, [VP, U32, U32]),
+    "gpufhe_server_submit": (I32, [VP, U32, U32, VP, U32, DBL, U64, VP, VP, C.POINTER(U64)]),
+    "gpufhe_server_start": (I32, [VP]),
+    "gpufhe_server_step": (I32, [VP, C.POINTER(U32)]),
+    "gpufhe_server_drain": (I32, [VP, DBL]),
+    "gpufhe_server_pending": (U64, [VP]),
+    "gpufhe_server_get_stats": (I32, [VP, VP]),
+    "gpufhe_server_records": (I32, [VP, VP, U32, C.POINTER(U32)]),
 }
 
 EVALMULT_RESCALE, KEYSWITCH, ROTATE, RESCALE = 0, 1, 2, 3
@@ -197,6 +207,93 @@ class Plan:
         if getattr(self, "h", None):
             lib().gpufhe_plan_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ReqOp(C.Structure):
+    """struct gpufhe_req_op (include/gpufhe_b200.h)."""
+    _fields_ = [("mode", U32), ("reserved", U32), ("galois", U64)]
+
+
+class ServerStats(C.Structure):
+    """struct gpufhe_server_stats."""
+    _fields_ = [("steps", U64), ("ops", U64), ("emr_ops", U64), ("completed", U64), ("peak_active", U64),
+                ("max_batch", U64), ("peak_bytes", U64), ("arena_bytes", U64), ("resident_bytes", U64),
+                ("busy_s", DBL)]
+
+
+class RequestRecord(C.Structure):
+    """struct gpufhe_request_record."""
+    _fields_ = [("id", U64), ("ctx", U32), ("start_level", U32), ("final_level", U32), ("nops", U32),
+                ("t_arrival", DBL), ("t_admit", DBL), ("t_finish", DBL)]
+
+
+class Server:
+    """Continuous-batching server over contexts of one device (gpufhe_server_*)."""
+
+    def __init__(self, ctxs, budget_bytes, max_active=0, batch_cap=0, plain=False):
+        self._ctxs = list(ctxs)          # keep the contexts alive
+        arr = (VP * len(self._ctxs))(*[c.h.value for c in self._ctxs])
+        h = VP()
+        check(lib().gpufhe_server_create(arr, len(self._ctxs), int(budget_bytes), max_active, batch_cap,
+                                         1 if plain else 0, C.byref(h)))
+        self.h = h
+        self._keep = []                  # host buffers referenced by queued requests
+
+    def request_bytes(self, ctx, level):
+        return int(lib().gpufhe_server_request_bytes(self.h, ctx, level))
+
+    def submit(self, ctx, level, ops, arrival_s=0.0, seed=0, h_in=None, h_out=None):
+        """ops: list of (mode, galois). h_in / h_out: host numpy uint64 arrays or None."""
+        arr = (ReqOp * max(1, len(ops)))()
+        for i, (m, g) in enumerate(ops):
+            arr[i].mode, arr[i].galois = m, g
+        if h_in is not None:
+            self._keep.append(h_in)
+        if h_out is not None:
+            self._keep.append(h_out)
+        rid = U64()
+        check(lib().gpufhe_server_submit(self.h, ctx, level, C.cast(arr, VP), len(ops), float(arrival_s), seed,
+                                         None if h_in is None else h_in.ctypes.data,
+                                         None if h_out is None else h_out.ctypes.data, C.byref(rid)))
+        return rid.value
+
+    def start(self):
+        check(lib().gpufhe_server_start(self.h))
+
+    def step(self):
+        q = U32()
+        check(lib().gpufhe_server_step(self.h, C.byref(q)))
+        return q.value
+
+    def drain(self, max_seconds=600.0):
+        check(lib().gpufhe_server_drain(self.h, float(max_seconds)))
+
+    def pending(self):
+        return int(lib().gpufhe_server_pending(self.h))
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().gpufhe_server_get_stats(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def records(self):
+        cnt = U32()
+        check(lib().gpufhe_server_records(self.h, None, 0, C.byref(cnt)))
+        arr = (RequestRecord * max(1, cnt.value))()
+        check(lib().gpufhe_server_records(self.h, C.cast(arr, VP), cnt.value, C.byref(cnt)))
+        return [{k: getattr(arr[i], k) for k, _ in RequestRecord._fields_} for i in range(cnt.value)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpufhe_server_destroy(self.h)
+            self.h = None
+        self._keep = []
 
     def __del__(self):
         try:

@@ -107,11 +107,11 @@ uint64_t gpufhe_op_workspace_bytes(gpufhe_ctx* ctx, uint32_t level);
  * d_ws: caller workspace of ws_bytes, or NULL for a plan-owned one. */
 int  gpufhe_plan_create(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, uint64_t* d_ws, uint64_t ws_bytes,
                         gpufhe_plan** out);
-/* Launches the seven phase kernels for the whole batch on `stream`
+/* Launches the nine phase kernels for the whole batch on `stream`
  * (kernel launches only: capturable in a CUDA graph). */
 int  gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t stream);
 void gpufhe_plan_destroy(gpufhe_plan* plan);
-/* One phase (0..6 = K1..K7) only, for per-kernel timing. */
+/* One phase (0..8 = P1..P9) only, for per-kernel timing. */
 int  gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t stream);
 /* Number of kernels one gpufhe_plan_launch enqueues. */
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
@@ -140,6 +140,71 @@ int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaSt
  * overlap on the GPU race. */
 int      gpufhe_rescale_noalloc(gpufhe_ctx* ctx, uint32_t level, uint64_t* d_comp, cudaStream_t stream);
 uint64_t gpufhe_rescale_noalloc_max_words(void);
+
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference (its multi-ciphertext driver runs chains on
+ * separate streams, bench/bench_batch.cpp:95-105). A continuous-batching
+ * server over one or more contexts (ring sizes) on one device. A request is
+ * a chain of EvalMult+Rescale (the ciphertext times itself) and rotation
+ * operations on one ciphertext. Each step queues the next operation of every
+ * admitted request as one batched plan per context; two steps stay in
+ * flight. Requests are admitted FIFO, once arrived, while the device arena
+ * (budget_bytes minus the contexts' resident tables and keys) has room for
+ * two ciphertexts at their start level plus their workspace; a request's
+ * memory returns to the arena when the step finishing it completes.
+ * max_active caps admitted requests (0 = budget only); batch_cap caps the
+ * operations of one plan (0 = none); plain != 0 runs one request at a time
+ * (the plain one-chain-at-a-time form). */
+typedef struct gpufhe_server gpufhe_server;
+
+typedef struct gpufhe_req_op {
+    uint32_t mode;      /* GPUFHE_EVALMULT_RESCALE or GPUFHE_ROTATE */
+    uint32_t reserved;
+    uint64_t galois;    /* GPUFHE_ROTATE: Galois element, also the key id */
+} gpufhe_req_op;
+
+typedef struct gpufhe_server_stats {
+    uint64_t steps, ops, emr_ops, completed, peak_active, max_batch;
+    uint64_t peak_bytes;       /* most arena bytes in use */
+    uint64_t arena_bytes;      /* arena capacity */
+    uint64_t resident_bytes;   /* tables + keys of every context */
+    double busy_s;             /* first admission to last completion */
+} gpufhe_server_stats;
+
+typedef struct gpufhe_request_record {
+    uint64_t id;
+    uint32_t ctx, start_level, final_level, nops;
+    /* seconds since the epoch (gpufhe_server_start); t_finish is the device
+     * time at which the step holding the request's last operation completed */
+    double t_arrival, t_admit, t_finish;
+} gpufhe_request_record;
+
+int      gpufhe_server_create(gpufhe_ctx* const* ctxs, uint32_t nctx, uint64_t budget_bytes, uint32_t max_active,
+                              uint32_t batch_cap, int plain, gpufhe_server** out);
+void     gpufhe_server_destroy(gpufhe_server* srv);
+/* Arena bytes one request of context ctx starting at `level` holds. */
+uint64_t gpufhe_server_request_bytes(gpufhe_server* srv, uint32_t ctx, uint32_t level);
+/* Queues a request that arrives arrival_s seconds after the epoch. h_in:
+ * host ciphertext [2][level][n] uploaded on admission, or NULL for seeded
+ * residues generated on the device (SplitMix64 of seed, component, tower,
+ * index). h_out: host buffer [2][final level][n] that receives the result,
+ * or NULL. Pinned host buffers keep the copies asynchronous. GPUFHE_EINVAL
+ * for an invalid chain (EvalMult+Rescale below level 2, a missing key),
+ * GPUFHE_ENOMEM for a request larger than the whole arena. */
+int      gpufhe_server_submit(gpufhe_server* srv, uint32_t ctx, uint32_t level, const gpufhe_req_op* ops,
+                              uint32_t nops, double arrival_s, uint64_t seed, const uint64_t* h_in, uint64_t* h_out,
+                              uint64_t* id);
+/* Sets the epoch to now. */
+int      gpufhe_server_start(gpufhe_server* srv);
+/* One scheduling step; *queued = operations queued (0 when idle). */
+int      gpufhe_server_step(gpufhe_server* srv, uint32_t* queued);
+/* Steps until every request finished; GPUFHE_ETIMEOUT after max_seconds. */
+int      gpufhe_server_drain(gpufhe_server* srv, double max_seconds);
+uint64_t gpufhe_server_pending(gpufhe_server* srv);
+int      gpufhe_server_get_stats(gpufhe_server* srv, gpufhe_server_stats* out);
+/* Finished requests in completion order: *count = how many finished; up to
+ * cap records are written to out (out may be NULL to ask for the count). */
+int      gpufhe_server_records(gpufhe_server* srv, gpufhe_request_record* out, uint32_t cap, uint32_t* count);
 
 #ifdef __cplusplus
 }
