@@ -60,9 +60,9 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def workload_levels(seed):
+def workload_levels(seed, count=PAIRS):
     rng = np.random.default_rng(seed)
-    return [int(x) for x in rng.integers(LEVEL_RANGE[0], LEVEL_RANGE[1] + 1, PAIRS)]
+    return [int(x) for x in rng.integers(LEVEL_RANGE[0], LEVEL_RANGE[1] + 1, count)]
 
 
 def chain(primes_fn, n):
@@ -367,7 +367,8 @@ def run_gpu(args):
     av = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
     bv = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
     ctx.set_key(0, av, bv)
-    levels = workload_levels(SEED + rank)
+    pairs = args.pairs
+    levels = workload_levels(SEED + rank, pairs)
     gen = torch.Generator(device=dev)
     gen.manual_seed(SEED + rank)
 
@@ -418,7 +419,7 @@ def run_gpu(args):
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     ms_step = ms / args.steps
-    value = world * PAIRS * args.steps / (ms * 1e-3)
+    value = world * pairs * args.steps / (ms * 1e-3)
 
     # per-phase device times (outside the timed region)
     cur = torch.cuda.current_stream().cuda_stream
@@ -456,7 +457,7 @@ def run_gpu(args):
     b.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(a.elapsed_time(b) / e2e_steps, dist, dev)
-    e2e_value = world * PAIRS / (e2e_ms * 1e-3)
+    e2e_value = world * pairs / (e2e_ms * 1e-3)
 
     # plain per-chain form: one pair per plan, graph per chain, 16 streams
     plain = None
@@ -492,38 +493,78 @@ def run_gpu(args):
         b.record()
         torch.cuda.synchronize()
         pms = a.elapsed_time(b) / reps
-        plain = {"value": PAIRS / (pms * 1e-3), "unit": "ops/s", "ms_per_step": pms,
-                 "form": "one pair per launch set (9 kernels), CUDA graph per chain, 16 streams"}
+        # one chain at a time: every chain's graph on one stream
+        g1 = pgraphs[0][1]
+        def plain_one():
+            with torch.cuda.stream(g1):
+                for g, _ in pgraphs:
+                    g.replay()
+        plain_one()
+        torch.cuda.synchronize()
+        a.record(g1)
+        for _ in range(reps):
+            plain_one()
+        b.record(g1)
+        torch.cuda.synchronize()
+        p1ms = a.elapsed_time(b) / reps
+        plain = {"value": pairs / (p1ms * 1e-3), "unit": "ops/s", "ms_per_step": p1ms,
+                 "form": "one chain at a time: one pair per launch set (9 kernels), a CUDA graph per chain, "
+                         "replayed in turn on one stream",
+                 "streams16": {"value": pairs / (pms * 1e-3), "ms_per_step": pms,
+                               "form": "the same per-chain graphs spread over 16 streams"}}
         del pgraphs, pplans
 
     # config-2 NTT kernel isolation: 64 polys x 12 towers x 2^16
     ntt = None
     if not args.no_ntt:
         npol, tw = 64, 12
+        Q2 = G.native_primes(tw, 50, n)            # twelve 50-bit primes = 1 mod 2^17
+        ctx2 = G.Context(n, Q2, G.native_primes(1, 60, n, avoid=list(Q2)), 1, device=local)
         data = torch.empty(npol * tw * n, dtype=torch.int64, device=dev)
         for t_ in range(tw):
-            data.view(npol, tw, n)[:, t_, :].random_(0, int(Q[t_]), generator=gen)
+            data.view(npol, tw, n)[:, t_, :].random_(0, int(Q2[t_]), generator=gen)
         jb = int(G.lib().gpufhe_ntt_job_bytes())
         jf = torch.empty(npol * tw * jb // 8, dtype=torch.int64, device=dev)
         ji = torch.empty_like(jf)
-        G.check(G.lib().gpufhe_ntt_batch(ctx.h, data.data_ptr(), npol, tw, 0, 0, jf.data_ptr(), cur))
-        G.check(G.lib().gpufhe_ntt_batch(ctx.h, data.data_ptr(), npol, tw, 0, 1, ji.data_ptr(), cur))
+        G.check(G.lib().gpufhe_ntt_batch(ctx2.h, data.data_ptr(), npol, tw, 0, 0, jf.data_ptr(), cur))
+        G.check(G.lib().gpufhe_ntt_batch(ctx2.h, data.data_ptr(), npol, tw, 0, 1, ji.data_ptr(), cur))
         torch.cuda.synchronize()
         res = {}
         for name, inv, jt in (("fwd", 0, jf), ("inv", 1, ji)):
             for _ in range(3):
-                G.lib().gpufhe_ntt_run_jobs(ctx.h, jt.data_ptr(), npol * tw, inv, cur)
+                G.lib().gpufhe_ntt_run_jobs(ctx2.h, jt.data_ptr(), npol * tw, inv, cur)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             for _ in range(10):
-                G.lib().gpufhe_ntt_run_jobs(ctx.h, jt.data_ptr(), npol * tw, inv, cur)
+                G.lib().gpufhe_ntt_run_jobs(ctx2.h, jt.data_ptr(), npol * tw, inv, cur)
             b.record()
             torch.cuda.synchronize()
             t_ms = a.elapsed_time(b) / 10
             gbs = 2 * 8 * n * npol * tw / (t_ms * 1e-3) / 1e9
-            res[name] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"]}
-        ntt = {"workload": "64 polys x 12 towers x 2^16, 50-bit primes", "bytes_per_tower": 2 * 8 * n, **res}
-        del data
+            res[name] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"],
+                         "tbfly_per_s": npol * tw * (n // 2) * N_LOG / (t_ms * 1e-3) / 1e12}
+        # RNS multiply out = a * b over the same batch (3 words moved per coefficient)
+        other = torch.empty_like(data)
+        for t_ in range(tw):
+            other.view(npol, tw, n)[:, t_, :].random_(0, int(Q2[t_]), generator=gen)
+        prod = torch.empty_like(data)
+        mul = lambda: G.check(G.lib().gpufhe_rns_mult_batch(ctx2.h, data.data_ptr(), other.data_ptr(),
+                                                            prod.data_ptr(), npol, tw, 0, cur))
+        for _ in range(3):
+            mul()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(10):
+            mul()
+        b.record()
+        torch.cuda.synchronize()
+        t_ms = a.elapsed_time(b) / 10
+        gbs = 3 * 8 * n * npol * tw / (t_ms * 1e-3) / 1e9
+        res["rns_mult"] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"]}
+        ntt = {"workload": "64 polys x 12 towers x 2^16, 50-bit primes", "bytes_per_tower_transform": 2 * 8 * n,
+               "bytes_per_tower_mult": 3 * 8 * n, **res}
+        del data, other, prod
+        ctx2.close()
 
     # serving trace (continuous batching vs one request at a time)
     serving = None
@@ -552,7 +593,8 @@ def run_gpu(args):
         "metric": METRIC, "value": value, "unit": "ops/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform residues and key)",
-        "config": {"workload": WORKLOAD, "n": n, "pairs_per_gpu": PAIRS, "levels": "U{4..12} seeded",
+        "config": {"workload": WORKLOAD if pairs == PAIRS else f"profiling case: {pairs} pairs of " + WORKLOAD,
+                   "n": n, "pairs_per_gpu": pairs, "levels": "U{4..12} seeded",
                    "mean_level": float(np.mean(levels)), "l2": "inputs larger than L2 (no flush)",
                    "graph": f"{kernels_per_step} kernels per step, one CUDA graph"},
         "roofline": {"bound": "hbm", "kernel": "fused EvalMult+Rescale step (phases P1..P9)", "achieved": achieved,
@@ -563,6 +605,7 @@ def run_gpu(args):
                 "ms_per_step": e2e_ms},
         "plain": plain,
         "served_vs_plain": (value / world / plain["value"]) if plain else None,
+        "served_vs_plain_16streams": (value / world / plain["streams16"]["value"]) if plain else None,
         "latency_ms": (dict(serving["served"]["latency_ms"], source="serving trace, served form") if serving
                        else {"p50": ms_step, "p99": ms_step, "source": "whole batch per step"}),
         "ntt_kernel_isolation": ntt,
@@ -585,6 +628,7 @@ def main():
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--pairs", type=int, default=PAIRS, help="pairs per step (smaller only for profiling)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -11,6 +11,40 @@ using gfx::Context;
 
 struct gpufhe_ctx { Context* c; };
 
+namespace {
+
+// out = a * b mod q_t over [poly][tower][n] (plain residues in and out, the
+// result LaunchRNSMultTower gives, rns_arith.cu:13-56). One block covers
+// MUL_CHUNK words of one tower; each thread loads all its 16-byte pairs
+// before it computes, so every thread has four loads of each operand in flight.
+constexpr int MUL_NT = 256, MUL_VEC = 4, MUL_CHUNK = MUL_NT * 2 * MUL_VEC;
+
+__global__ void __launch_bounds__(MUL_NT) k_rns_mult_batch(const u64* __restrict__ a, const u64* __restrict__ b,
+                                                           u64* __restrict__ out, const ModC* __restrict__ mod,
+                                                           uint32_t towers, uint32_t first, uint32_t n) {
+    const size_t base = (size_t)blockIdx.x * MUL_CHUNK;
+    const uint32_t t = (uint32_t)((base / n) % towers);
+    const ModC m = mod[first + t];
+    const ulonglong2* A = reinterpret_cast<const ulonglong2*>(a + base);
+    const ulonglong2* B = reinterpret_cast<const ulonglong2*>(b + base);
+    ulonglong2* O = reinterpret_cast<ulonglong2*>(out + base);
+    ulonglong2 x[MUL_VEC], y[MUL_VEC];
+#pragma unroll
+    for (int k = 0; k < MUL_VEC; ++k) {
+        x[k] = __ldcs(A + threadIdx.x + k * MUL_NT);
+        y[k] = __ldcs(B + threadIdx.x + k * MUL_NT);
+    }
+#pragma unroll
+    for (int k = 0; k < MUL_VEC; ++k) {
+        ulonglong2 r;
+        r.x = mulmod(x[k].x, y[k].x, m);
+        r.y = mulmod(x[k].y, y[k].y, m);
+        __stcs(O + threadIdx.x + k * MUL_NT, r);
+    }
+}
+
+}  // namespace
+
 #define GPUFHE_TRY(...)                                          \
     try { __VA_ARGS__ } catch (const std::invalid_argument& e) {        \
         gfx::set_error(e.what()); return GPUFHE_EINVAL;          \
@@ -96,6 +130,26 @@ int gpufhe_ntt_batch(gpufhe_ctx* h, uint64_t* d_data, uint32_t npolys, uint32_t 
 }
 
 uint64_t gpufhe_ntt_job_bytes(void) { return sizeof(xf::Job); }
+
+int gpufhe_rns_mult_batch(gpufhe_ctx* h, const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_out, uint32_t npolys,
+                          uint32_t towers, uint32_t first_tower, cudaStream_t s) {
+    if (!h || !d_a || !d_b || !d_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    Context* c = h->c;
+    if (first_tower + towers > c->fullQ() + c->K() || !towers) { gfx::set_error("tower range"); return GPUFHE_EINVAL; }
+    const uint32_t n = c->n();
+    if (n % MUL_CHUNK) { gfx::set_error("gpufhe_rns_mult_batch needs n >= 2048"); return GPUFHE_EINVAL; }
+    if ((reinterpret_cast<uintptr_t>(d_a) | reinterpret_cast<uintptr_t>(d_b) | reinterpret_cast<uintptr_t>(d_out)) & 15) {
+        gfx::set_error("gpufhe_rns_mult_batch needs 16-byte aligned buffers");
+        return GPUFHE_EINVAL;
+    }
+    const size_t words = (size_t)npolys * towers * n;
+    if (!words) return GPUFHE_OK;
+    k_rns_mult_batch<<<(unsigned)(words / MUL_CHUNK), MUL_NT, 0, s>>>(d_a, d_b, d_out, c->dev().mod, towers,
+                                                                     first_tower, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
+}
 
 int gpufhe_ntt_run_jobs(gpufhe_ctx* h, const uint64_t* d_jobs, uint32_t njobs, int inverse, cudaStream_t s) {
     if (!h || !d_jobs) return GPUFHE_EINVAL;

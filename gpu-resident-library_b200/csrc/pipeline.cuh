@@ -229,12 +229,21 @@ p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
 // shared memory once, then for each listed pair accumulates
 //   res_c = sum_p digit_p * key_p   (128-bit, one Barrett at the end)
 // over that pair's digits and writes the epilogue for its QlP position.
+// A thread owns MAC_TILE / MAC_NT elements as 16-byte pairs; for each pair it
+// issues every load first (the pair's own-digit source and, for
+// EvalMult+Rescale, the four tensor inputs; then the digits in chunks of
+// MAC_PCH) so that many loads are in flight before the first multiply.
+constexpr int MAC_PCH = 4;
+
+__device__ __forceinline__ u64 v2get(const ulonglong2& v, int j) { return j ? v.y : v.x; }
+__device__ __forceinline__ void v2set(ulonglong2& v, int j, u64 x) { if (j) v.y = x; else v.x = x; }
+
 template <int LOGN>
 __global__ void __launch_bounds__(MAC_NT)
 p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
        const u32* __restrict__ plist) {
     constexpr int TILES = (1 << LOGN) / MAC_TILE;
-    constexpr int EPT = MAC_TILE / MAC_NT;
+    constexpr int NV = MAC_TILE / (2 * MAC_NT);   // 16-byte vectors per thread
     extern __shared__ __align__(16) u64 sm[];     // [dnum][2][MAC_TILE]
     const uint4 jb = jobs[blockIdx.x / TILES];
     const u32 tile0 = (blockIdx.x % TILES) * MAC_TILE;
@@ -243,89 +252,159 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
     const u32 dnum = D.dnum;
     // every listed pair uses the same key (checked on the host)
     const PairDesc& P0 = pairs[plist[jb.y]];
-    for (u32 k = threadIdx.x; k < dnum * MAC_TILE; k += MAC_NT) {
-        const u32 p = k / MAC_TILE, e = k % MAC_TILE;
+    for (u32 k = threadIdx.x; k < dnum * (MAC_TILE / 2); k += MAC_NT) {
+        const u32 p = k / (MAC_TILE / 2), e = 2 * (k % (MAC_TILE / 2));
         const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0 + e;
-        sm[(2 * p) * MAC_TILE + e] = P0.kbv[off];
-        sm[(2 * p + 1) * MAC_TILE + e] = P0.kav[off];
+        *reinterpret_cast<ulonglong2*>(sm + (2 * p) * MAC_TILE + e) = *reinterpret_cast<const ulonglong2*>(P0.kbv + off);
+        *reinterpret_cast<ulonglong2*>(sm + (2 * p + 1) * MAC_TILE + e) =
+            *reinterpret_cast<const ulonglong2*>(P0.kav + off);
     }
     __syncthreads();
     const bool is_p = r >= D.fullQ;
+    const u64 q = m.q;
     for (u32 g = 0; g < jb.z; ++g) {
         const PairDesc& P = pairs[plist[jb.y + g]];
         const u32 L = P.L, K = D.K, QlP = L + K;
         const u32 i = is_p ? L + (r - D.fullQ) : r;       // QlP position of row r
         const Level& lv = D.lvl[L];
         const WsLayout w = ws_layout(L, K, D.alpha);
-        u64 a0l[EPT], a0h[EPT], a1l[EPT], a1h[EPT];
+        const u32 nparts = lv.nparts;
+        const u32 pin = is_p ? 0xffffffffu : i / D.alpha; // digit holding tower i
+        const bool emr = P.mode == EMR;
+        const size_t o = ((size_t)i << LOGN) + tile0;
+        // own-digit source s (eval form) and, for EvalMult+Rescale, tensor t0, t1
+        ulonglong2 s[NV], t0[NV], t1[NV];
+        if (!is_p) {
+            if (emr) {
+                ulonglong2 x0[NV], x1[NV], y0[NV], y1[NV];
 #pragma unroll
-        for (int k = 0; k < EPT; ++k) a0l[k] = a0h[k] = a1l[k] = a1h[k] = 0;
-        for (u32 p = 0; p < lv.nparts; ++p) {
-            const u32 st0 = lv.part_st[p], sp = lv.part_sp[p];
-            const bool in_range = !is_p && i >= st0 && i < st0 + sp;
-            const u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + tile0;
-            const u64* kb = sm + (2 * p) * MAC_TILE;
-            const u64* ka = sm + (2 * p + 1) * MAC_TILE;
+                for (int k = 0; k < NV; ++k) {
+                    const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                    x0[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + e);
+                    x1[k] = *reinterpret_cast<const ulonglong2*>(P.in[1] + o + e);
+                    y0[k] = *reinterpret_cast<const ulonglong2*>(P.in[2] + o + e);
+                    y1[k] = *reinterpret_cast<const ulonglong2*>(P.in[3] + o + e);
+                }
 #pragma unroll
-            for (int k = 0; k < EPT; ++k) {
-                const u32 e = threadIdx.x + k * MAC_NT;
-                const u64 v = in_range ? digit_src<LOGN>(P, i, tile0 + e, m) : Y[e];
-                mac_wide(a0l[k], a0h[k], v, kb[e]);
-                mac_wide(a1l[k], a1h[k], v, ka[e]);
+                for (int k = 0; k < NV; ++k)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const u64 a0 = v2get(x0[k], j), a1 = v2get(x1[k], j);
+                        const u64 b0 = v2get(y0[k], j), b1 = v2get(y1[k], j);
+                        v2set(s[k], j, mulmod(a1, b1, m));
+                        v2set(t0[k], j, mulmod(a0, b0, m));
+                        u64 lo, hi;
+                        mul_wide(a0, b1, lo, hi);
+                        mac_wide(lo, hi, a1, b0);
+                        v2set(t1[k], j, barrett(lo, hi, m));
+                    }
+            } else if (P.mode == ROT) {
+                const u64* src = P.in[1] + ((size_t)i << LOGN);
+#pragma unroll
+                for (int k = 0; k < NV; ++k)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j)
+                        v2set(s[k], j, src[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * MAC_NT) + j, P.galois)]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < NV; ++k)
+                    s[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + 2 * (threadIdx.x + k * MAC_NT));
             }
         }
-        u64 r0[EPT], r1[EPT];
+        u64 a0l[2 * NV], a0h[2 * NV], a1l[2 * NV], a1h[2 * NV];
 #pragma unroll
-        for (int k = 0; k < EPT; ++k) {
-            r0[k] = barrett(a0l[k], a0h[k], m);
-            r1[k] = barrett(a1l[k], a1h[k], m);
+        for (int k = 0; k < 2 * NV; ++k) a0l[k] = a0h[k] = a1l[k] = a1h[k] = 0;
+        for (u32 p0 = 0; p0 < nparts; p0 += MAC_PCH) {
+            ulonglong2 v[MAC_PCH][NV];
+#pragma unroll
+            for (int pp = 0; pp < MAC_PCH; ++pp) {
+                const u32 p = p0 + pp;
+                if (p < nparts && p != pin) {
+                    const ulonglong2* Y =
+                        reinterpret_cast<const ulonglong2*>(slot_ptr(P, w.Y + p * QlP + i, LOGN) + tile0);
+#pragma unroll
+                    for (int k = 0; k < NV; ++k) v[pp][k] = __ldcs(Y + threadIdx.x + k * MAC_NT);
+                }
+            }
+#pragma unroll
+            for (int pp = 0; pp < MAC_PCH; ++pp) {
+                const u32 p = p0 + pp;
+                if (p >= nparts) break;
+                const u64* kb = sm + (2 * p) * MAC_TILE;
+                const u64* ka = sm + (2 * p + 1) * MAC_TILE;
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                    const ulonglong2 kbv = *reinterpret_cast<const ulonglong2*>(kb + e);
+                    const ulonglong2 kav = *reinterpret_cast<const ulonglong2*>(ka + e);
+                    const ulonglong2 dv = p == pin ? s[k] : v[pp][k];
+                    mac_wide(a0l[2 * k], a0h[2 * k], dv.x, kbv.x);
+                    mac_wide(a0l[2 * k + 1], a0h[2 * k + 1], dv.y, kbv.y);
+                    mac_wide(a1l[2 * k], a1h[2 * k], dv.x, kav.x);
+                    mac_wide(a1l[2 * k + 1], a1h[2 * k + 1], dv.y, kav.y);
+                }
+            }
         }
-        const u64 q = m.q;
+        ulonglong2 r0[NV], r1[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                v2set(r0[k], j, barrett(a0l[2 * k + j], a0h[2 * k + j], m));
+                v2set(r1[k], j, barrett(a1l[2 * k + j], a1h[2 * k + j], m));
+            }
         u64 *d0, *d1;
         if (is_p) {
             d0 = slot_ptr(P, w.RP + (i - L), LOGN) + tile0;
             d1 = slot_ptr(P, w.RP + K + (i - L), LOGN) + tile0;
 #pragma unroll
-            for (int k = 0; k < EPT; ++k) {
-                const u32 e = threadIdx.x + k * MAC_NT;
-                d0[e] = r0[k];
-                d1[e] = r1[k];
+            for (int k = 0; k < NV; ++k) {
+                const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                *reinterpret_cast<ulonglong2*>(d0 + e) = r0[k];
+                *reinterpret_cast<ulonglong2*>(d1 + e) = r1[k];
             }
             continue;
         }
         const u64 pv = D.pinv[i], pvp = D.pinvp[i];
-        if (P.mode != EMR) {   // keyswitch / rotation: W = res * P^-1
+        if (!emr) {   // keyswitch / rotation: W = res * P^-1
             d0 = slot_ptr(P, w.W + i, LOGN) + tile0;
             d1 = slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
-            for (int k = 0; k < EPT; ++k) {
-                const u32 e = threadIdx.x + k * MAC_NT;
-                d0[e] = shoup(r0[k], pv, pvp, q);
-                d1[e] = shoup(r1[k], pv, pvp, q);
+            for (int k = 0; k < NV; ++k) {
+                const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                ulonglong2 o0, o1;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    v2set(o0, j, shoup(v2get(r0[k], j), pv, pvp, q));
+                    v2set(o1, j, shoup(v2get(r1[k], j), pv, pvp, q));
+                }
+                *reinterpret_cast<ulonglong2*>(d0 + e) = o0;
+                *reinterpret_cast<ulonglong2*>(d1 + e) = o1;
             }
             continue;
         }
-        const size_t o = ((size_t)i << LOGN) + tile0;
         const bool drop = i == L - 1;
         const u64 s1 = lv.s1[i], s1p = lv.s1p[i], ps1 = lv.ps1[i], ps1p = lv.ps1p[i];
         d0 = drop ? slot_ptr(P, w.U, LOGN) + tile0 : slot_ptr(P, w.W + i, LOGN) + tile0;
         d1 = drop ? slot_ptr(P, w.U + 1, LOGN) + tile0 : slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
-        for (int k = 0; k < EPT; ++k) {
-            const u32 e = threadIdx.x + k * MAC_NT;
-            const u64 x0 = P.in[0][o + e], x1 = P.in[1][o + e], y0 = P.in[2][o + e], y1 = P.in[3][o + e];
-            const u64 t0 = mulmod(x0, y0, m);
-            u64 lo, hi;
-            mul_wide(x0, y1, lo, hi);
-            mac_wide(lo, hi, x1, y0);
-            const u64 t1 = barrett(lo, hi, m);
-            if (drop) {   // u = t + res * P^-1 (eval), INTT'd in P6/P7
-                d0[e] = csub(t0 + shoup(r0[k], pv, pvp, q), q);
-                d1[e] = csub(t1 + shoup(r1[k], pv, pvp, q), q);
-            } else {      // W = t*s1 + res*P^-1*s1
-                d0[e] = csub(csub(shoup_lazy(t0, s1, s1p, q) + shoup_lazy(r0[k], ps1, ps1p, q), m.two_q), q);
-                d1[e] = csub(csub(shoup_lazy(t1, s1, s1p, q) + shoup_lazy(r1[k], ps1, ps1p, q), m.two_q), q);
+        for (int k = 0; k < NV; ++k) {
+            const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+            ulonglong2 o0, o1;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const u64 ta = v2get(t0[k], j), tb = v2get(t1[k], j);
+                const u64 ra = v2get(r0[k], j), rb = v2get(r1[k], j);
+                if (drop) {   // u = t + res * P^-1 (eval), INTT'd in P6/P7
+                    v2set(o0, j, csub(ta + shoup(ra, pv, pvp, q), q));
+                    v2set(o1, j, csub(tb + shoup(rb, pv, pvp, q), q));
+                } else {      // W = t*s1 + res*P^-1*s1
+                    v2set(o0, j, csub(csub(shoup_lazy(ta, s1, s1p, q) + shoup_lazy(ra, ps1, ps1p, q), m.two_q), q));
+                    v2set(o1, j, csub(csub(shoup_lazy(tb, s1, s1p, q) + shoup_lazy(rb, ps1, ps1p, q), m.two_q), q));
+                }
             }
+            *reinterpret_cast<ulonglong2*>(d0 + e) = o0;
+            *reinterpret_cast<ulonglong2*>(d1 + e) = o1;
         }
     }
 }

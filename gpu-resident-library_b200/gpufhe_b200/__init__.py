@@ -46,6 +46,7 @@ _API: dict = {
     "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
     "gpufhe_ntt_job_bytes": (U64, []),
     "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),
+    "gpufhe_rns_mult_batch": (I32, [VP, VP, VP, VP, U32, U32, U32, VP]),
     "gpufhe_op_workspace_bytes": (U64, [VP, U32]),
     "gpufhe_plan_create": (I32, [VP, U32, VP, VP, U64, C.POINTER(VP)]),
     "gpufhe_plan_launch": (I32, [VP, VP]),

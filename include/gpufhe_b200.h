@@ -69,6 +69,12 @@ int gpufhe_ntt_batch(gpufhe_ctx* ctx, uint64_t* d_data, uint32_t npolys, uint32_
 uint64_t gpufhe_ntt_job_bytes(void);
 int gpufhe_ntt_run_jobs(gpufhe_ctx* ctx, const uint64_t* d_jobs, uint32_t njobs, int inverse,
                         cudaStream_t stream);
+/* Batched RNS multiply out = a * b mod q over [npolys][towers][n] (tower t
+ * uses modulus first_tower + t): plain residues in and out, the result of
+ * LaunchRNSMultTower (reference rns_arith.cu:13-56) for every tower in one
+ * launch. Buffers 16-byte aligned, n >= 2048; out may alias a or b. */
+int gpufhe_rns_mult_batch(gpufhe_ctx* ctx, const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_out,
+                          uint32_t npolys, uint32_t towers, uint32_t first_tower, cudaStream_t stream);
 
 
 /* ---------------------------------------------------------------- batched ops
