@@ -344,6 +344,60 @@ def run_reference(args):
     return 0
 
 
+def ntt_isolation(G, torch, dev, local, cur, gen):
+    """Forward / inverse NTT and RNS multiply over 64 polys x 12 towers x 2^16 (twelve 50-bit primes)."""
+    n = 1 << N_LOG
+    npol, tw = 64, 12
+    Q2 = G.native_primes(tw, 50, n)            # twelve 50-bit primes = 1 mod 2^17
+    ctx2 = G.Context(n, Q2, G.native_primes(1, 60, n, avoid=list(Q2)), 1, device=local)
+    data = torch.empty(npol * tw * n, dtype=torch.int64, device=dev)
+    for t_ in range(tw):
+        data.view(npol, tw, n)[:, t_, :].random_(0, int(Q2[t_]), generator=gen)
+    jb = int(G.lib().gpufhe_ntt_job_bytes())
+    jf = torch.empty(npol * tw * jb // 8, dtype=torch.int64, device=dev)
+    ji = torch.empty_like(jf)
+    G.check(G.lib().gpufhe_ntt_batch(ctx2.h, data.data_ptr(), npol, tw, 0, 0, jf.data_ptr(), cur))
+    G.check(G.lib().gpufhe_ntt_batch(ctx2.h, data.data_ptr(), npol, tw, 0, 1, ji.data_ptr(), cur))
+    torch.cuda.synchronize()
+    res = {}
+    for name, inv, jt in (("fwd", 0, jf), ("inv", 1, ji)):
+        for _ in range(3):
+            G.lib().gpufhe_ntt_run_jobs(ctx2.h, jt.data_ptr(), npol * tw, inv, cur)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(10):
+            G.lib().gpufhe_ntt_run_jobs(ctx2.h, jt.data_ptr(), npol * tw, inv, cur)
+        b.record()
+        torch.cuda.synchronize()
+        t_ms = a.elapsed_time(b) / 10
+        gbs = 2 * 8 * n * npol * tw / (t_ms * 1e-3) / 1e9
+        res[name] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"],
+                     "tbfly_per_s": npol * tw * (n // 2) * N_LOG / (t_ms * 1e-3) / 1e12}
+    # RNS multiply out = a * b over the same batch (3 words moved per coefficient)
+    other = torch.empty_like(data)
+    for t_ in range(tw):
+        other.view(npol, tw, n)[:, t_, :].random_(0, int(Q2[t_]), generator=gen)
+    prod = torch.empty_like(data)
+    mul = lambda: G.check(G.lib().gpufhe_rns_mult_batch(ctx2.h, data.data_ptr(), other.data_ptr(),
+                                                        prod.data_ptr(), npol, tw, 0, cur))
+    for _ in range(3):
+        mul()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(10):
+        mul()
+    b.record()
+    torch.cuda.synchronize()
+    t_ms = a.elapsed_time(b) / 10
+    gbs = 3 * 8 * n * npol * tw / (t_ms * 1e-3) / 1e9
+    res["rns_mult"] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"]}
+    ntt = {"workload": "64 polys x 12 towers x 2^16, 50-bit primes", "bytes_per_tower_transform": 2 * 8 * n,
+           "bytes_per_tower_mult": 3 * 8 * n, **res}
+    del data, other, prod
+    ctx2.close()
+    return ntt
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_gpu(args):
     import torch
@@ -358,6 +412,12 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
+    if args.section == "ntt":   # kernel isolation only (profiling and quick checks)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SEED)
+        res = ntt_isolation(G, torch, dev, local, torch.cuda.current_stream().cuda_stream, gen)
+        print(json.dumps({"section": "ntt", "ntt_kernel_isolation": res}), flush=True)
+        return 0
     n = 1 << N_LOG
     Q, P = chain(G.native_primes, n)
     ctx = G.Context(n, Q, P, ALPHA, device=local)
@@ -514,57 +574,8 @@ def run_gpu(args):
                                "form": "the same per-chain graphs spread over 16 streams"}}
         del pgraphs, pplans
 
-    # config-2 NTT kernel isolation: 64 polys x 12 towers x 2^16
-    ntt = None
-    if not args.no_ntt:
-        npol, tw = 64, 12
-        Q2 = G.native_primes(tw, 50, n)            # twelve 50-bit primes = 1 mod 2^17
-        ctx2 = G.Context(n, Q2, G.native_primes(1, 60, n, avoid=list(Q2)), 1, device=local)
-        data = torch.empty(npol * tw * n, dtype=torch.int64, device=dev)
-        for t_ in range(tw):
-            data.view(npol, tw, n)[:, t_, :].random_(0, int(Q2[t_]), generator=gen)
-        jb = int(G.lib().gpufhe_ntt_job_bytes())
-        jf = torch.empty(npol * tw * jb // 8, dtype=torch.int64, device=dev)
-        ji = torch.empty_like(jf)
-        G.check(G.lib().gpufhe_ntt_batch(ctx2.h, data.data_ptr(), npol, tw, 0, 0, jf.data_ptr(), cur))
-        G.check(G.lib().gpufhe_ntt_batch(ctx2.h, data.data_ptr(), npol, tw, 0, 1, ji.data_ptr(), cur))
-        torch.cuda.synchronize()
-        res = {}
-        for name, inv, jt in (("fwd", 0, jf), ("inv", 1, ji)):
-            for _ in range(3):
-                G.lib().gpufhe_ntt_run_jobs(ctx2.h, jt.data_ptr(), npol * tw, inv, cur)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            for _ in range(10):
-                G.lib().gpufhe_ntt_run_jobs(ctx2.h, jt.data_ptr(), npol * tw, inv, cur)
-            b.record()
-            torch.cuda.synchronize()
-            t_ms = a.elapsed_time(b) / 10
-            gbs = 2 * 8 * n * npol * tw / (t_ms * 1e-3) / 1e9
-            res[name] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"],
-                         "tbfly_per_s": npol * tw * (n // 2) * N_LOG / (t_ms * 1e-3) / 1e12}
-        # RNS multiply out = a * b over the same batch (3 words moved per coefficient)
-        other = torch.empty_like(data)
-        for t_ in range(tw):
-            other.view(npol, tw, n)[:, t_, :].random_(0, int(Q2[t_]), generator=gen)
-        prod = torch.empty_like(data)
-        mul = lambda: G.check(G.lib().gpufhe_rns_mult_batch(ctx2.h, data.data_ptr(), other.data_ptr(),
-                                                            prod.data_ptr(), npol, tw, 0, cur))
-        for _ in range(3):
-            mul()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(10):
-            mul()
-        b.record()
-        torch.cuda.synchronize()
-        t_ms = a.elapsed_time(b) / 10
-        gbs = 3 * 8 * n * npol * tw / (t_ms * 1e-3) / 1e9
-        res["rns_mult"] = {"ms": t_ms, "gbs": gbs, "frac": gbs / peaks()["hbm_gbs"]}
-        ntt = {"workload": "64 polys x 12 towers x 2^16, 50-bit primes", "bytes_per_tower_transform": 2 * 8 * n,
-               "bytes_per_tower_mult": 3 * 8 * n, **res}
-        del data, other, prod
-        ctx2.close()
+    # kernel isolation: 64 polys x 12 towers x 2^16
+    ntt = None if args.no_ntt else ntt_isolation(G, torch, dev, local, cur, gen)
 
     # serving trace (continuous batching vs one request at a time)
     serving = None
@@ -629,6 +640,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--pairs", type=int, default=PAIRS, help="pairs per step (smaller only for profiling)")
+    ap.add_argument("--section", default="all", choices=["all", "ntt"],
+                    help="ntt: only the NTT / RNS-multiply kernel isolation (prints its own line)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -120,6 +120,9 @@ int gpufhe_ntt_batch(gpufhe_ctx* h, uint64_t* d_data, uint32_t npolys, uint32_t 
             j.q = mods[qi].q;
             j.scale = ninv[qi];
             j.scale_p = ninvp[qi];
+            j.fp = fp_tower(j.q) ? 1u : 0u;
+            j.twd = j.fp ? (inverse ? D.twid : D.twfd) + (size_t)qi * n : nullptr;
+            j.reserved = 0;
         }
     cudaError_t e = cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(xf::Job), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }

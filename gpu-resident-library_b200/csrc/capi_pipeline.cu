@@ -74,7 +74,7 @@ int gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t s) 
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     if (!plan) return 0;
     uint32_t k = 0;
-    for (int i = 0; i < pl::NPHASE; ++i) k += plan->p->job_cnt[i] ? 1 : 0;
+    for (int i = 0; i < pl::NPHASE; ++i) k += (plan->p->job_cnt[i][0] ? 1 : 0) + (plan->p->job_cnt[i][1] ? 1 : 0);
     return k;
 }
 

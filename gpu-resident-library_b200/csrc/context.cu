@@ -158,6 +158,18 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
     dc_.mod = upload(mc);
     dc_.twf = upload(twf);
     dc_.twi = upload(twi);
+    {
+        std::vector<double> fd((size_t)QP * n, 0.0), id((size_t)QP * n, 0.0);
+        for (uint32_t i = 0; i < QP; ++i) {
+            if (!fp_tower(mc[i].q)) continue;
+            for (uint32_t k = 0; k < n; ++k) {
+                fd[(size_t)i * n + k] = (double)twf[(size_t)i * n + k].w;
+                id[(size_t)i * n + k] = (double)twi[(size_t)i * n + k].w;
+            }
+        }
+        dc_.twfd = upload(fd);
+        dc_.twid = upload(id);
+    }
     dc_.ninv = upload(ninv);
     dc_.ninvp = upload(ninvp);
     dc_.lvl = upload(lv_host_);

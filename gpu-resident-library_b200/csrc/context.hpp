@@ -38,6 +38,8 @@ struct DevCtx {
     const ModC* mod;          // [QP]: Q towers then P towers
     const Tw* twf;            // [QP][n]
     const Tw* twi;            // [QP][n]
+    const double* twfd;       // [QP][n] forward twiddles as doubles (towers with q < 2^50; else 0)
+    const double* twid;       // [QP][n] inverse twiddles as doubles
     const u64* ninv;          // [QP] n^-1 mod q
     const u64* ninvp;
     const Level* lvl;         // [fullQ + 1]

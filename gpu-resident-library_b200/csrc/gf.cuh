@@ -19,8 +19,12 @@ struct __align__(16) ModC {
     u64 q, two_q;
     u64 mu_lo, mu_hi;   // floor(2^128 / q)
     u64 r64;            // floor(2^64 / q)
-    u64 pad;
+    u64 qinv_bits;      // bits of the double RN(1/q) (FP64 NTT path)
 };
+
+// Towers whose transforms may take the FP64 path (4q < 2^52).
+__host__ __device__ __forceinline__ bool fp_tower(u64 q) { return q < (1ull << 50); }
+__device__ __forceinline__ double qinv_of(const ModC& m) { return __longlong_as_double((long long)m.qinv_bits); }
 
 __device__ __forceinline__ u64 csub(u64 a, u64 m) { return a >= m ? a - m : a; }
 

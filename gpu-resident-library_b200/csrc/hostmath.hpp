@@ -1,5 +1,6 @@
 // Host-side exact modular helpers (setup only; never on a timed path).
 #pragma once
+#include <cstring>
 #include <cstdint>
 #include <stdexcept>
 #include <vector>
@@ -33,7 +34,8 @@ inline ModC modc(u64 q) {
     m.mu_lo = (u64)mu;
     m.mu_hi = (u64)(mu >> 64);
     m.r64 = (~0ull) / q;
-    m.pad = 0;
+    const double qinv = 1.0 / (double)q;   // RN(1/q), the FP64 NTT path's quotient scale
+    std::memcpy(&m.qinv_bits, &qinv, 8);
     return m;
 }
 

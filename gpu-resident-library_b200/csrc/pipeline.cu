@@ -13,6 +13,41 @@ namespace pl {
 
 namespace {
 
+template <int LOGN, bool FP>
+struct Variant {
+    static void attrs() {
+        using G = ntt::Geo<LOGN>;
+        cudaFuncSetAttribute(p1_inv_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p2_inv_col<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+        cudaFuncSetAttribute(p3_modup_fwd_col<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+        cudaFuncSetAttribute(p4_modup_fwd_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p6_moddown_inv_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p8_moddown_fwd_col<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+        cudaFuncSetAttribute(p9_final_fwd_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+    }
+    // Phase k of the jobs routed to this arithmetic path (P5 and P7 have one
+    // integer kernel and are launched by the caller).
+    static void phase(int k, const Plan& p, cudaStream_t s) {
+        using G = ntt::Geo<LOGN>;
+        const int v = FP ? 1 : 0;
+        const uint32_t cnt = p.job_cnt[k][v];
+        if (!cnt) return;
+        const DevCtx& D = p.dc;
+        const PairDesc* pd = p.d_pairs;
+        const uint2* J = p.d_jobs + p.job_off[k][v];
+        switch (k) {
+            case 0: p1_inv_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 1: p2_inv_col<LOGN, FP><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
+            case 2: p3_modup_fwd_col<LOGN, FP><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
+            case 3: p4_modup_fwd_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 5: p6_moddown_inv_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 7: p8_moddown_fwd_col<LOGN, FP><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
+            case 8: p9_final_fwd_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            default: break;
+        }
+    }
+};
+
 template <int LOGN>
 struct Launcher {
     static void attrs(uint32_t dnum) {
@@ -20,14 +55,9 @@ struct Launcher {
         static bool done = false;
         static uint32_t mac_dnum = 0;
         if (!done) {
-            cudaFuncSetAttribute(p1_inv_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-            cudaFuncSetAttribute(p2_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-            cudaFuncSetAttribute(p3_modup_fwd_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-            cudaFuncSetAttribute(p4_modup_fwd_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-            cudaFuncSetAttribute(p6_moddown_inv_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+            Variant<LOGN, false>::attrs();
+            Variant<LOGN, true>::attrs();
             cudaFuncSetAttribute(p7_moddown_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-            cudaFuncSetAttribute(p8_moddown_fwd_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-            cudaFuncSetAttribute(p9_final_fwd_row<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
             done = true;
         }
         if (dnum > mac_dnum) {
@@ -40,19 +70,21 @@ struct Launcher {
         constexpr int MAC_TILES = (1 << LOGN) / MAC_TILE;
         attrs(p.dc.dnum);
         const DevCtx& D = p.dc;
-        const PairDesc* pd = p.d_pairs;
-        auto J = [&](int k) { return p.d_jobs + p.job_off[k]; };
-        auto cnt = [&](int k) { return p.job_cnt[k]; };
-        auto on = [&](int k) { return (mask >> k & 1) && cnt(k); };
-        if (on(0)) p1_inv_row<LOGN><<<cnt(0) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(0));
-        if (on(1)) p2_inv_col<LOGN><<<cnt(1) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(1));
-        if (on(2)) p3_modup_fwd_col<LOGN><<<cnt(2) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(2));
-        if (on(3)) p4_modup_fwd_row<LOGN><<<cnt(3) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(3));
-        if (on(4)) p5_mac<LOGN><<<cnt(4) * MAC_TILES, MAC_NT, mac_smem(D.dnum), s>>>(D, pd, p.d_mac_jobs, p.d_plist);
-        if (on(5)) p6_moddown_inv_row<LOGN><<<cnt(5) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(5));
-        if (on(6)) p7_moddown_inv_col<LOGN><<<cnt(6) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(6));
-        if (on(7)) p8_moddown_fwd_col<LOGN><<<cnt(7) * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J(7));
-        if (on(8)) p9_final_fwd_row<LOGN><<<cnt(8) * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J(8));
+        for (int k = 0; k < NPHASE; ++k) {
+            if (!(mask >> k & 1)) continue;
+            if (k == 4) {
+                if (p.job_cnt[4][0])
+                    p5_mac<LOGN><<<p.job_cnt[4][0] * MAC_TILES, MAC_NT, mac_smem(D.dnum), s>>>(D, p.d_pairs,
+                                                                                            p.d_mac_jobs, p.d_plist);
+            } else if (k == 6) {
+                if (p.job_cnt[6][0])
+                    p7_moddown_inv_col<LOGN><<<p.job_cnt[6][0] * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(
+                        D, p.d_pairs, p.d_jobs + p.job_off[6][0]);
+            } else {
+                Variant<LOGN, false>::phase(k, p, s);
+                Variant<LOGN, true>::phase(k, p, s);
+            }
+        }
     }
 };
 
@@ -85,8 +117,8 @@ struct HostTables {
     std::vector<uint2> jobs;       // all phases, concatenated
     std::vector<uint4> mac_jobs;
     std::vector<uint32_t> plist;
-    size_t job_off[NPHASE] = {};
-    uint32_t job_cnt[NPHASE] = {};
+    size_t job_off[NPHASE][2] = {};     // [phase][integer, FP64]
+    uint32_t job_cnt[NPHASE][2] = {};
 };
 
 static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const std::vector<u64*>& ws_ptrs,
@@ -146,16 +178,35 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
             T.plist.insert(T.plist.end(), v.begin() + g, v.begin() + g + cnt);
         }
     }
-    size_t total = 0;
-    for (int k = 0; k < NPHASE; ++k) {
-        T.job_off[k] = total;
-        T.job_cnt[k] = (uint32_t)jobs[k].size();
-        total += jobs[k].size();
-    }
-    T.job_cnt[4] = (uint32_t)T.mac_jobs.size();
+    // Route the transform jobs of each NTT phase to the integer or the FP64
+    // kernel by the modulus of the tower they transform (P7 stays integer:
+    // one CTA there mixes P towers and tower L-1).
+    const std::vector<u64>& Qv = c.Q();
+    const std::vector<u64>& Pv = c.P();
+    auto qp_mod = [&](u32 qp) { return qp < c.fullQ() ? Qv[qp] : Pv[qp - c.fullQ()]; };
+    auto tower = [&](int k, const uint2& j) -> u32 {
+        const PairDesc& P = T.pairs[j.x];
+        switch (k) {
+            case 0: case 1: return j.y;
+            case 2: case 3: return qp_of(j.y % (P.L + K), P.L, c.fullQ());
+            case 5: { const u32 t = j.y % (K + 1); return t == 0 ? P.L - 1 : c.fullQ() + t - 1; }
+            default: return j.y % P.L;   // 7, 8
+        }
+    };
     T.jobs.clear();
-    T.jobs.reserve(total);
-    for (int k = 0; k < NPHASE; ++k) T.jobs.insert(T.jobs.end(), jobs[k].begin(), jobs[k].end());
+    for (int k = 0; k < NPHASE; ++k) {
+        const bool split = k != 4 && k != 6;
+        for (int v = 0; v < 2; ++v) {
+            T.job_off[k][v] = T.jobs.size();
+            for (const uint2& j : jobs[k]) {
+                const bool fp = split && fp_tower(qp_mod(tower(k, j)));
+                if ((int)fp == v) T.jobs.push_back(j);
+            }
+            T.job_cnt[k][v] = (uint32_t)(T.jobs.size() - T.job_off[k][v]);
+        }
+    }
+    T.job_cnt[4][0] = (uint32_t)T.mac_jobs.size();
+    T.job_cnt[4][1] = 0;
 }
 
 Plan::Plan() : staging(std::make_unique<HostTables>()) {}
@@ -203,7 +254,8 @@ static void commit(Plan& p, const HostTables& T, const std::vector<Op>& ops, cud
     p.d_jobs = reinterpret_cast<uint2*>(d + b_pairs);
     p.d_mac_jobs = reinterpret_cast<uint4*>(d + b_pairs + b_jobs);
     p.d_plist = reinterpret_cast<uint32_t*>(d + b_pairs + b_jobs + b_mac);
-    for (int k = 0; k < NPHASE; ++k) { p.job_off[k] = T.job_off[k]; p.job_cnt[k] = T.job_cnt[k]; }
+    for (int k = 0; k < NPHASE; ++k)
+        for (int v = 0; v < 2; ++v) { p.job_off[k][v] = T.job_off[k][v]; p.job_cnt[k][v] = T.job_cnt[k][v]; }
     p.nops = (uint32_t)ops.size();
     p.ops = ops;
     p.pairs_host = T.pairs;

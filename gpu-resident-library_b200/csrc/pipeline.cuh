@@ -15,7 +15,10 @@
 // SwitchModulus(q_l -> q_i). Every step is an exact residue computation, so
 // each output equals the reference's bit for bit.
 //
-// Phases (one launch each; jobs are (pair, sub) unless noted):
+// Pass-to-pass intermediates (X after P1, Y after P3, Z after P8) are kept in
+// the arithmetic path's own word format; every other slot holds u64 residues.
+//
+// Phases (one launch each per arithmetic path; jobs are (pair, sub) unless noted):
 //   P1 inv-row  (pair,i)       tensor / gather prologue, INTT row stages     -> X
 //   P2 inv-col  (pair,i)       INTT column stages, * n^-1 QHatInv            -> X
 //   P3 fwd-col  (pair,p,i)     ModUp conversion prologue, NTT column stages  -> Y
@@ -103,8 +106,26 @@ __device__ __forceinline__ u64* slot_ptr(const PairDesc& P, u32 slot, int logn) 
     return P.ws + ((size_t)slot << logn);
 }
 
+// Arithmetic policy and twiddle accessors of the integer (FP = false) or the
+// FP64 (FP = true, towers with q < 2^50) instantiation of a phase kernel.
+template <bool FP>
+__device__ __forceinline__ auto ar_of(const ModC& m) {
+    if constexpr (FP) return ntt::FpAr{ntt::u2d(m.q), qinv_of(m)};
+    else return ntt::IntAr{m.q, m.two_q};
+}
+template <bool FP>
+__device__ __forceinline__ auto twf_of(const DevCtx& D, u32 qp, int logn) {
+    if constexpr (FP) return ntt::TwD{D.twfd + ((size_t)qp << logn)};
+    else return ntt::TwPacked{D.twf + ((size_t)qp << logn)};
+}
+template <bool FP>
+__device__ __forceinline__ auto twi_of(const DevCtx& D, u32 qp, int logn) {
+    if constexpr (FP) return ntt::TwD{D.twid + ((size_t)qp << logn)};
+    else return ntt::TwPacked{D.twi + ((size_t)qp << logn)};
+}
+
 // ------------------------------------------------------------------ P1
-template <int LOGN>
+template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
 p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
@@ -114,19 +135,19 @@ p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
     const PairDesc& P = pairs[jb.x];
     const u32 i = jb.y;
     const ModC m = D.mod[i];
+    const auto ar = ar_of<FP>(m);
     const WsLayout w = ws_layout(P.L, D.K, D.alpha);
     u64* X = slot_ptr(P, w.X + i, LOGN) + (size_t)R0 * 256;
-    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
-        sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = digit_src<LOGN>(P, i, (R0 + rl) * 256 + c, m);
-    });
+    ntt::row_tile_stage<G::RB, G::ROW_THREADS>(
+        [&](int rl, int c) { return digit_src<LOGN>(P, i, (R0 + rl) * 256 + c, m); },
+        [&](int rl, int c, u64 v) { sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = ar.stage_in(v); });
     __syncthreads();
     auto st = [&](int rl, int c, u64 v) { X[rl * 256 + c] = v; };
-    ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, ntt::TwPacked{D.twi + ((size_t)i << LOGN)}, R0,
-                                                           m.q, m.two_q, st);
+    ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8, true>(sm, twi_of<FP>(D, i, LOGN), R0, ar, st);
 }
 
 // ------------------------------------------------------------------ P2
-template <int LOGN>
+template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
 p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
@@ -143,12 +164,11 @@ p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
     u64* X = slot_ptr(P, w.X + i, LOGN) + c0;
     auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
     auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
-    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)i << LOGN)}, m.q,
-                                                          m.two_q, ld, st);
+    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, twi_of<FP>(D, i, LOGN), ar_of<FP>(m), ld, st);
 }
 
 // ------------------------------------------------------------------ P3
-template <int LOGN, int SP>
+template <int LOGN, int SP, bool FP>
 __device__ __forceinline__ void p3_body(const DevCtx& D, const PairDesc& P, u32 p, u32 i, int c0, u64* sm) {
     using G = ntt::Geo<LOGN>;
     const u32 L = P.L, K = D.K, QlP = L + K;
@@ -176,11 +196,10 @@ __device__ __forceinline__ void p3_body(const DevCtx& D, const PairDesc& P, u32 
         return barrett_lazy(lo, hi, m.q, m.mu_lo, m.mu_hi);
     };
     auto stf = [&](int r, int cl, u64 v) { Y[r * 256 + cl] = v; };
-    ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0>(sm, ntt::TwPacked{D.twf + ((size_t)qp << LOGN)}, m.q,
-                                                       m.two_q, ld, stf);
+    ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(sm, twf_of<FP>(D, qp, LOGN), ar_of<FP>(m), ld, stf);
 }
 
-template <int LOGN>
+template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
 p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
@@ -191,17 +210,17 @@ p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     const u32 QlP = P.L + D.K;
     const u32 p = jb.y / QlP, i = jb.y % QlP;
     switch (D.lvl[P.L].part_sp[p]) {
-        case 1: p3_body<LOGN, 1>(D, P, p, i, c0, sm); break;
-        case 2: p3_body<LOGN, 2>(D, P, p, i, c0, sm); break;
-        case 3: p3_body<LOGN, 3>(D, P, p, i, c0, sm); break;
-        case 4: p3_body<LOGN, 4>(D, P, p, i, c0, sm); break;
-        default: p3_body<LOGN, 0>(D, P, p, i, c0, sm); break;
+        case 1: p3_body<LOGN, 1, FP>(D, P, p, i, c0, sm); break;
+        case 2: p3_body<LOGN, 2, FP>(D, P, p, i, c0, sm); break;
+        case 3: p3_body<LOGN, 3, FP>(D, P, p, i, c0, sm); break;
+        case 4: p3_body<LOGN, 4, FP>(D, P, p, i, c0, sm); break;
+        default: p3_body<LOGN, 0, FP>(D, P, p, i, c0, sm); break;
     }
 }
 
 // ------------------------------------------------------------------ P4
 // NTT row stages of one digit tower; output reduced to [0, 2q).
-template <int LOGN>
+template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
 p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
@@ -216,10 +235,10 @@ p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     const WsLayout w = ws_layout(L, D.K, D.alpha);
     u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + (size_t)R0 * 256;
     auto ld = [&](int rl, int c) { return Y[rl * 256 + c]; };
-    ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0>(sm, ntt::TwPacked{D.twf + ((size_t)qp << LOGN)}, R0,
-                                                           m.q, m.two_q, ld);
+    const auto ar = ar_of<FP>(m);
+    ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0, true>(sm, twf_of<FP>(D, qp, LOGN), R0, ar, ld);
     ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
-        Y[rl * 256 + c] = csub(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)], m.two_q);
+        Y[rl * 256 + c] = csub(ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)]), m.two_q);
     });
 }
 
@@ -411,7 +430,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
 
 // ------------------------------------------------------------------ P6
 // INTT row stages of U[c] (t = 0, EvalMult+Rescale only) and RP[c][t-1].
-template <int LOGN>
+template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
 p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
@@ -425,14 +444,14 @@ p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
     const u32 qp = t == 0 ? L - 1 : D.fullQ + t - 1;
     const u32 slot = t == 0 ? w.U + c : w.RP + c * K + (t - 1);
     const ModC m = D.mod[qp];
+    const auto ar = ar_of<FP>(m);
     u64* X = slot_ptr(P, slot, LOGN) + (size_t)R0 * 256;
-    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int cc) {
-        sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)] = X[rl * 256 + cc];
-    });
+    ntt::row_tile_stage<G::RB, G::ROW_THREADS>(
+        [&](int rl, int cc) { return X[rl * 256 + cc]; },
+        [&](int rl, int cc, u64 v) { sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)] = ar.stage_in(v); });
     __syncthreads();
     auto st = [&](int rl, int cc, u64 v) { X[rl * 256 + cc] = v; };
-    ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, ntt::TwPacked{D.twi + ((size_t)qp << LOGN)}, R0,
-                                                           m.q, m.two_q, st);
+    ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, twi_of<FP>(D, qp, LOGN), R0, ar, st);
 }
 
 // ------------------------------------------------------------------ P7
@@ -459,8 +478,8 @@ p7_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
         u64* X = slot_ptr(P, w.RP + c * K + (t - 1), LOGN) + c0;
         auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
         auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
-        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)qp << LOGN)}, m.q,
-                                                              m.two_q, ld, st);
+        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)qp << LOGN)},
+                                                              ntt::IntAr{m.q, m.two_q}, ld, st);
         __syncthreads();
     }
     if (P.mode != EMR) return;
@@ -477,12 +496,12 @@ p7_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
         const u64 tmp = shoup(barrett_lazy(lo, hi, m.q, m.mu_lo, m.mu_hi), pv, pvp, m.q);
         U[e] = u >= tmp ? u - tmp : u + m.q - tmp;
     };
-    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)l << LOGN)}, m.q,
-                                                          m.two_q, ld, st);
+    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)l << LOGN)},
+                                                          ntt::IntAr{m.q, m.two_q}, ld, st);
 }
 
 // ------------------------------------------------------------------ P8
-template <int LOGN, u32 MODE>
+template <int LOGN, u32 MODE, bool FP>
 __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 c, u32 i, int c0, u64* sm,
                                         const u64* ci) {
     using G = ntt::Geo<LOGN>;
@@ -521,11 +540,10 @@ __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 
         return v;
     };
     auto st = [&](int r, int cl, u64 v) { Z[r * 256 + cl] = v; };
-    ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0>(sm, ntt::TwPacked{D.twf + ((size_t)i << LOGN)}, q, m.two_q,
-                                                       ld, st);
+    ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(sm, twf_of<FP>(D, i, LOGN), ar_of<FP>(m), ld, st);
 }
 
-template <int LOGN>
+template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
 p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     extern __shared__ __align__(16) u64 sm[];
@@ -536,13 +554,13 @@ p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
     const u32 c = jb.y / P.L, i = jb.y % P.L;
     if (threadIdx.x < D.K) ci[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + i];
     __syncthreads();
-    if (P.mode == EMR) p8_body<LOGN, EMR>(D, P, c, i, c0, sm, ci);
-    else if (P.mode == RESCALE) p8_body<LOGN, RESCALE>(D, P, c, i, c0, sm, ci);
-    else p8_body<LOGN, KS>(D, P, c, i, c0, sm, ci);
+    if (P.mode == EMR) p8_body<LOGN, EMR, FP>(D, P, c, i, c0, sm, ci);
+    else if (P.mode == RESCALE) p8_body<LOGN, RESCALE, FP>(D, P, c, i, c0, sm, ci);
+    else p8_body<LOGN, KS, FP>(D, P, c, i, c0, sm, ci);
 }
 
 // ------------------------------------------------------------------ P9
-template <int LOGN>
+template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
 p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
@@ -557,8 +575,8 @@ p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     const size_t tile0 = (size_t)R0 * 256;
     const u64* Z = slot_ptr(P, w.Z + c * L + i, LOGN) + tile0;
     auto ld = [&](int rl, int cc) { return Z[rl * 256 + cc]; };
-    ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0>(sm, ntt::TwPacked{D.twf + ((size_t)i << LOGN)}, R0, m.q,
-                                                           m.two_q, ld);
+    const auto ar = ar_of<FP>(m);
+    ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0, true>(sm, twf_of<FP>(D, i, LOGN), R0, ar, ld);
     const size_t o = ((size_t)i << LOGN) + tile0;
     u64* out = P.out[c] + o;
     const u64* Wt = slot_ptr(P, w.W + c * L + i, LOGN) + tile0;
@@ -566,7 +584,7 @@ p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     const u64 s1 = lv.s1[i], s1p = lv.s1p[i];
     ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int cc) {
         const int e = rl * 256 + cc;
-        const u64 v = csub(csub(sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)], m.two_q), m.q);
+        const u64 v = csub(csub(ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)]), m.two_q), m.q);
         u64 r;
         if (mode == RESCALE) {
             r = csub(shoup(P.in[0][o + e], s1, s1p, m.q) + v, m.q);

@@ -26,8 +26,8 @@ struct Plan {
     uint32_t logn = 0, nops = 0;
     PairDesc* d_pairs = nullptr;
     uint2* d_jobs = nullptr;
-    size_t job_off[NPHASE] = {};
-    uint32_t job_cnt[NPHASE] = {};
+    size_t job_off[NPHASE][2] = {};    // [phase][integer kernel, FP64 kernel]
+    uint32_t job_cnt[NPHASE][2] = {};
     uint4* d_mac_jobs = nullptr;
     uint32_t* d_plist = nullptr;
     u64* ws = nullptr;

@@ -222,7 +222,7 @@ void LaunchNTT_CT(uint64_t* d_x, const uint64_t* d_roots, const uint64_t* d_prec
                   cudaStream_t s) {
     const int logn = hm::ilog2(n);
     if (hm::is_pow2(n) && xf_supported_logn(logn)) {
-        xf::Job j{d_x, nullptr, d_roots, d_precon, q, 0, 0};
+        xf::Job j{d_x, nullptr, d_roots, d_precon, q, 0, 0, nullptr, fp_tower(q) ? 1u : 0u, 0};
         xf_launch_ntt(nullptr, &j, 1, logn, false, s);
     } else if (n >= 2) {
         fallback_ntt(d_x, d_roots, d_precon, n, q, false, 0, 0, s);
@@ -234,7 +234,7 @@ void LaunchINTT_GS(uint64_t* d_x, const uint64_t* d_invroots, const uint64_t* d_
                    uint64_t n_inv, uint64_t n_inv_precon, cudaStream_t s) {
     const int logn = hm::ilog2(n);
     if (hm::is_pow2(n) && xf_supported_logn(logn)) {
-        xf::Job j{d_x, nullptr, d_invroots, d_invprecon, q, n_inv, n_inv_precon};
+        xf::Job j{d_x, nullptr, d_invroots, d_invprecon, q, n_inv, n_inv_precon, nullptr, fp_tower(q) ? 1u : 0u, 0};
         xf_launch_ntt(nullptr, &j, 1, logn, true, s);
     } else if (n >= 2) {
         fallback_ntt(d_x, d_invroots, d_invprecon, n, q, true, n_inv, n_inv_precon, s);

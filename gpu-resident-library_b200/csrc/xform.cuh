@@ -1,4 +1,7 @@
 // Batched in-place forward / inverse NTT kernels over a list of tower jobs.
+// Between its two passes a transform keeps the tower in the arithmetic
+// path's own word format (FP64 bits on that path); only the second pass
+// writes canonical residues.
 // One launch per pass covers every job (ciphertexts x towers): grid =
 // jobs x tiles-per-job. Used by the reference ABI (LaunchNTT_CT /
 // LaunchINTT_GS, one job) and by the batched transform entry points.
@@ -8,7 +11,10 @@
 namespace xf {
 
 // One tower to transform in place. Twiddles either packed {w, wp} (library
-// tables) or split (two arrays, the reference's table layout).
+// tables) or split (two arrays, the reference's table layout). fp != 0 (only
+// for q < 2^50) selects the FP64 arithmetic, with the double table twd or,
+// when twd is null, the split w table converted on load. Fields after
+// scale_p default to zero (integer path) in brace initialisation.
 struct Job {
     u64* x;
     const Tw* tw;        // packed tables, or nullptr when split
@@ -16,12 +22,24 @@ struct Job {
     const u64* wp;
     u64 q;
     u64 scale, scale_p;  // inverse only: n^-1 (and precon) folded in at the end
+    const double* twd;   // FP64 twiddles (fp path), or nullptr
+    u32 fp;
+    u32 reserved;
 };
 
+// Calls f(arith policy, twiddle accessor) for the job's path.
 template <class F>
-__device__ __forceinline__ auto with_tw(const Job& j, F&& f) {
-    if (j.tw) return f(ntt::TwPacked{j.tw});
-    return f(ntt::TwSplit{j.w, j.wp});
+__device__ __forceinline__ void with_path(const Job& j, F&& f) {
+    if (j.fp) {
+        const double qd = ntt::u2d(j.q);
+        const ntt::FpAr ar{qd, __ddiv_rn(1.0, qd)};
+        if (j.twd) f(ar, ntt::TwD{j.twd});
+        else f(ar, ntt::TwDConv{j.w});
+        return;
+    }
+    const ntt::IntAr ar{j.q, 2 * j.q};
+    if (j.tw) f(ar, ntt::TwPacked{j.tw});
+    else f(ar, ntt::TwSplit{j.w, j.wp});
 }
 
 // Jobs come either from a device array (SINGLE = false) or a single by-value
@@ -40,13 +58,11 @@ k_fwd_col(const Job* __restrict__ arr, const Job one) {
     const int job = blockIdx.x / G::COL_TILES;
     const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
     const Job j = get_job<SINGLE>(arr, one, job);
-    const u64 q = j.q, two_q = 2 * q;
     u64* x = j.x;
     auto ld = [&](int r, int cl) { return x[r * 256 + c0 + cl]; };
     auto st = [&](int r, int cl, u64 v) { x[r * 256 + c0 + cl] = v; };
-    with_tw(j, [&](auto tw) {
-        ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0>(sm, tw, q, two_q, ld, st);
-        return 0;
+    with_path(j, [&](const auto& ar, const auto& tw) {
+        ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(sm, tw, ar, ld, st);
     });
 }
 
@@ -61,14 +77,12 @@ k_fwd_row(const Job* __restrict__ arr, const Job one) {
     const u64 q = j.q, two_q = 2 * q;
     u64* x = j.x + (size_t)R0 * 256;
     auto ld = [&](int rl, int c) { return x[rl * 256 + c]; };
-    with_tw(j, [&](auto tw) {
-        ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0>(sm, tw, R0, q, two_q, ld);
-        return 0;
-    });
-    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
-        u64 v = sm[rl * G::ROW_STRIDE + ntt::rowpad(c)];
-        v = csub(csub(v, two_q), q);
-        x[rl * 256 + c] = v;
+    with_path(j, [&](const auto& ar, const auto& tw) {
+        ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0, true>(sm, tw, R0, ar, ld);
+        ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
+            const u64 v = ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)]);
+            x[rl * 256 + c] = csub(csub(v, two_q), q);
+        });
     });
 }
 
@@ -80,16 +94,14 @@ k_inv_row(const Job* __restrict__ arr, const Job one) {
     const int job = blockIdx.x / G::ROW_TILES;
     const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
     const Job j = get_job<SINGLE>(arr, one, job);
-    const u64 q = j.q, two_q = 2 * q;
     u64* x = j.x + (size_t)R0 * 256;
-    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
-        sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = x[rl * 256 + c];
-    });
-    __syncthreads();
     auto st = [&](int rl, int c, u64 v) { x[rl * 256 + c] = v; };
-    with_tw(j, [&](auto tw) {
-        ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, tw, R0, q, two_q, st);
-        return 0;
+    with_path(j, [&](const auto& ar, const auto& tw) {
+        ntt::row_tile_stage<G::RB, G::ROW_THREADS>(
+            [&](int rl, int c) { return x[rl * 256 + c]; },
+            [&](int rl, int c, u64 v) { sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = ar.stage_in(v); });
+        __syncthreads();
+        ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8, true>(sm, tw, R0, ar, st);
     });
 }
 
@@ -101,14 +113,13 @@ k_inv_col(const Job* __restrict__ arr, const Job one) {
     const int job = blockIdx.x / G::COL_TILES;
     const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
     const Job j = get_job<SINGLE>(arr, one, job);
-    const u64 q = j.q, two_q = 2 * q;
+    const u64 q = j.q;
     u64* x = j.x;
     auto ld = [&](int r, int cl) { return x[r * 256 + c0 + cl]; };
     const u64 sc = j.scale, scp = j.scale_p;
     auto st = [&](int r, int cl, u64 v) { x[r * 256 + c0 + cl] = shoup(v, sc, scp, q); };
-    with_tw(j, [&](auto tw) {
-        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, tw, q, two_q, ld, st);
-        return 0;
+    with_path(j, [&](const auto& ar, const auto& tw) {
+        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, tw, ar, ld, st);
     });
 }
 
