@@ -416,4 +416,28 @@ __device__ __forceinline__ void row_tile_stage(LD&& ld, ST&& st) {
     }
 }
 
+// Two-operand staging in batches of 8 words per thread: both operands of a
+// batch are loaded before st(rl, c, a, b) combines them.
+template <int RB, int NT, class LDA, class LDB, class ST>
+__device__ __forceinline__ void row_tile_stage2(LDA&& lda, LDB&& ldb, ST&& st) {
+    constexpr int PER = RB * 256 / NT;
+    constexpr int BT = PER < 8 ? PER : 8;
+    static_assert(PER * NT == RB * 256 && PER % BT == 0, "stage geometry");
+#pragma unroll
+    for (int k0 = 0; k0 < PER; k0 += BT) {
+        u64 a[BT], b[BT];
+#pragma unroll
+        for (int k = 0; k < BT; ++k) {
+            const int e = threadIdx.x + (k0 + k) * NT;
+            a[k] = lda(e >> 8, e & 255);
+            b[k] = ldb(e >> 8, e & 255);
+        }
+#pragma unroll
+        for (int k = 0; k < BT; ++k) {
+            const int e = threadIdx.x + (k0 + k) * NT;
+            st(e >> 8, e & 255, a[k], b[k]);
+        }
+    }
+}
+
 }  // namespace ntt

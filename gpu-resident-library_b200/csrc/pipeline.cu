@@ -109,6 +109,11 @@ void validate(const gfx::Context& c, const Op& op) {
     for (int k = 0; k < nin; ++k) if (!op.in[k]) throw std::invalid_argument("null input");
     if (!op.out[0] || (op.mode != RESCALE && !op.out[1])) throw std::invalid_argument("null output");
     if (op.mode == ROT && (op.galois % 2 == 0 || op.galois >= 2ull * c.n())) throw std::invalid_argument("bad Galois element");
+    auto misaligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) != 0; };
+    for (int k = 0; k < nin; ++k)
+        if (misaligned(op.in[k])) throw std::invalid_argument("input buffers must be 16-byte aligned");
+    if (misaligned(op.out[0]) || (op.mode != RESCALE && misaligned(op.out[1])))
+        throw std::invalid_argument("output buffers must be 16-byte aligned");
 }
 
 // Host tables of a batch: pair descriptors, per-phase jobs and P5 groups.
@@ -275,6 +280,8 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
         ws = plan->ws;
     } else if (ws_words < need) {
         throw std::length_error("workspace too small");
+    } else if (reinterpret_cast<uintptr_t>(ws) & 15) {
+        throw std::invalid_argument("workspace must be 16-byte aligned");
     }
     plan->ws_words = need;
     std::vector<u64*> wsp(ops.size());
@@ -290,6 +297,8 @@ void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops,
                      cudaStream_t s) {
     if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
     if (ws_ptrs.size() != ops.size()) throw std::invalid_argument("one workspace per operation");
+    for (u64* w : ws_ptrs)
+        if (!w || (reinterpret_cast<uintptr_t>(w) & 15)) throw std::invalid_argument("workspace must be 16-byte aligned");
     for (const Op& op : ops) validate(c, op);
     p.dc = c.dev();
     p.logn = c.logn();

@@ -124,6 +124,53 @@ __device__ __forceinline__ auto twi_of(const DevCtx& D, u32 qp, int logn) {
     else return ntt::TwPacked{D.twi + ((size_t)qp << logn)};
 }
 
+// Column-tile staging: the prologue of a column pass (a basis conversion)
+// is computed for the whole tile into shared memory before the first round,
+// reading its inputs as 16-byte column pairs with the loads of CS_VB pairs
+// (and up to four conversion terms) in flight together. Thread t covers
+// pairs t + k * COL_THREADS, k < PER; pair v sits at row v / (C/2), column
+// 2 * (v % (C/2)), so a warp reads whole 128-byte row segments.
+constexpr int CS_VB = 2;
+
+template <int LOGN>
+struct ColStage {
+    using G = ntt::Geo<LOGN>;
+    static constexpr int VPR = G::C / 2;
+    static constexpr int PER = G::R1 * VPR / G::COL_THREADS;
+    static_assert(PER * G::COL_THREADS == G::R1 * VPR && PER % CS_VB == 0, "column staging geometry");
+    __device__ static __forceinline__ void pos(int k, int& r, int& cl) {
+        const int v = threadIdx.x + k * G::COL_THREADS;
+        r = v / VPR;
+        cl = 2 * (v % VPR);
+    }
+};
+
+__device__ __forceinline__ ulonglong2 ld2(const u64* p) { return *reinterpret_cast<const ulonglong2*>(p); }
+
+// lo/hi[b][j] += sum_{t < nterms} base[t * stride + e[b] + j] * coef[t] (128-bit).
+template <int VB>
+__device__ __forceinline__ void mac_terms(u64 (&lo)[VB][2], u64 (&hi)[VB][2], const u64* base, size_t stride,
+                                          u32 nterms, const u64* coef, const size_t (&e)[VB]) {
+    for (u32 t0 = 0; t0 < nterms; t0 += 4) {
+        ulonglong2 xv[4][VB];
+#pragma unroll
+        for (int tt = 0; tt < 4; ++tt)
+            if (t0 + tt < nterms)
+#pragma unroll
+                for (int b = 0; b < VB; ++b) xv[tt][b] = ld2(base + (t0 + tt) * stride + e[b]);
+#pragma unroll
+        for (int tt = 0; tt < 4; ++tt)
+            if (t0 + tt < nterms) {
+                const u64 c = coef[t0 + tt];
+#pragma unroll
+                for (int b = 0; b < VB; ++b) {
+                    mac_wide(lo[b][0], hi[b][0], xv[tt][b].x, c);
+                    mac_wide(lo[b][1], hi[b][1], xv[tt][b].y, c);
+                }
+            }
+    }
+}
+
 // ------------------------------------------------------------------ P1
 template <int LOGN, bool FP>
 __global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
@@ -138,9 +185,17 @@ p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
     const auto ar = ar_of<FP>(m);
     const WsLayout w = ws_layout(P.L, D.K, D.alpha);
     u64* X = slot_ptr(P, w.X + i, LOGN) + (size_t)R0 * 256;
-    ntt::row_tile_stage<G::RB, G::ROW_THREADS>(
-        [&](int rl, int c) { return digit_src<LOGN>(P, i, (R0 + rl) * 256 + c, m); },
-        [&](int rl, int c, u64 v) { sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = ar.stage_in(v); });
+    if (P.mode == EMR) {   // d2 = a1 * b1: both operands of a batch loaded before the products
+        const size_t o = ((size_t)i << LOGN) + (size_t)R0 * 256;
+        ntt::row_tile_stage2<G::RB, G::ROW_THREADS>(
+            [&](int rl, int c) { return P.in[1][o + rl * 256 + c]; },
+            [&](int rl, int c) { return P.in[3][o + rl * 256 + c]; },
+            [&](int rl, int c, u64 a, u64 b) { sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = ar.stage_in(mulmod(a, b, m)); });
+    } else {
+        ntt::row_tile_stage<G::RB, G::ROW_THREADS>(
+            [&](int rl, int c) { return digit_src<LOGN>(P, i, (R0 + rl) * 256 + c, m); },
+            [&](int rl, int c, u64 v) { sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = ar.stage_in(v); });
+    }
     __syncthreads();
     auto st = [&](int rl, int c, u64 v) { X[rl * 256 + c] = v; };
     ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8, true>(sm, twi_of<FP>(D, i, LOGN), R0, ar, st);
@@ -168,54 +223,51 @@ p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
 }
 
 // ------------------------------------------------------------------ P3
-template <int LOGN, int SP, bool FP>
-__device__ __forceinline__ void p3_body(const DevCtx& D, const PairDesc& P, u32 p, u32 i, int c0, u64* sm) {
+template <int LOGN, bool FP>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     using G = ntt::Geo<LOGN>;
+    using CS = ColStage<LOGN>;
+    extern __shared__ __align__(16) u64 sm[];
+    __shared__ u64 cst[MAXA];
+    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
+    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
+    const PairDesc& P = pairs[jb.x];
     const u32 L = P.L, K = D.K, QlP = L + K;
+    const u32 p = jb.y / QlP, i = jb.y % QlP;
     const Level& lv = D.lvl[L];
-    const u32 st0 = lv.part_st[p];
-    const u32 sp = SP > 0 ? (u32)SP : lv.part_sp[p];
+    const u32 st0 = lv.part_st[p], sp = lv.part_sp[p];
     const u32 qp = qp_of(i, L, D.fullQ);
     const ModC m = D.mod[qp];
     const WsLayout w = ws_layout(L, K, D.alpha);
     const u64* X = slot_ptr(P, w.X + st0, LOGN) + c0;
     u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + c0;
     const u64* pool = D.pool + lv.qmp_off + (size_t)st0 * QlP + i;
-    __shared__ u64 cst[MAXA];
     if (threadIdx.x < sp) cst[threadIdx.x] = pool[(size_t)threadIdx.x * QlP];
     __syncthreads();
-    auto ld = [&](int r, int cl) {
-        const u64* x = X + r * 256 + cl;
-        u64 lo = 0, hi = 0;
-        if constexpr (SP > 0) {
+    // conv_i = sum_s x_s * QHatModp[s][i] (ApproxSwitchCRTBasis), lazy in [0, 4q)
+#pragma unroll 1
+    for (int k0 = 0; k0 < CS::PER; k0 += CS_VB) {
+        int r[CS_VB], cl[CS_VB];
+        size_t e[CS_VB];
+        u64 lo[CS_VB][2] = {}, hi[CS_VB][2] = {};
 #pragma unroll
-            for (int s = 0; s < SP; ++s) mac_wide(lo, hi, x[(size_t)s << LOGN], cst[s]);
-        } else {
-            for (u32 s = 0; s < sp; ++s) mac_wide(lo, hi, x[(size_t)s << LOGN], cst[s]);
+        for (int b = 0; b < CS_VB; ++b) {
+            CS::pos(k0 + b, r[b], cl[b]);
+            e[b] = (size_t)r[b] * 256 + cl[b];
         }
-        return barrett_lazy(lo, hi, m.q, m.mu_lo, m.mu_hi);
-    };
+        mac_terms<CS_VB>(lo, hi, X, (size_t)1 << LOGN, sp, cst, e);
+#pragma unroll
+        for (int b = 0; b < CS_VB; ++b) {
+            u64* d = sm + r[b] * G::C + cl[b];
+            d[0] = barrett_lazy(lo[b][0], hi[b][0], m.q, m.mu_lo, m.mu_hi);
+            d[1] = barrett_lazy(lo[b][1], hi[b][1], m.q, m.mu_lo, m.mu_hi);
+        }
+    }
+    __syncthreads();
+    auto ld = [&](int r, int cl) { return sm[r * G::C + cl]; };
     auto stf = [&](int r, int cl, u64 v) { Y[r * 256 + cl] = v; };
     ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(sm, twf_of<FP>(D, qp, LOGN), ar_of<FP>(m), ld, stf);
-}
-
-template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
-p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
-    using G = ntt::Geo<LOGN>;
-    extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
-    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
-    const PairDesc& P = pairs[jb.x];
-    const u32 QlP = P.L + D.K;
-    const u32 p = jb.y / QlP, i = jb.y % QlP;
-    switch (D.lvl[P.L].part_sp[p]) {
-        case 1: p3_body<LOGN, 1, FP>(D, P, p, i, c0, sm); break;
-        case 2: p3_body<LOGN, 2, FP>(D, P, p, i, c0, sm); break;
-        case 3: p3_body<LOGN, 3, FP>(D, P, p, i, c0, sm); break;
-        case 4: p3_body<LOGN, 4, FP>(D, P, p, i, c0, sm); break;
-        default: p3_body<LOGN, 0, FP>(D, P, p, i, c0, sm); break;
-    }
 }
 
 // ------------------------------------------------------------------ P4
@@ -505,6 +557,7 @@ template <int LOGN, u32 MODE, bool FP>
 __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 c, u32 i, int c0, u64* sm,
                                         const u64* ci) {
     using G = ntt::Geo<LOGN>;
+    using CS = ColStage<LOGN>;
     const u32 L = P.L, K = D.K, l = L - 1;
     const WsLayout w = ws_layout(L, K, D.alpha);
     const Level& lv = D.lvl[L];
@@ -521,30 +574,51 @@ __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 
     const u64 s2 = lv.s2[i], s2p = lv.s2p[i];
     const u64 cm = MODE == EMR ? lv.ps1[i] : D.pinv[i];
     const u64 cmp = MODE == EMR ? lv.ps1p[i] : D.pinvp[i];
-    auto ld = [&](int r, int cl) -> u64 {
-        const int e = r * 256 + cl;
+    // v = sw_i(r_l) * s2 - conv'_i * cm, lazy in [0, 4q)
+    auto finish = [&](u64 x, u64 lo, u64 hi) -> u64 {
         u64 v = 0;
         if constexpr (MODE == EMR || MODE == RESCALE) {
-            const u64 x = R[e];
             const u64 d = x > half ? diff : 0;
             u64 sw;
             if (larger) sw = x + d;
             else { const u64 xm = reduce64(x, m); sw = xm >= d ? xm - d : xm + q - d; }
             v = shoup_lazy(sw, s2, s2p, q);
         }
-        if constexpr (MODE != RESCALE) {
-            u64 lo = 0, hi = 0;
-            for (u32 j = 0; j < K; ++j) mac_wide(lo, hi, XP[((size_t)j << LOGN) + e], ci[j]);
-            v += 2 * q - shoup_lazy(barrett_lazy(lo, hi, q, m.mu_lo, m.mu_hi), cm, cmp, q);
-        }
+        if constexpr (MODE != RESCALE) v += 2 * q - shoup_lazy(barrett_lazy(lo, hi, q, m.mu_lo, m.mu_hi), cm, cmp, q);
         return v;
     };
+#pragma unroll 1
+    for (int k0 = 0; k0 < CS::PER; k0 += CS_VB) {
+        int r[CS_VB], cl[CS_VB];
+        size_t e[CS_VB];
+#pragma unroll
+        for (int b = 0; b < CS_VB; ++b) {
+            CS::pos(k0 + b, r[b], cl[b]);
+            e[b] = (size_t)r[b] * 256 + cl[b];
+        }
+        ulonglong2 xr[CS_VB];
+        if constexpr (MODE == EMR || MODE == RESCALE) {
+#pragma unroll
+            for (int b = 0; b < CS_VB; ++b) xr[b] = ld2(R + e[b]);
+        }
+        u64 lo[CS_VB][2] = {}, hi[CS_VB][2] = {};
+        if constexpr (MODE != RESCALE) mac_terms<CS_VB>(lo, hi, XP, (size_t)1 << LOGN, K, ci, e);
+#pragma unroll
+        for (int b = 0; b < CS_VB; ++b) {
+            u64* d = sm + r[b] * G::C + cl[b];
+            const bool has_r = MODE == EMR || MODE == RESCALE;
+            d[0] = finish(has_r ? xr[b].x : 0, lo[b][0], hi[b][0]);
+            d[1] = finish(has_r ? xr[b].y : 0, lo[b][1], hi[b][1]);
+        }
+    }
+    __syncthreads();
+    auto ld = [&](int r, int cl) { return sm[r * G::C + cl]; };
     auto st = [&](int r, int cl, u64 v) { Z[r * 256 + cl] = v; };
     ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(sm, twf_of<FP>(D, i, LOGN), ar_of<FP>(m), ld, st);
 }
 
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 2)
 p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     extern __shared__ __align__(16) u64 sm[];
     __shared__ u64 ci[gfx::MAXP];
@@ -582,19 +656,23 @@ p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     const u64* Wt = slot_ptr(P, w.W + c * L + i, LOGN) + tile0;
     const Level& lv = D.lvl[L];
     const u64 s1 = lv.s1[i], s1p = lv.s1p[i];
-    ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int cc) {
-        const int e = rl * 256 + cc;
-        const u64 v = csub(csub(ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)]), m.two_q), m.q);
-        u64 r;
-        if (mode == RESCALE) {
-            r = csub(shoup(P.in[0][o + e], s1, s1p, m.q) + v, m.q);
-        } else {
-            r = csub(Wt[e] + v, m.q);
-            if (mode == ROT && c == 0)
-                r = csub(r + P.in[0][((size_t)i << LOGN) + galois_slot<LOGN>((u32)(tile0 + e), P.galois)], m.q);
-        }
-        out[e] = r;
-    });
+    // every W (or rescale input) word of the thread is loaded before the sums
+    const u64* addend = mode == RESCALE ? P.in[0] + o : Wt;
+    ntt::row_tile_stage<G::RB, G::ROW_THREADS>(
+        [&](int rl, int cc) { return addend[rl * 256 + cc]; },
+        [&](int rl, int cc, u64 a) {
+            const int e = rl * 256 + cc;
+            const u64 v = csub(csub(ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)]), m.two_q), m.q);
+            u64 r;
+            if (mode == RESCALE) {
+                r = csub(shoup(a, s1, s1p, m.q) + v, m.q);
+            } else {
+                r = csub(a + v, m.q);
+                if (mode == ROT && c == 0)
+                    r = csub(r + P.in[0][((size_t)i << LOGN) + galois_slot<LOGN>((u32)(tile0 + e), P.galois)], m.q);
+            }
+            out[e] = r;
+        });
 }
 
 }  // namespace pl
