@@ -453,8 +453,10 @@ def run_gpu(args):
 
     stream = torch.cuda.Stream(device=dev)
     graph = torch.cuda.CUDAGraph()
-    plan.launch(stream.cuda_stream)   # first launch outside capture (sets kernel attributes)
+    plan.launch(stream.cuda_stream)   # first launch outside capture: kernel attributes, autotuner
     torch.cuda.synchronize()
+    schedule = plan.schedule()
+    kernels_per_step = plan.kernel_count()
     with torch.cuda.graph(graph, stream=stream):
         plan.launch(torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
@@ -607,7 +609,8 @@ def run_gpu(args):
         "config": {"workload": WORKLOAD if pairs == PAIRS else f"profiling case: {pairs} pairs of " + WORKLOAD,
                    "n": n, "pairs_per_gpu": pairs, "levels": "U{4..12} seeded",
                    "mean_level": float(np.mean(levels)), "l2": "inputs larger than L2 (no flush)",
-                   "graph": f"{kernels_per_step} kernels per step, one CUDA graph"},
+                   "graph": f"{kernels_per_step} kernels per step, one CUDA graph",
+                   "schedule": schedule},
         "roofline": {"bound": "hbm", "kernel": "fused EvalMult+Rescale step (phases P1..P9)", "achieved": achieved,
                      "peak": pk["hbm_gbs"], "peak_source": pk["source"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "algorithmic_bytes_per_launch": alg, "traffic": None},

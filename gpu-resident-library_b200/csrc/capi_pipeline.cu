@@ -59,6 +59,7 @@ int gpufhe_plan_create(gpufhe_ctx* h, uint32_t nops, const gpufhe_op* ops, uint6
 
 int gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t s) {
     if (!plan) { gfx::set_error("null plan"); return GPUFHE_EINVAL; }
+    pl::tune(*plan->p, s);
     cudaError_t e = pl::launch(*plan->p, s);
     if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
     return GPUFHE_OK;
@@ -71,10 +72,20 @@ int gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t s) 
     return GPUFHE_OK;
 }
 
+uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan) {
+    if (!plan) return 0;
+    const pl::Plan& p = *plan->p;
+    return (p.p5_async ? 1u : 0u) | (p.mix ? 2u : 0u) | (p.tuned ? 4u : 0u);
+}
+
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     if (!plan) return 0;
     uint32_t k = 0;
-    for (int i = 0; i < pl::NPHASE; ++i) k += (plan->p->job_cnt[i][0] ? 1 : 0) + (plan->p->job_cnt[i][1] ? 1 : 0);
+    const pl::Plan& p = *plan->p;
+    for (int i = 0; i < pl::NPHASE; ++i) {
+        if (p.mix && p.job_cnt[i][2]) k += 1;
+        else k += (p.job_cnt[i][0] ? 1 : 0) + (p.job_cnt[i][1] ? 1 : 0);
+    }
     return k;
 }
 
@@ -92,6 +103,7 @@ int gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint
             if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
         }
     }
+    pl::tune(*plan->p, s);
     cudaError_t e = pl::launch(p, s);
     if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
     for (size_t i = 0; i < p.ops.size(); ++i) {

@@ -209,6 +209,19 @@ void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
     keys_[id] = k;
 }
 
+bool Context::tuned_choice(uint64_t key, int& choice) const {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = tune_.find(key);
+    if (it == tune_.end()) return false;
+    choice = it->second;
+    return true;
+}
+
+void Context::set_tuned_choice(uint64_t key, int choice) const {
+    std::lock_guard<std::mutex> g(mu_);
+    tune_[key] = choice;
+}
+
 const Key* Context::key(uint64_t id) const {
     std::lock_guard<std::mutex> g(mu_);
     auto it = keys_.find(id);

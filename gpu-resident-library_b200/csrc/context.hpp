@@ -86,6 +86,10 @@ public:
     size_t key_bytes() const;
     size_t resident_bytes() const { return table_bytes_ + key_bytes(); }
 
+    // Autotuner cache: launch-schedule choice per batch shape key.
+    bool tuned_choice(uint64_t key, int& choice) const;
+    void set_tuned_choice(uint64_t key, int choice) const;
+
 private:
     uint32_t n_, logn_, alpha_, dnum_;
     int device_;
@@ -95,6 +99,7 @@ private:
     std::vector<void*> allocs_;
     size_t table_bytes_ = 0;
     std::map<uint64_t, Key> keys_;
+    mutable std::map<uint64_t, int> tune_;
     mutable std::mutex mu_;
     void* dalloc(size_t bytes);
     template <class T>

@@ -13,36 +13,37 @@ namespace pl {
 
 namespace {
 
-template <int LOGN, bool FP>
+// PATH 0 / 1: the integer / FP64 job segment of a phase; PATH 2: the mixed
+// segment (both kinds interleaved, one launch).
+template <int LOGN, int PATH>
 struct Variant {
     static void attrs() {
         using G = ntt::Geo<LOGN>;
-        cudaFuncSetAttribute(p1_inv_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-        cudaFuncSetAttribute(p2_inv_col<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-        cudaFuncSetAttribute(p3_modup_fwd_col<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-        cudaFuncSetAttribute(p4_modup_fwd_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-        cudaFuncSetAttribute(p6_moddown_inv_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-        cudaFuncSetAttribute(p8_moddown_fwd_col<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
-        cudaFuncSetAttribute(p9_final_fwd_row<LOGN, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p1_inv_row<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p2_inv_col<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+        cudaFuncSetAttribute(p3_modup_fwd_col<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+        cudaFuncSetAttribute(p4_modup_fwd_row<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p6_moddown_inv_row<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p8_moddown_fwd_col<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+        cudaFuncSetAttribute(p9_final_fwd_row<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
     }
-    // Phase k of the jobs routed to this arithmetic path (P5 and P7 have one
-    // integer kernel and are launched by the caller).
+    // Phase k of the jobs in segment PATH (P5 and P7 have one integer kernel
+    // and are launched by the caller).
     static void phase(int k, const Plan& p, cudaStream_t s) {
         using G = ntt::Geo<LOGN>;
-        const int v = FP ? 1 : 0;
-        const uint32_t cnt = p.job_cnt[k][v];
+        const uint32_t cnt = p.job_cnt[k][PATH];
         if (!cnt) return;
         const DevCtx& D = p.dc;
         const PairDesc* pd = p.d_pairs;
-        const uint2* J = p.d_jobs + p.job_off[k][v];
+        const uint2* J = p.d_jobs + p.job_off[k][PATH];
         switch (k) {
-            case 0: p1_inv_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
-            case 1: p2_inv_col<LOGN, FP><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
-            case 2: p3_modup_fwd_col<LOGN, FP><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
-            case 3: p4_modup_fwd_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
-            case 5: p6_moddown_inv_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
-            case 7: p8_moddown_fwd_col<LOGN, FP><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
-            case 8: p9_final_fwd_row<LOGN, FP><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 0: p1_inv_row<LOGN, PATH><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 1: p2_inv_col<LOGN, PATH><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
+            case 2: p3_modup_fwd_col<LOGN, PATH><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
+            case 3: p4_modup_fwd_row<LOGN, PATH><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 5: p6_moddown_inv_row<LOGN, PATH><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 7: p8_moddown_fwd_col<LOGN, PATH><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
+            case 8: p9_final_fwd_row<LOGN, PATH><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
             default: break;
         }
     }
@@ -55,13 +56,17 @@ struct Launcher {
         static bool done = false;
         static uint32_t mac_dnum = 0;
         if (!done) {
-            Variant<LOGN, false>::attrs();
-            Variant<LOGN, true>::attrs();
+            Variant<LOGN, 0>::attrs();
+            Variant<LOGN, 1>::attrs();
+            Variant<LOGN, 2>::attrs();
             cudaFuncSetAttribute(p7_moddown_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
             done = true;
         }
         if (dnum > mac_dnum) {
             cudaFuncSetAttribute(p5_mac<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(dnum));
+            if (mac_async_ok(dnum))
+                cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     maca_smem((int)dnum));
             mac_dnum = dnum;
         }
     }
@@ -73,16 +78,22 @@ struct Launcher {
         for (int k = 0; k < NPHASE; ++k) {
             if (!(mask >> k & 1)) continue;
             if (k == 4) {
-                if (p.job_cnt[4][0])
+                if (!p.job_cnt[4][0]) continue;
+                if (p.p5_async && mac_async_ok(D.dnum))
+                    p5_mac_async<LOGN><<<p.job_cnt[4][0] * MAC_TILES, MACA_NT, maca_smem((int)D.dnum), s>>>(
+                        D, p.d_pairs, p.d_mac_jobs, p.d_plist);
+                else
                     p5_mac<LOGN><<<p.job_cnt[4][0] * MAC_TILES, MAC_NT, mac_smem(D.dnum), s>>>(D, p.d_pairs,
                                                                                             p.d_mac_jobs, p.d_plist);
             } else if (k == 6) {
                 if (p.job_cnt[6][0])
                     p7_moddown_inv_col<LOGN><<<p.job_cnt[6][0] * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(
                         D, p.d_pairs, p.d_jobs + p.job_off[6][0]);
+            } else if (p.mix && p.job_cnt[k][0] && p.job_cnt[k][1]) {
+                Variant<LOGN, 2>::phase(k, p, s);
             } else {
-                Variant<LOGN, false>::phase(k, p, s);
-                Variant<LOGN, true>::phase(k, p, s);
+                Variant<LOGN, 0>::phase(k, p, s);
+                Variant<LOGN, 1>::phase(k, p, s);
             }
         }
     }
@@ -122,8 +133,8 @@ struct HostTables {
     std::vector<uint2> jobs;       // all phases, concatenated
     std::vector<uint4> mac_jobs;
     std::vector<uint32_t> plist;
-    size_t job_off[NPHASE][2] = {};     // [phase][integer, FP64]
-    uint32_t job_cnt[NPHASE][2] = {};
+    size_t job_off[NPHASE][3] = {};     // [phase][integer, FP64, mixed]
+    uint32_t job_cnt[NPHASE][3] = {};
 };
 
 static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const std::vector<u64*>& ws_ptrs,
@@ -209,9 +220,23 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
             }
             T.job_cnt[k][v] = (uint32_t)(T.jobs.size() - T.job_off[k][v]);
         }
+        // mixed segment: the two lists interleaved in proportion, FP64 jobs
+        // tagged with JOB_FP, so neighbouring CTAs load different pipes
+        T.job_off[k][2] = T.jobs.size();
+        const uint32_t na = T.job_cnt[k][0], nb = T.job_cnt[k][1];
+        if (split && na && nb) {
+            const size_t oa = T.job_off[k][0], ob = T.job_off[k][1];
+            uint32_t ia = 0, ib = 0;
+            while (ia < na || ib < nb) {
+                const bool take_b = ia == na || (ib < nb && (uint64_t)ib * na <= (uint64_t)ia * nb);
+                if (take_b) { uint2 j = T.jobs[ob + ib++]; j.y |= JOB_FP; T.jobs.push_back(j); }
+                else { const uint2 j = T.jobs[oa + ia++]; T.jobs.push_back(j); }
+            }
+        }
+        T.job_cnt[k][2] = (uint32_t)(T.jobs.size() - T.job_off[k][2]);
     }
     T.job_cnt[4][0] = (uint32_t)T.mac_jobs.size();
-    T.job_cnt[4][1] = 0;
+    T.job_cnt[4][1] = T.job_cnt[4][2] = 0;
 }
 
 Plan::Plan() : staging(std::make_unique<HostTables>()) {}
@@ -260,7 +285,7 @@ static void commit(Plan& p, const HostTables& T, const std::vector<Op>& ops, cud
     p.d_mac_jobs = reinterpret_cast<uint4*>(d + b_pairs + b_jobs);
     p.d_plist = reinterpret_cast<uint32_t*>(d + b_pairs + b_jobs + b_mac);
     for (int k = 0; k < NPHASE; ++k)
-        for (int v = 0; v < 2; ++v) { p.job_off[k][v] = T.job_off[k][v]; p.job_cnt[k][v] = T.job_cnt[k][v]; }
+        for (int v = 0; v < 3; ++v) { p.job_off[k][v] = T.job_off[k][v]; p.job_cnt[k][v] = T.job_cnt[k][v]; }
     p.nops = (uint32_t)ops.size();
     p.ops = ops;
     p.pairs_host = T.pairs;
@@ -269,6 +294,7 @@ static void commit(Plan& p, const HostTables& T, const std::vector<Op>& ops, cud
 std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words) {
     if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
     auto plan = std::make_unique<Plan>();
+    plan->ctx = &c;
     plan->dc = c.dev();
     plan->logn = c.logn();
     size_t need = 0;
@@ -300,8 +326,10 @@ void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops,
     for (u64* w : ws_ptrs)
         if (!w || (reinterpret_cast<uintptr_t>(w) & 15)) throw std::invalid_argument("workspace must be 16-byte aligned");
     for (const Op& op : ops) validate(c, op);
+    p.ctx = &c;
     p.dc = c.dev();
     p.logn = c.logn();
+    p.tuned = false;
     HostTables& T = *p.staging;
     fill_tables(c, ops, ws_ptrs, T);
     commit(p, T, ops, s, true);
@@ -335,6 +363,59 @@ void rebind(Plan& p, uint32_t idx, const Op& op, const gfx::Context& c, cudaStre
     p.pairs_host[idx] = P;
     p.ops[idx] = op;
     k_set_pair<<<1, 1, 0, s>>>(p.d_pairs + idx, P);
+}
+
+namespace {
+uint64_t tune_key(const Plan& p) {
+    uint32_t cls = 0;
+    while ((1u << (cls + 1)) <= p.nops) ++cls;   // batch-size class: floor(log2(nops))
+    return ((uint64_t)p.logn << 40) | ((uint64_t)p.dc.dnum << 32) | cls;
+}
+void apply_choice(Plan& p, int choice) {
+    p.p5_async = (choice & 1) && mac_async_ok(p.dc.dnum);
+    p.mix = (choice & 2) != 0;
+}
+}  // namespace
+
+void tune(Plan& p, cudaStream_t s) {
+    if (p.tuned || !p.nops || !p.ctx) return;
+    const gfx::Context& c = *p.ctx;
+    const uint64_t key = tune_key(p);
+    int choice = 0;
+    if (c.tuned_choice(key, choice)) {
+        apply_choice(p, choice);
+        p.tuned = true;
+        return;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+    for (const Op& op : p.ops)
+        if (op.mode == RESCALE) return;          // may be in place: re-running would change its input
+    const int ncand = mac_async_ok(p.dc.dnum) ? 4 : 2;
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return;
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
+    float best = 0;
+    int best_choice = 2;
+    for (int k = 0; k < 4; ++k) {
+        const int cand = ncand == 4 ? k : (k & 2);
+        if (ncand == 2 && (k & 1)) continue;
+        apply_choice(p, cand);
+        launch(p, s);                            // warm
+        cudaEventRecord(a, s);
+        launch(p, s);
+        launch(p, s);
+        cudaEventRecord(b, s);
+        if (cudaEventSynchronize(b) != cudaSuccess) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (k == 0 || ms < best) { best = ms; best_choice = cand; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    apply_choice(p, best_choice);
+    c.set_tuned_choice(key, best_choice);
+    p.tuned = true;
 }
 
 cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask) {

@@ -31,6 +31,8 @@
 //   P8 fwd-col  (pair,c,i)     ModDown conversion + SwitchModulus prologue   -> Z
 //   P9 fwd-row  (pair,c,i)     NTT row stages, final combine                -> out
 #pragma once
+#include <type_traits>
+
 #include "context.hpp"
 #include "ntt.cuh"
 
@@ -124,6 +126,22 @@ __device__ __forceinline__ auto twi_of(const DevCtx& D, u32 qp, int logn) {
     else return ntt::TwPacked{D.twi + ((size_t)qp << logn)};
 }
 
+// Arithmetic path of a transform kernel launch: PATH 0 = integer jobs only,
+// 1 = FP64 jobs only, 2 = a mixed job list whose FP64 jobs carry bit 31 of
+// job.y (integer- and FP64-bound CTAs then share each SM's pipes).
+constexpr u32 JOB_FP = 0x80000000u;
+template <int PATH, class F>
+__device__ __forceinline__ void on_path(uint2& jb, F&& f) {
+    if constexpr (PATH == 2) {
+        const bool fp = (jb.y & JOB_FP) != 0;
+        jb.y &= ~JOB_FP;
+        if (fp) f(std::true_type{});
+        else f(std::false_type{});
+    } else {
+        f(std::integral_constant<bool, PATH == 1>{});
+    }
+}
+
 // Column-tile staging: the prologue of a column pass (a basis conversion)
 // is computed for the whole tile into shared memory before the first round,
 // reading its inputs as 16-byte column pairs with the loads of CS_VB pairs
@@ -173,12 +191,11 @@ __device__ __forceinline__ void mac_terms(u64 (&lo)[VB][2], u64 (&hi)[VB][2], co
 
 // ------------------------------------------------------------------ P1
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
-p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__device__ __forceinline__ void p1_inv_row_body(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint2 jb,
+                                              const u32 tile) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
-    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
+    const u32 R0 = tile * G::RB;
     const PairDesc& P = pairs[jb.x];
     const u32 i = jb.y;
     const ModC m = D.mod[i];
@@ -201,14 +218,21 @@ p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
     ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8, true>(sm, twi_of<FP>(D, i, LOGN), R0, ar, st);
 }
 
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p1_inv_row_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
+}
+
 // ------------------------------------------------------------------ P2
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
-p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__device__ __forceinline__ void p2_inv_col_body(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint2 jb,
+                                              const u32 tile) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
-    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
+    const int c0 = tile * G::C;
     const PairDesc& P = pairs[jb.x];
     const u32 i = jb.y;
     const ModC m = D.mod[i];
@@ -222,16 +246,23 @@ p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __re
     ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, twi_of<FP>(D, i, LOGN), ar_of<FP>(m), ld, st);
 }
 
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p2_inv_col_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
+}
+
 // ------------------------------------------------------------------ P3
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
-p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__device__ __forceinline__ void p3_modup_fwd_col_body(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint2 jb,
+                                              const u32 tile) {
     using G = ntt::Geo<LOGN>;
     using CS = ColStage<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
     __shared__ u64 cst[MAXA];
-    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
-    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
+    const int c0 = tile * G::C;
     const PairDesc& P = pairs[jb.x];
     const u32 L = P.L, K = D.K, QlP = L + K;
     const u32 p = jb.y / QlP, i = jb.y % QlP;
@@ -270,15 +301,22 @@ p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(sm, twf_of<FP>(D, qp, LOGN), ar_of<FP>(m), ld, stf);
 }
 
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p3_modup_fwd_col_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
+}
+
 // ------------------------------------------------------------------ P4
 // NTT row stages of one digit tower; output reduced to [0, 2q).
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
-p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__device__ __forceinline__ void p4_modup_fwd_row_body(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint2 jb,
+                                              const u32 tile) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
-    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
+    const u32 R0 = tile * G::RB;
     const PairDesc& P = pairs[jb.x];
     const u32 L = P.L, QlP = L + D.K;
     const u32 p = jb.y / QlP, i = jb.y % QlP;
@@ -292,6 +330,14 @@ p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
         Y[rl * 256 + c] = csub(ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)]), m.two_q);
     });
+}
+
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p4_modup_fwd_row_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
 }
 
 // ------------------------------------------------------------------ P5
@@ -480,15 +526,172 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
     }
 }
 
+// P5, pipelined form (dnum small enough for the staging buffers): 256
+// threads, each owning one 16-byte pair of the 512-element tile. While a
+// pair is multiplied, the tiles of the next pair (the four tensor inputs or
+// the keyswitch input, and every other digit of tower i) are already in
+// flight into the other shared-memory stage with cp.async; each thread copies
+// and later reads only its own 16 bytes, so the stages need no barrier.
+// Results equal p5_mac's word for word.
+constexpr int MACA_NT = 256;
+constexpr int MACA_IN = 4;   // stage slots for tensor / keyswitch inputs
+__host__ __device__ constexpr int maca_slots(int dnum) { return MACA_IN + dnum; }
+__host__ __device__ constexpr int maca_smem(int dnum) {
+    return (2 * dnum + 2 * maca_slots(dnum)) * MAC_TILE * 8;
+}
+
+__device__ __forceinline__ void cp_async16(u64* smem, const u64* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int LOGN>
+__global__ void __launch_bounds__(MACA_NT)
+p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
+             const u32* __restrict__ plist) {
+    constexpr int TILES = (1 << LOGN) / MAC_TILE;
+    extern __shared__ __align__(16) u64 sm[];   // key [dnum][2][TILE] | stage [2][slots][TILE]
+    const uint4 jb = jobs[blockIdx.x / TILES];
+    const u32 tile0 = (blockIdx.x % TILES) * MAC_TILE;
+    const u32 r = jb.x;
+    const ModC m = D.mod[r];
+    const u32 dnum = D.dnum, slots = maca_slots((int)dnum);
+    u64* stage = sm + 2 * dnum * MAC_TILE;
+    const PairDesc& P0 = pairs[plist[jb.y]];
+    for (u32 k = threadIdx.x; k < dnum * (MAC_TILE / 2); k += MACA_NT) {
+        const u32 p = k / (MAC_TILE / 2), e = 2 * (k % (MAC_TILE / 2));
+        const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0 + e;
+        *reinterpret_cast<ulonglong2*>(sm + (2 * p) * MAC_TILE + e) = ld2(P0.kbv + off);
+        *reinterpret_cast<ulonglong2*>(sm + (2 * p + 1) * MAC_TILE + e) = ld2(P0.kav + off);
+    }
+    __syncthreads();
+    const bool is_p = r >= D.fullQ;
+    const u32 e = 2 * threadIdx.x;               // this thread's pair within the tile
+    const u32 K = D.K;
+    // queue the copies of pair g into stage buffer b (one commit group per pair)
+    auto issue = [&](u32 g, int b) {
+        const PairDesc& P = pairs[plist[jb.y + g]];
+        const u32 L = P.L, QlP = L + K;
+        const u32 i = is_p ? L + (r - D.fullQ) : r;
+        const u32 pin = is_p ? 0xffffffffu : i / D.alpha;
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        u64* sb = stage + (size_t)b * slots * MAC_TILE + e;
+        const size_t o = ((size_t)i << LOGN) + tile0 + e;
+        if (!is_p) {
+            if (P.mode == EMR) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) cp_async16(sb + k * MAC_TILE, P.in[k] + o);
+            } else if (P.mode == KS) {
+                cp_async16(sb + MAC_TILE, P.in[0] + o);
+            }
+        }
+        const u32 nparts = D.lvl[L].nparts;
+        for (u32 p = 0; p < nparts; ++p)
+            if (p != pin) cp_async16(sb + (MACA_IN + p) * MAC_TILE, slot_ptr(P, w.Y + p * QlP + i, LOGN) + tile0 + e);
+        cp_async_commit();
+    };
+    issue(0, 0);
+    for (u32 g = 0; g < jb.z; ++g) {
+        if (g + 1 < jb.z) issue(g + 1, (int)((g + 1) & 1));
+        else cp_async_commit();                  // empty group keeps the wait count uniform
+        cp_async_wait1();                        // pair g's copies have landed
+        const PairDesc& P = pairs[plist[jb.y + g]];
+        const u32 L = P.L;
+        const u32 i = is_p ? L + (r - D.fullQ) : r;
+        const Level& lv = D.lvl[L];
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        const u32 nparts = lv.nparts;
+        const u32 pin = is_p ? 0xffffffffu : i / D.alpha;
+        const bool emr = P.mode == EMR;
+        const u64* sb = stage + (size_t)(g & 1) * slots * MAC_TILE + e;
+        ulonglong2 s{0, 0}, t0{0, 0}, t1{0, 0};
+        if (!is_p) {
+            if (emr) {
+                const ulonglong2 x0 = ld2(sb), x1 = ld2(sb + MAC_TILE);
+                const ulonglong2 y0 = ld2(sb + 2 * MAC_TILE), y1 = ld2(sb + 3 * MAC_TILE);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const u64 a0 = v2get(x0, j), a1 = v2get(x1, j), b0 = v2get(y0, j), b1 = v2get(y1, j);
+                    v2set(s, j, mulmod(a1, b1, m));
+                    v2set(t0, j, mulmod(a0, b0, m));
+                    u64 lo, hi;
+                    mul_wide(a0, b1, lo, hi);
+                    mac_wide(lo, hi, a1, b0);
+                    v2set(t1, j, barrett(lo, hi, m));
+                }
+            } else if (P.mode == ROT) {
+                const u64* src = P.in[1] + ((size_t)i << LOGN);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) v2set(s, j, src[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
+            } else {
+                s = ld2(sb + MAC_TILE);
+            }
+        }
+        u64 a0l[2] = {0, 0}, a0h[2] = {0, 0}, a1l[2] = {0, 0}, a1h[2] = {0, 0};
+        for (u32 p = 0; p < nparts; ++p) {
+            const ulonglong2 dv = p == pin ? s : ld2(sb + (MACA_IN + p) * MAC_TILE);
+            const ulonglong2 kbv = ld2(sm + (2 * p) * MAC_TILE + e);
+            const ulonglong2 kav = ld2(sm + (2 * p + 1) * MAC_TILE + e);
+            mac_wide(a0l[0], a0h[0], dv.x, kbv.x);
+            mac_wide(a0l[1], a0h[1], dv.y, kbv.y);
+            mac_wide(a1l[0], a1h[0], dv.x, kav.x);
+            mac_wide(a1l[1], a1h[1], dv.y, kav.y);
+        }
+        ulonglong2 r0, r1;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            v2set(r0, j, barrett(a0l[j], a0h[j], m));
+            v2set(r1, j, barrett(a1l[j], a1h[j], m));
+        }
+        const u64 q = m.q;
+        if (is_p) {
+            *reinterpret_cast<ulonglong2*>(slot_ptr(P, w.RP + (i - L), LOGN) + tile0 + e) = r0;
+            *reinterpret_cast<ulonglong2*>(slot_ptr(P, w.RP + K + (i - L), LOGN) + tile0 + e) = r1;
+            continue;
+        }
+        const u64 pv = D.pinv[i], pvp = D.pinvp[i];
+        ulonglong2 o0, o1;
+        u64 *d0, *d1;
+        if (!emr) {   // keyswitch / rotation: W = res * P^-1
+            d0 = slot_ptr(P, w.W + i, LOGN);
+            d1 = slot_ptr(P, w.W + L + i, LOGN);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                v2set(o0, j, shoup(v2get(r0, j), pv, pvp, q));
+                v2set(o1, j, shoup(v2get(r1, j), pv, pvp, q));
+            }
+        } else {
+            const bool drop = i == L - 1;
+            const u64 s1 = lv.s1[i], s1p = lv.s1p[i], ps1 = lv.ps1[i], ps1p = lv.ps1p[i];
+            d0 = drop ? slot_ptr(P, w.U, LOGN) : slot_ptr(P, w.W + i, LOGN);
+            d1 = drop ? slot_ptr(P, w.U + 1, LOGN) : slot_ptr(P, w.W + L + i, LOGN);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const u64 ta = v2get(t0, j), tb = v2get(t1, j), ra = v2get(r0, j), rb = v2get(r1, j);
+                if (drop) {
+                    v2set(o0, j, csub(ta + shoup(ra, pv, pvp, q), q));
+                    v2set(o1, j, csub(tb + shoup(rb, pv, pvp, q), q));
+                } else {
+                    v2set(o0, j, csub(csub(shoup_lazy(ta, s1, s1p, q) + shoup_lazy(ra, ps1, ps1p, q), m.two_q), q));
+                    v2set(o1, j, csub(csub(shoup_lazy(tb, s1, s1p, q) + shoup_lazy(rb, ps1, ps1p, q), m.two_q), q));
+                }
+            }
+        }
+        *reinterpret_cast<ulonglong2*>(d0 + tile0 + e) = o0;
+        *reinterpret_cast<ulonglong2*>(d1 + tile0 + e) = o1;
+    }
+}
+
 // ------------------------------------------------------------------ P6
 // INTT row stages of U[c] (t = 0, EvalMult+Rescale only) and RP[c][t-1].
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
-p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__device__ __forceinline__ void p6_moddown_inv_row_body(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint2 jb,
+                                              const u32 tile) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
-    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
+    const u32 R0 = tile * G::RB;
     const PairDesc& P = pairs[jb.x];
     const u32 L = P.L, K = D.K;
     const u32 c = jb.y / (K + 1), t = jb.y % (K + 1);
@@ -504,6 +707,14 @@ p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
     __syncthreads();
     auto st = [&](int rl, int cc, u64 v) { X[rl * 256 + cc] = v; };
     ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, twi_of<FP>(D, qp, LOGN), R0, ar, st);
+}
+
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p6_moddown_inv_row_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
 }
 
 // ------------------------------------------------------------------ P7
@@ -618,12 +829,11 @@ __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 
 }
 
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 2)
-p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__device__ __forceinline__ void p8_moddown_fwd_col_body(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint2 jb,
+                                              const u32 tile) {
     extern __shared__ __align__(16) u64 sm[];
     __shared__ u64 ci[gfx::MAXP];
-    const uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
-    const int c0 = (blockIdx.x % ntt::Geo<LOGN>::COL_TILES) * ntt::Geo<LOGN>::C;
+    const int c0 = tile * ntt::Geo<LOGN>::C;
     const PairDesc& P = pairs[jb.x];
     const u32 c = jb.y / P.L, i = jb.y % P.L;
     if (threadIdx.x < D.K) ci[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + i];
@@ -633,14 +843,21 @@ p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
     else p8_body<LOGN, KS, FP>(D, P, c, i, c0, sm, ci);
 }
 
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 2)
+p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p8_moddown_fwd_col_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
+}
+
 // ------------------------------------------------------------------ P9
 template <int LOGN, bool FP>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
-p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+__device__ __forceinline__ void p9_final_fwd_row_body(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint2 jb,
+                                              const u32 tile) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
-    const uint2 jb = jobs[blockIdx.x / G::ROW_TILES];
-    const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
+    const u32 R0 = tile * G::RB;
     const PairDesc& P = pairs[jb.x];
     const u32 L = P.L, K = D.K, mode = P.mode;
     const u32 c = jb.y / L, i = jb.y % L;
@@ -673,6 +890,14 @@ p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
             }
             out[e] = r;
         });
+}
+
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p9_final_fwd_row_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
 }
 
 }  // namespace pl

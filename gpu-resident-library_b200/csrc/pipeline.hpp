@@ -26,8 +26,8 @@ struct Plan {
     uint32_t logn = 0, nops = 0;
     PairDesc* d_pairs = nullptr;
     uint2* d_jobs = nullptr;
-    size_t job_off[NPHASE][2] = {};    // [phase][integer kernel, FP64 kernel]
-    uint32_t job_cnt[NPHASE][2] = {};
+    size_t job_off[NPHASE][3] = {};    // [phase][integer jobs, FP64 jobs, both interleaved]
+    uint32_t job_cnt[NPHASE][3] = {};
     uint4* d_mac_jobs = nullptr;
     uint32_t* d_plist = nullptr;
     u64* ws = nullptr;
@@ -35,6 +35,11 @@ struct Plan {
     bool own_ws = false;
     std::vector<Op> ops;      // host copy (device pointers and levels)
     std::vector<PairDesc> pairs_host;
+    // launch schedule (chosen by tune() or the context's tuning cache)
+    bool p5_async = false;             // pipelined P5 instead of the register-prefetch one
+    bool mix = true;                   // one launch per phase over the interleaved job list
+    bool tuned = false;
+    const gfx::Context* ctx = nullptr;
     void* d_blob = nullptr;            // device tables (pairs, jobs, P5 groups, pair lists)
     void* h_blob = nullptr;            // pinned host mirror of d_blob
     size_t blob_cap = 0;
@@ -55,8 +60,17 @@ void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops,
                      cudaStream_t s);
 // mask selects phases P1..P9 (bit k = phase k+1); 0x1ff runs the whole batch.
 cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
+// Picks the launch schedule of `p` (P5 variant; integer and FP64 transform
+// jobs as two launches or one interleaved launch): from the context's tuning cache when it holds
+// this shape (ring size, digits, batch-size class), else by timing every
+// candidate with CUDA events on `s` and caching the fastest. Timing re-runs
+// the batch, so it is skipped (defaults kept) while `s` is capturing a graph
+// or when an operation writes over its own input (in-place rescale).
+void tune(Plan& p, cudaStream_t s);
 constexpr int MAC_MAX_DNUM = 16;
 inline int mac_smem(uint32_t dnum) { return (int)(dnum * 2 * MAC_TILE * sizeof(u64)); }
+// The pipelined P5 runs when two CTAs' key tiles and staging buffers fit in one SM.
+inline bool mac_async_ok(uint32_t dnum) { return maca_smem((int)dnum) <= 113 * 1024; }
 int input_count(uint32_t mode);
 // Rebinds operation `idx` of a built plan to new buffers / mode (same level
 // and job shape) by a one-thread kernel on `s`: no allocation and no host

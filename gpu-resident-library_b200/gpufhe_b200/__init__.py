@@ -54,6 +54,7 @@ _API: dict = {
     "gpufhe_run_ops": (I32, [VP, U32, VP, VP]),
     "gpufhe_plan_launch_phase": (I32, [VP, U32, VP]),
     "gpufhe_plan_kernel_count": (U32, [VP]),
+    "gpufhe_plan_schedule": (U32, [VP]),
     "gpufhe_plan_launch_host": (I32, [VP, VP, VP, VP]),
     "gpufhe_native_primes": (I32, [VP, U32, U32, U32, VP, U32]),
     "gpufhe_native_root": (U64, [U32, U64]),
@@ -197,6 +198,11 @@ class Plan:
 
     def kernel_count(self):
         return int(lib().gpufhe_plan_kernel_count(self.h))
+
+    def schedule(self):
+        """Autotuner choice: {'p5_async', 'mixed_paths', 'tuned'}."""
+        b = int(lib().gpufhe_plan_schedule(self.h))
+        return {"p5_async": bool(b & 1), "mixed_paths": bool(b & 2), "tuned": bool(b & 4)}
 
     def launch_host(self, h_in, h_out, stream=None):
         """h_in: list of 4 host pointers per op (0 for unused); h_out: 2 per op."""

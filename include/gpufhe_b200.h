@@ -113,14 +113,21 @@ uint64_t gpufhe_op_workspace_bytes(gpufhe_ctx* ctx, uint32_t level);
  * d_ws: caller workspace of ws_bytes, or NULL for a plan-owned one. */
 int  gpufhe_plan_create(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, uint64_t* d_ws, uint64_t ws_bytes,
                         gpufhe_plan** out);
-/* Launches the nine phase kernels for the whole batch on `stream`
- * (kernel launches only: capturable in a CUDA graph). */
+/* Launches the phase kernels for the whole batch on `stream` (kernel
+ * launches only: capturable in a CUDA graph). The first launch outside
+ * capture runs the autotuner, which re-runs the batch to time the candidate
+ * schedules (skipped for in-place rescales). */
 int  gpufhe_plan_launch(gpufhe_plan* plan, cudaStream_t stream);
 void gpufhe_plan_destroy(gpufhe_plan* plan);
 /* One phase (0..8 = P1..P9) only, for per-kernel timing. */
 int  gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t stream);
 /* Number of kernels one gpufhe_plan_launch enqueues. */
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
+/* Launch schedule chosen by the autotuner (first gpufhe_plan_launch outside
+ * graph capture, cached per context and batch shape): bit 0 = pipelined P5,
+ * bit 1 = integer and FP64 transform jobs of a phase interleaved in one
+ * launch (else two launches), bit 2 = tuned. */
+uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan);
 /* Host-buffer form: copies h_in[4*i+k] (host, level*n words) into op i's
  * device inputs, launches the batch and copies each op's outputs back into
  * h_out[2*i+k]; synchronizes `stream`. NULL entries are skipped. Pinned host
