@@ -398,6 +398,89 @@ def ntt_isolation(G, torch, dev, local, cur, gen):
     return ntt
 
 
+# ---------------------------------------------------------------- rotation batch
+ROT_TOWERS, ROT_COUNT, ROT_HOIST = 10, 256, 16
+
+
+def rotation_batch(G, torch, dev, local, gen, steps):
+    """256 ciphertexts at N=2^16, 10 towers, each rotated by a seeded index from
+    {+-1, +-2, ..., +-2^14} with its own resident key; then hoisted: 16
+    ciphertexts x 16 rotations sharing one ModUp each. Rotations/s by CUDA
+    events over graph replays, plus the resident key bytes."""
+    n = 1 << N_LOG
+    q0 = G.native_primes(1, 60, n)
+    Q = np.concatenate([q0, G.native_primes(ROT_TOWERS - 1, 50, n, avoid=list(q0))])
+    P = G.native_primes(K_SPECIAL, 60, n, avoid=list(Q))
+    ctx = G.Context(n, Q, P, ALPHA, device=local)
+    steps_r = [s * (1 << j) for j in range(15) for s in (1, -1)]
+    gal = [galois_element(r, n) for r in steps_r]
+    rows = -(-ROT_TOWERS // ALPHA) * (ROT_TOWERS + K_SPECIAL)
+    rng = np.random.default_rng(SEED + 44)
+    pool = rng.integers(0, 1 << 49, 2 * rows * n, dtype=np.uint64)
+    for j, k in enumerate(gal):
+        key = np.roll(pool, 104729 * (j + 1))
+        ctx.set_key(k, key[: rows * n], key[rows * n:])
+    evk_bytes = ctx.resident_bytes()
+    L = ROT_TOWERS
+
+    def ct():
+        t = torch.empty((2, L, n), dtype=torch.int64, device=dev)
+        for i in range(L):
+            t[:, i].random_(0, int(Q[i]), generator=gen)
+        return t
+
+    def timed(specs):
+        wsb = sum(ctx.workspace_bytes(sp["level"]) for sp in specs)
+        ws = torch.empty(wsb // 8, dtype=torch.int64, device=dev)
+        plan = G.Plan(ctx, specs, ws.data_ptr(), wsb)
+        st = torch.cuda.Stream(device=dev)
+        plan.launch(st.cuda_stream)          # autotuner + attributes, outside capture
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=st):
+            plan.launch(torch.cuda.current_stream().cuda_stream)
+        for _ in range(3):
+            graph.replay()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            graph.replay()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
+        sched = plan.schedule()
+        del graph, plan, ws
+        return ms, sched
+
+    idx = np.random.default_rng(SEED + 45).integers(0, len(gal), ROT_COUNT)
+    cts = [ct() for _ in range(ROT_COUNT)]
+    outs = [torch.empty((2, L, n), dtype=torch.int64, device=dev) for _ in range(ROT_COUNT)]
+    specs = [dict(level=L, mode=G.ROTATE, key_id=gal[k], galois=gal[k],
+                  inp=[c[0].data_ptr(), c[1].data_ptr()], out=[o[0].data_ptr(), o[1].data_ptr()])
+             for c, o, k in zip(cts, outs, idx)]
+    ms_plain, sched_plain = timed(specs)
+    del cts
+    hrng = np.random.default_rng(SEED + 46)
+    hcts = [ct() for _ in range(ROT_COUNT // ROT_HOIST)]
+    hspecs = []
+    for g, c in enumerate(hcts):
+        for k in hrng.choice(len(gal), ROT_HOIST, replace=False):
+            o = outs[len(hspecs)]
+            hspecs.append(dict(level=L, mode=G.ROTATE_HOISTED, key_id=gal[k], galois=gal[k],
+                               inp=[c[0].data_ptr(), c[1].data_ptr()], out=[o[0].data_ptr(), o[1].data_ptr()]))
+    ms_hoist, sched_hoist = timed(hspecs)
+    del hcts, outs
+    ctx.close()
+    return {"workload": "256 ciphertexts, N=2^16, 10 towers (1x60+9x50), P=3x60, alpha=3, index from "
+                        "{+-1,...,+-2^14} with resident keys; hoisted: 16 ciphertexts x 16 rotations",
+            "rotations_per_s": ROT_COUNT / (ms_plain * 1e-3), "ms_per_batch": ms_plain, "schedule": sched_plain,
+            "hoisted_rotations_per_s": ROT_COUNT / (ms_hoist * 1e-3), "hoisted_ms_per_batch": ms_hoist,
+            "hoisted_schedule": sched_hoist, "resident_bytes": evk_bytes,
+            "distinct_keys": len(set(gal)), "evk_bytes": len(set(gal)) * 2 * rows * n * 8,
+            "note": "rotations by +2^14 and -2^14 share one Galois element at N=2^16 (2^15 slots)"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_gpu(args):
     import torch
@@ -417,6 +500,12 @@ def run_gpu(args):
         gen.manual_seed(SEED)
         res = ntt_isolation(G, torch, dev, local, torch.cuda.current_stream().cuda_stream, gen)
         print(json.dumps({"section": "ntt", "ntt_kernel_isolation": res}), flush=True)
+        return 0
+    if args.section == "rot":
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SEED)
+        res = rotation_batch(G, torch, dev, local, gen, max(3, min(args.steps, 10)))
+        print(json.dumps({"section": "rot", "rotation_batch": res}), flush=True)
         return 0
     n = 1 << N_LOG
     Q, P = chain(G.native_primes, n)
@@ -579,6 +668,11 @@ def run_gpu(args):
     # kernel isolation: 64 polys x 12 towers x 2^16
     ntt = None if args.no_ntt else ntt_isolation(G, torch, dev, local, cur, gen)
 
+    # rotation batch (plain and hoisted)
+    rotation = None
+    if not args.no_rot:
+        rotation = rotation_batch(G, torch, dev, local, gen, max(3, min(args.steps, 10)))
+
     # serving trace (continuous batching vs one request at a time)
     serving = None
     if not args.no_serve:
@@ -623,6 +717,7 @@ def run_gpu(args):
         "latency_ms": (dict(serving["served"]["latency_ms"], source="serving trace, served form") if serving
                        else {"p50": ms_step, "p99": ms_step, "source": "whole batch per step"}),
         "ntt_kernel_isolation": ntt,
+        "rotation_batch": rotation,
         "serving": serving,
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk.summary(),
@@ -642,9 +737,10 @@ def main():
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-rot", action="store_true")
     ap.add_argument("--pairs", type=int, default=PAIRS, help="pairs per step (smaller only for profiling)")
-    ap.add_argument("--section", default="all", choices=["all", "ntt"],
-                    help="ntt: only the NTT / RNS-multiply kernel isolation (prints its own line)")
+    ap.add_argument("--section", default="all", choices=["all", "ntt", "rot"],
+                    help="ntt / rot: only the kernel isolation or the rotation batch (prints its own line)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -103,8 +103,8 @@ struct Launcher {
 
 bool supported_logn(int logn) { return logn >= 11 && logn <= 16; }
 
-int input_count(uint32_t mode) { return mode == EMR ? 4 : mode == ROT ? 2 : 1; }
-uint32_t output_towers(const Op& op) { return (op.mode == EMR || op.mode == RESCALE) ? op.L - 1 : op.L; }
+int input_count(uint32_t mode) { return mode == EMR ? 4 : (mode == ROT || mode == HROT) ? 2 : 1; }
+uint32_t output_towers(const Op& op) { return (op.mode == EMR || op.mode == RESCALE) ? op.L - 1 : op.L; }  // ROT, HROT, KS: L
 
 size_t op_workspace_words(const gfx::Context& c, uint32_t L) {
     return (size_t)ws_layout(L, c.K(), c.alpha()).total * c.n();
@@ -115,11 +115,12 @@ void validate(const gfx::Context& c, const Op& op) {
     if ((op.mode == EMR || op.mode == RESCALE) && op.L < 2) throw std::invalid_argument("rescale needs L >= 2");
     if (c.alpha() > (uint32_t)MAXA) throw std::invalid_argument("digit width above the fused limit");
     if (c.dnum() > (uint32_t)MAC_MAX_DNUM) throw std::invalid_argument("too many digits for the key-stationary MAC");
-    if (op.mode > RESCALE) throw std::invalid_argument("unknown mode");
-    const int nin = op.mode == EMR ? 4 : op.mode == ROT ? 2 : 1;
+    if (op.mode > HROT) throw std::invalid_argument("unknown mode");
+    const int nin = input_count(op.mode);
     for (int k = 0; k < nin; ++k) if (!op.in[k]) throw std::invalid_argument("null input");
     if (!op.out[0] || (op.mode != RESCALE && !op.out[1])) throw std::invalid_argument("null output");
-    if (op.mode == ROT && (op.galois % 2 == 0 || op.galois >= 2ull * c.n())) throw std::invalid_argument("bad Galois element");
+    if ((op.mode == ROT || op.mode == HROT) && (op.galois % 2 == 0 || op.galois >= 2ull * c.n()))
+        throw std::invalid_argument("bad Galois element");
     auto misaligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) != 0; };
     for (int k = 0; k < nin; ++k)
         if (misaligned(op.in[k])) throw std::invalid_argument("input buffers must be 16-byte aligned");
@@ -143,6 +144,7 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
     T.pairs.assign(ops.size(), PairDesc{});
     std::vector<uint2> jobs[NPHASE];
     std::map<std::pair<uint64_t, uint32_t>, std::vector<uint32_t>> rows;
+    std::map<std::pair<const u64*, uint32_t>, uint32_t> hoist_lead;   // (c1, level) -> first HROT op
     for (size_t pi = 0; pi < ops.size(); ++pi) {
         const Op& op = ops[pi];
         PairDesc& P = T.pairs[pi];
@@ -154,6 +156,15 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
         P.out[0] = op.out[0];
         P.out[1] = op.out[1];
         P.ws = ws_ptrs[pi];
+        P.ysrc = P.ws;
+        bool modup = true;   // this op computes its own ModUp (P1-P4)
+        if (op.mode == HROT) {
+            auto ins = hoist_lead.emplace(std::make_pair(op.in[1], op.L), (uint32_t)pi);
+            if (!ins.second) {
+                P.ysrc = T.pairs[ins.first->second].ws;
+                modup = false;
+            }
+        }
         if (op.mode != RESCALE) {
             const gfx::Key* key = c.key(op.key_id);
             if (!key) throw std::invalid_argument("missing eval key");
@@ -168,11 +179,16 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
             for (uint32_t i = 0; i + 1 < L; ++i) { jobs[7].push_back({pu, i}); jobs[8].push_back({pu, i}); }
             continue;
         }
-        for (uint32_t i = 0; i < L; ++i) { jobs[0].push_back({pu, i}); jobs[1].push_back({pu, i}); }
-        for (uint32_t p = 0; p < nparts; ++p) {
-            const uint32_t st = c.alpha() * p, sp = std::min(c.alpha(), L - st);
-            for (uint32_t i = 0; i < QlP; ++i)
-                if (i < st || i >= st + sp) { jobs[2].push_back({pu, p * QlP + i}); jobs[3].push_back({pu, p * QlP + i}); }
+        if (modup) {
+            for (uint32_t i = 0; i < L; ++i) { jobs[0].push_back({pu, i}); jobs[1].push_back({pu, i}); }
+            for (uint32_t p = 0; p < nparts; ++p) {
+                const uint32_t st = c.alpha() * p, sp = std::min(c.alpha(), L - st);
+                for (uint32_t i = 0; i < QlP; ++i)
+                    if (i < st || i >= st + sp) {
+                        jobs[2].push_back({pu, p * QlP + i});
+                        jobs[3].push_back({pu, p * QlP + i});
+                    }
+            }
         }
         for (uint32_t i = 0; i < QlP; ++i) rows[{op.key_id, qp_of(i, L, c.fullQ())}].push_back(pu);
         const bool emr = op.mode == EMR;
@@ -343,6 +359,7 @@ void rebind(Plan& p, uint32_t idx, const Op& op, const gfx::Context& c, cudaStre
     if (idx >= p.pairs_host.size()) throw std::invalid_argument("rebind: index");
     validate(c, op);
     const Op& old = p.ops[idx];
+    if (old.mode == HROT || op.mode == HROT) throw std::invalid_argument("rebind: hoisted rotations cannot be rebound");
     const bool same_shape = old.L == op.L && (old.mode == op.mode ||
                             ((old.mode == KS || old.mode == ROT) && (op.mode == KS || op.mode == ROT)));
     if (!same_shape) throw std::invalid_argument("rebind: level or job shape differs");

@@ -52,6 +52,9 @@ enum Mode : u32 {
     KS = 1,        // keyswitch: in[0] = a [L]; out0,out1 = ba0, ba1 [L]
     ROT = 2,       // rotation: in = c0, c1 [L]; out = sigma(c0)+ba0, ba1 [L]
     RESCALE = 3,   // rescale: in[0] = comp [L]; out0 = [L-1] (may alias in[0])
+    HROT = 4,      // hoisted rotation: as ROT, but operations of one batch with the same
+                   // c1 buffer and level share one ModUp of c1 (computed by the first of
+                   // them); each applies sigma_k to the shared digits in eval form
 };
 
 struct PairDesc {
@@ -61,6 +64,7 @@ struct PairDesc {
     const u64* in[4];
     u64* out[2];
     u64* ws;
+    const u64* ysrc;       // workspace holding the ModUp digits (own ws; HROT: the group's first)
     const u64* kav;        // key [dnum][fullQ+K][n]
     const u64* kbv;
 };
@@ -101,6 +105,7 @@ __device__ __forceinline__ u64 digit_src(const PairDesc& P, u32 i, u32 e, const 
     const size_t o = ((size_t)i << LOGN);
     if (P.mode == EMR) return mulmod(P.in[1][o + e], P.in[3][o + e], m);
     if (P.mode == ROT) return P.in[1][o + galois_slot<LOGN>(e, P.galois)];
+    if (P.mode == HROT) return P.in[1][o + e];   // ModUp source of a hoisted group: c1 itself
     return P.in[0][o + e];
 }
 
@@ -415,7 +420,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
                         mac_wide(lo, hi, a1, b0);
                         v2set(t1[k], j, barrett(lo, hi, m));
                     }
-            } else if (P.mode == ROT) {
+            } else if (P.mode == ROT || P.mode == HROT) {
                 const u64* src = P.in[1] + ((size_t)i << LOGN);
 #pragma unroll
                 for (int k = 0; k < NV; ++k)
@@ -437,10 +442,19 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
             for (int pp = 0; pp < MAC_PCH; ++pp) {
                 const u32 p = p0 + pp;
                 if (p < nparts && p != pin) {
-                    const ulonglong2* Y =
-                        reinterpret_cast<const ulonglong2*>(slot_ptr(P, w.Y + p * QlP + i, LOGN) + tile0);
+                    const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN);
+                    if (P.mode == HROT) {   // sigma_k of the shared digit: eval-slot gather
 #pragma unroll
-                    for (int k = 0; k < NV; ++k) v[pp][k] = __ldcs(Y + threadIdx.x + k * MAC_NT);
+                        for (int k = 0; k < NV; ++k)
+#pragma unroll
+                            for (int j = 0; j < 2; ++j)
+                                v2set(v[pp][k], j,
+                                      Yt[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * MAC_NT) + j, P.galois)]);
+                    } else {
+                        const ulonglong2* Y = reinterpret_cast<const ulonglong2*>(Yt + tile0);
+#pragma unroll
+                        for (int k = 0; k < NV; ++k) v[pp][k] = __ldcs(Y + threadIdx.x + k * MAC_NT);
+                    }
                 }
             }
 #pragma unroll
@@ -544,6 +558,10 @@ __device__ __forceinline__ void cp_async16(u64* smem, const u64* gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(u64* smem, const u64* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
@@ -588,8 +606,17 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
             }
         }
         const u32 nparts = D.lvl[L].nparts;
-        for (u32 p = 0; p < nparts; ++p)
-            if (p != pin) cp_async16(sb + (MACA_IN + p) * MAC_TILE, slot_ptr(P, w.Y + p * QlP + i, LOGN) + tile0 + e);
+        for (u32 p = 0; p < nparts; ++p) {
+            if (p == pin) continue;
+            const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN);
+            if (P.mode == HROT) {   // sigma_k of the shared digit: two 8-byte gathers
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+                    cp_async8(sb + (MACA_IN + p) * MAC_TILE + j, Yt + galois_slot<LOGN>(tile0 + e + j, P.galois));
+            } else {
+                cp_async16(sb + (MACA_IN + p) * MAC_TILE, Yt + tile0 + e);
+            }
+        }
         cp_async_commit();
     };
     issue(0, 0);
@@ -621,7 +648,7 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
                     mac_wide(lo, hi, a1, b0);
                     v2set(t1, j, barrett(lo, hi, m));
                 }
-            } else if (P.mode == ROT) {
+            } else if (P.mode == ROT || P.mode == HROT) {
                 const u64* src = P.in[1] + ((size_t)i << LOGN);
 #pragma unroll
                 for (int j = 0; j < 2; ++j) v2set(s, j, src[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
@@ -885,7 +912,7 @@ __device__ __forceinline__ void p9_final_fwd_row_body(const DevCtx& D, const Pai
                 r = csub(shoup(a, s1, s1p, m.q) + v, m.q);
             } else {
                 r = csub(a + v, m.q);
-                if (mode == ROT && c == 0)
+                if ((mode == ROT || mode == HROT) && c == 0)
                     r = csub(r + P.in[0][((size_t)i << LOGN) + galois_slot<LOGN>((u32)(tile0 + e), P.galois)], m.q);
             }
             out[e] = r;

@@ -73,7 +73,7 @@ _API: dict = {
     "gpufhe_server_records": (I32, [VP, VP, U32, C.POINTER(U32)]),
 }
 
-EVALMULT_RESCALE, KEYSWITCH, ROTATE, RESCALE = 0, 1, 2, 3
+EVALMULT_RESCALE, KEYSWITCH, ROTATE, RESCALE, ROTATE_HOISTED = 0, 1, 2, 3, 4
 
 
 class Op(C.Structure):

@@ -90,11 +90,19 @@ int gpufhe_rns_mult_batch(gpufhe_ctx* ctx, const uint64_t* d_a, const uint64_t* 
  *       rotate.cpp:118-132). Outputs must not alias inputs.
  *   GPUFHE_RESCALE: in[0] = comp [level][n] -> out[0] [level-1][n]
  *       (rescale_resident_raw, keyswitch_resident.cpp:227-244); out may alias in.
- * Device pointers; ring sizes 2^11..2^16. */
+ *   GPUFHE_ROTATE_HOISTED: as GPUFHE_ROTATE, but every such operation of the
+ *       batch with the same in[1] (c1) buffer and level shares one ModUp of c1,
+ *       computed by the first of them; each rotation applies sigma_k to the
+ *       shared digits in eval form before its key product. No counterpart in
+ *       the reference (its rotate_ct_device, rotate.cpp:118-132, does one ModUp
+ *       per rotation); the result differs from GPUFHE_ROTATE by the
+ *       approximate-basis-conversion term, as hoisting always does.
+ * Device pointers, 16-byte aligned; ring sizes 2^11..2^16. */
 #define GPUFHE_EVALMULT_RESCALE 0u
 #define GPUFHE_KEYSWITCH 1u
 #define GPUFHE_ROTATE 2u
 #define GPUFHE_RESCALE 3u
+#define GPUFHE_ROTATE_HOISTED 4u
 
 typedef struct gpufhe_op {
     uint32_t level;

@@ -99,3 +99,37 @@ def test_evalmult_rescale_decrypts(G, S, gctx):
     ql = int(S.Q[L - 1])
     got = [round(v * ql / (D * D)) for v in dec[:6]]
     assert got == [12, -8, 15, -10, 0, 0]
+
+
+def test_rotate_hoisted_groups(G, S, gctx):
+    """Hoisted rotations (one shared ModUp per c1 buffer and level) next to a
+    plain rotation of the same ciphertext, in one batch."""
+    rng = np.random.default_rng(300)
+    ks = list(S.rot)
+    n = S.n
+    cases = [(8, ks), (4, ks[:1])]
+    keep, specs, want = [], [], []
+    for L, group in cases:
+        c0, c1 = S.rand_ct(rng, L)
+        d0, d1 = dev(c0), dev(c1)
+        keep += [d0, d1]
+        e0, e1 = S.octx.rotate_hoisted(L, group, group, c0, c1)
+        for r, k in enumerate(group):
+            o0, o1 = empty(L * n), empty(L * n)
+            keep += [o0, o1]
+            specs.append(dict(level=L, mode=G.ROTATE_HOISTED, key_id=k, galois=k, inp=[ptr(d0), ptr(d1)],
+                              out=[ptr(o0), ptr(o1)]))
+            want.append((o0, o1, e0[r], e1[r]))
+        # a plain rotation of the same buffers is not part of the hoisted group
+        p0, p1 = empty(L * n), empty(L * n)
+        keep += [p0, p1]
+        specs.append(dict(level=L, mode=G.ROTATE, key_id=group[0], galois=group[0], inp=[ptr(d0), ptr(d1)],
+                          out=[ptr(p0), ptr(p1)]))
+        f0, f1 = S.octx.rotate(L, group[0], c0, c1, group[0])
+        want.append((p0, p1, f0, f1))
+    plan = G.Plan(gctx, specs)
+    for rep in range(2):
+        plan.launch()
+        sync()
+        for j, (o0, o1, e0, e1) in enumerate(want):
+            assert np.array_equal(host(o0), e0) and np.array_equal(host(o1), e1), (rep, j)
