@@ -394,7 +394,7 @@ void apply_choice(Plan& p, int choice) {
 }
 }  // namespace
 
-void tune(Plan& p, cudaStream_t s) {
+void tune(Plan& p, cudaStream_t s, bool measure) {
     if (p.tuned || !p.nops || !p.ctx) return;
     const gfx::Context& c = *p.ctx;
     const uint64_t key = tune_key(p);
@@ -404,34 +404,44 @@ void tune(Plan& p, cudaStream_t s) {
         p.tuned = true;
         return;
     }
+    constexpr int DEFAULT = 2;                   // register P5, interleaved paths
+    apply_choice(p, DEFAULT);
+    if (!measure) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
     for (const Op& op : p.ops)
         if (op.mode == RESCALE) return;          // may be in place: re-running would change its input
-    const int ncand = mac_async_ok(p.dc.dnum) ? 4 : 2;
+    std::vector<int> cands = {DEFAULT, 0};
+    if (mac_async_ok(p.dc.dnum)) { cands.push_back(3); cands.push_back(1); }
+    std::vector<float> best(cands.size(), 1e30f);
     cudaEvent_t a, b;
     if (cudaEventCreate(&a) != cudaSuccess) return;
     if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
-    float best = 0;
-    int best_choice = 2;
-    for (int k = 0; k < 4; ++k) {
-        const int cand = ncand == 4 ? k : (k & 2);
-        if (ncand == 2 && (k & 1)) continue;
-        apply_choice(p, cand);
-        launch(p, s);                            // warm
-        cudaEventRecord(a, s);
-        launch(p, s);
-        launch(p, s);
-        cudaEventRecord(b, s);
-        if (cudaEventSynchronize(b) != cudaSuccess) break;
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a, b);
-        if (k == 0 || ms < best) { best = ms; best_choice = cand; }
-    }
+    bool ok = true;
+    // two interleaved passes, best of three timed launches per candidate and pass
+    for (int pass = 0; pass < 2 && ok; ++pass)
+        for (size_t ci = 0; ci < cands.size() && ok; ++ci) {
+            apply_choice(p, cands[ci]);
+            launch(p, s);
+            for (int r = 0; r < 3; ++r) {
+                cudaEventRecord(a, s);
+                launch(p, s);
+                cudaEventRecord(b, s);
+                if (cudaEventSynchronize(b) != cudaSuccess) { ok = false; break; }
+                float ms = 0;
+                cudaEventElapsedTime(&ms, a, b);
+                best[ci] = std::min(best[ci], ms);
+            }
+        }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    apply_choice(p, best_choice);
-    c.set_tuned_choice(key, best_choice);
+    size_t win = 0;
+    for (size_t ci = 1; ci < cands.size(); ++ci)
+        if (best[ci] < best[win]) win = ci;
+    // keep the default unless a candidate is clearly faster
+    if (!ok || best[win] > 0.985f * best[0]) win = 0;
+    apply_choice(p, cands[win]);
+    c.set_tuned_choice(key, cands[win]);
     p.tuned = true;
 }
 

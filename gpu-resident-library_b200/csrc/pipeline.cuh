@@ -361,7 +361,7 @@ __device__ __forceinline__ u64 v2get(const ulonglong2& v, int j) { return j ? v.
 __device__ __forceinline__ void v2set(ulonglong2& v, int j, u64 x) { if (j) v.y = x; else v.x = x; }
 
 template <int LOGN>
-__global__ void __launch_bounds__(MAC_NT)
+__global__ void __launch_bounds__(MAC_NT, 4)
 p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
        const u32* __restrict__ plist) {
     constexpr int TILES = (1 << LOGN) / MAC_TILE;

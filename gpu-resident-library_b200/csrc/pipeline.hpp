@@ -63,10 +63,12 @@ cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
 // Picks the launch schedule of `p` (P5 variant; integer and FP64 transform
 // jobs as two launches or one interleaved launch): from the context's tuning cache when it holds
 // this shape (ring size, digits, batch-size class), else by timing every
-// candidate with CUDA events on `s` and caching the fastest. Timing re-runs
-// the batch, so it is skipped (defaults kept) while `s` is capturing a graph
-// or when an operation writes over its own input (in-place rescale).
-void tune(Plan& p, cudaStream_t s);
+// candidate with CUDA events on `s` (two interleaved passes, best of three
+// launches each; the default stays unless another is 1.5% faster) and
+// caching the winner. Timing re-runs the batch, so it is skipped (defaults
+// kept) when `measure` is false, while `s` is capturing a graph, or when an
+// operation writes over its own input (in-place rescale).
+void tune(Plan& p, cudaStream_t s, bool measure = true);
 constexpr int MAC_MAX_DNUM = 16;
 inline int mac_smem(uint32_t dnum) { return (int)(dnum * 2 * MAC_TILE * sizeof(u64)); }
 // The pipelined P5 runs when two CTAs' key tiles and staging buffers fit in one SM.

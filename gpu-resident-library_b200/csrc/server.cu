@@ -335,7 +335,7 @@ int Server::step() {
         cudaStream_t s = streams_[c];
         pl::Plan& plan = *plans_[2 * c + slot];
         pl::build_plan_into(plan, *ctxs_[c], ops[c], ws[c], s);
-        pl::tune(plan, s);
+        pl::tune(plan, s, false);   // cached schedule or the default: no timing runs on the serving path
         ck(pl::launch(plan, s), "pipeline launch");
         for (size_t k = 0; k < who[c].size(); ++k) {
             Request& r = *who[c][k];
