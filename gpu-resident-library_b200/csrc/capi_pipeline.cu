@@ -75,7 +75,7 @@ int gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t s) 
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan) {
     if (!plan) return 0;
     const pl::Plan& p = *plan->p;
-    return (p.p5_async ? 1u : 0u) | (p.mix ? 2u : 0u) | (p.tuned ? 4u : 0u);
+    return (uint32_t)p.p5_form | (p.mix ? 4u : 0u) | (p.tuned ? 8u : 0u);
 }
 
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {

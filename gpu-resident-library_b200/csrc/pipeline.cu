@@ -63,7 +63,8 @@ struct Launcher {
             done = true;
         }
         if (dnum > mac_dnum) {
-            cudaFuncSetAttribute(p5_mac<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(dnum));
+            cudaFuncSetAttribute(p5_mac<LOGN, MAC_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(dnum));
+            cudaFuncSetAttribute(p5_mac<LOGN, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(dnum));
             if (mac_async_ok(dnum))
                 cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      maca_smem((int)dnum));
@@ -79,12 +80,15 @@ struct Launcher {
             if (!(mask >> k & 1)) continue;
             if (k == 4) {
                 if (!p.job_cnt[4][0]) continue;
-                if (p.p5_async && mac_async_ok(D.dnum))
-                    p5_mac_async<LOGN><<<p.job_cnt[4][0] * MAC_TILES, MACA_NT, maca_smem((int)D.dnum), s>>>(
-                        D, p.d_pairs, p.d_mac_jobs, p.d_plist);
+                const unsigned grid = p.job_cnt[4][0] * MAC_TILES;
+                if (p.p5_form == P5_ASYNC && mac_async_ok(D.dnum))
+                    p5_mac_async<LOGN><<<grid, MACA_NT, maca_smem((int)D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
+                                                                                     p.d_plist);
+                else if (p.p5_form == P5_REG256)
+                    p5_mac<LOGN, 256><<<grid, 256, mac_smem(D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs, p.d_plist);
                 else
-                    p5_mac<LOGN><<<p.job_cnt[4][0] * MAC_TILES, MAC_NT, mac_smem(D.dnum), s>>>(D, p.d_pairs,
-                                                                                            p.d_mac_jobs, p.d_plist);
+                    p5_mac<LOGN, MAC_NT><<<grid, MAC_NT, mac_smem(D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
+                                                                               p.d_plist);
             } else if (k == 6) {
                 if (p.job_cnt[6][0])
                     p7_moddown_inv_col<LOGN><<<p.job_cnt[6][0] * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(
@@ -388,9 +392,11 @@ uint64_t tune_key(const Plan& p) {
     while ((1u << (cls + 1)) <= p.nops) ++cls;   // batch-size class: floor(log2(nops))
     return ((uint64_t)p.logn << 40) | ((uint64_t)p.dc.dnum << 32) | cls;
 }
+// choice: bits 0-1 = P5 form, bit 2 = interleaved integer / FP64 jobs
 void apply_choice(Plan& p, int choice) {
-    p.p5_async = (choice & 1) && mac_async_ok(p.dc.dnum);
-    p.mix = (choice & 2) != 0;
+    p.p5_form = choice & 3;
+    if (p.p5_form == P5_ASYNC && !mac_async_ok(p.dc.dnum)) p.p5_form = P5_REG128;
+    p.mix = (choice & 4) != 0;
 }
 }  // namespace
 
@@ -404,15 +410,15 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         p.tuned = true;
         return;
     }
-    constexpr int DEFAULT = 2;                   // register P5, interleaved paths
+    constexpr int DEFAULT = P5_REG128 | 4;       // 4-word register P5, interleaved paths
     apply_choice(p, DEFAULT);
     if (!measure) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
     for (const Op& op : p.ops)
         if (op.mode == RESCALE) return;          // may be in place: re-running would change its input
-    std::vector<int> cands = {DEFAULT, 0};
-    if (mac_async_ok(p.dc.dnum)) { cands.push_back(3); cands.push_back(1); }
+    std::vector<int> cands = {DEFAULT, P5_REG128, P5_REG256 | 4, P5_REG256};
+    if (mac_async_ok(p.dc.dnum)) { cands.push_back(P5_ASYNC | 4); cands.push_back(P5_ASYNC); }
     std::vector<float> best(cands.size(), 1e30f);
     cudaEvent_t a, b;
     if (cudaEventCreate(&a) != cudaSuccess) return;

@@ -44,7 +44,7 @@ using gfx::Level;
 constexpr int NPHASE = 9;
 constexpr int MAXA = 16;       // digit width supported by the fused ModUp prologue
 constexpr int MAC_TILE = 512;  // P5 elements per CTA
-constexpr int MAC_NT = 128;    // P5 threads (4 elements each)
+constexpr int MAC_NT = 128;    // P5 threads of the 4-word form (the 2-word form has 256)
 constexpr int MAC_GROUP = 16;  // P5 pairs streamed per CTA
 
 enum Mode : u32 {
@@ -360,12 +360,12 @@ constexpr int MAC_PCH = 4;
 __device__ __forceinline__ u64 v2get(const ulonglong2& v, int j) { return j ? v.y : v.x; }
 __device__ __forceinline__ void v2set(ulonglong2& v, int j, u64 x) { if (j) v.y = x; else v.x = x; }
 
-template <int LOGN>
-__global__ void __launch_bounds__(MAC_NT, 4)
+template <int LOGN, int NT>
+__global__ void __launch_bounds__(NT, NT == 128 ? 4 : 3)
 p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
        const u32* __restrict__ plist) {
     constexpr int TILES = (1 << LOGN) / MAC_TILE;
-    constexpr int NV = MAC_TILE / (2 * MAC_NT);   // 16-byte vectors per thread
+    constexpr int NV = MAC_TILE / (2 * NT);   // 16-byte vectors per thread
     extern __shared__ __align__(16) u64 sm[];     // [dnum][2][MAC_TILE]
     const uint4 jb = jobs[blockIdx.x / TILES];
     const u32 tile0 = (blockIdx.x % TILES) * MAC_TILE;
@@ -374,7 +374,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
     const u32 dnum = D.dnum;
     // every listed pair uses the same key (checked on the host)
     const PairDesc& P0 = pairs[plist[jb.y]];
-    for (u32 k = threadIdx.x; k < dnum * (MAC_TILE / 2); k += MAC_NT) {
+    for (u32 k = threadIdx.x; k < dnum * (MAC_TILE / 2); k += NT) {
         const u32 p = k / (MAC_TILE / 2), e = 2 * (k % (MAC_TILE / 2));
         const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0 + e;
         *reinterpret_cast<ulonglong2*>(sm + (2 * p) * MAC_TILE + e) = *reinterpret_cast<const ulonglong2*>(P0.kbv + off);
@@ -401,7 +401,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
                 ulonglong2 x0[NV], x1[NV], y0[NV], y1[NV];
 #pragma unroll
                 for (int k = 0; k < NV; ++k) {
-                    const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                    const u32 e = 2 * (threadIdx.x + k * NT);
                     x0[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + e);
                     x1[k] = *reinterpret_cast<const ulonglong2*>(P.in[1] + o + e);
                     y0[k] = *reinterpret_cast<const ulonglong2*>(P.in[2] + o + e);
@@ -426,11 +426,11 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
                 for (int k = 0; k < NV; ++k)
 #pragma unroll
                     for (int j = 0; j < 2; ++j)
-                        v2set(s[k], j, src[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * MAC_NT) + j, P.galois)]);
+                        v2set(s[k], j, src[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * NT) + j, P.galois)]);
             } else {
 #pragma unroll
                 for (int k = 0; k < NV; ++k)
-                    s[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + 2 * (threadIdx.x + k * MAC_NT));
+                    s[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + 2 * (threadIdx.x + k * NT));
             }
         }
         u64 a0l[2 * NV], a0h[2 * NV], a1l[2 * NV], a1h[2 * NV];
@@ -449,11 +449,11 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
 #pragma unroll
                             for (int j = 0; j < 2; ++j)
                                 v2set(v[pp][k], j,
-                                      Yt[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * MAC_NT) + j, P.galois)]);
+                                      Yt[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * NT) + j, P.galois)]);
                     } else {
                         const ulonglong2* Y = reinterpret_cast<const ulonglong2*>(Yt + tile0);
 #pragma unroll
-                        for (int k = 0; k < NV; ++k) v[pp][k] = __ldcs(Y + threadIdx.x + k * MAC_NT);
+                        for (int k = 0; k < NV; ++k) v[pp][k] = __ldcs(Y + threadIdx.x + k * NT);
                     }
                 }
             }
@@ -465,7 +465,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
                 const u64* ka = sm + (2 * p + 1) * MAC_TILE;
 #pragma unroll
                 for (int k = 0; k < NV; ++k) {
-                    const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                    const u32 e = 2 * (threadIdx.x + k * NT);
                     const ulonglong2 kbv = *reinterpret_cast<const ulonglong2*>(kb + e);
                     const ulonglong2 kav = *reinterpret_cast<const ulonglong2*>(ka + e);
                     const ulonglong2 dv = p == pin ? s[k] : v[pp][k];
@@ -490,7 +490,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
             d1 = slot_ptr(P, w.RP + K + (i - L), LOGN) + tile0;
 #pragma unroll
             for (int k = 0; k < NV; ++k) {
-                const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                const u32 e = 2 * (threadIdx.x + k * NT);
                 *reinterpret_cast<ulonglong2*>(d0 + e) = r0[k];
                 *reinterpret_cast<ulonglong2*>(d1 + e) = r1[k];
             }
@@ -502,7 +502,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
             d1 = slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
             for (int k = 0; k < NV; ++k) {
-                const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+                const u32 e = 2 * (threadIdx.x + k * NT);
                 ulonglong2 o0, o1;
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
@@ -520,7 +520,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
         d1 = drop ? slot_ptr(P, w.U + 1, LOGN) + tile0 : slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
-            const u32 e = 2 * (threadIdx.x + k * MAC_NT);
+            const u32 e = 2 * (threadIdx.x + k * NT);
             ulonglong2 o0, o1;
 #pragma unroll
             for (int j = 0; j < 2; ++j) {

@@ -36,7 +36,7 @@ struct Plan {
     std::vector<Op> ops;      // host copy (device pointers and levels)
     std::vector<PairDesc> pairs_host;
     // launch schedule (chosen by tune() or the context's tuning cache)
-    bool p5_async = false;             // pipelined P5 instead of the register-prefetch one
+    int p5_form = 0;                   // P5_REG128, P5_ASYNC or P5_REG256
     bool mix = true;                   // one launch per phase over the interleaved job list
     bool tuned = false;
     const gfx::Context* ctx = nullptr;
@@ -60,7 +60,7 @@ void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops,
                      cudaStream_t s);
 // mask selects phases P1..P9 (bit k = phase k+1); 0x1ff runs the whole batch.
 cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
-// Picks the launch schedule of `p` (P5 variant; integer and FP64 transform
+// Picks the launch schedule of `p` (P5 form; integer and FP64 transform
 // jobs as two launches or one interleaved launch): from the context's tuning cache when it holds
 // this shape (ring size, digits, batch-size class), else by timing every
 // candidate with CUDA events on `s` (two interleaved passes, best of three
@@ -70,6 +70,9 @@ cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
 // operation writes over its own input (in-place rescale).
 void tune(Plan& p, cudaStream_t s, bool measure = true);
 constexpr int MAC_MAX_DNUM = 16;
+// P5 forms: register prefetch with 128 threads x 4 words, the cp.async
+// pipelined form, register prefetch with 256 threads x 2 words.
+constexpr int P5_REG128 = 0, P5_ASYNC = 1, P5_REG256 = 2;
 inline int mac_smem(uint32_t dnum) { return (int)(dnum * 2 * MAC_TILE * sizeof(u64)); }
 // The pipelined P5 runs when two CTAs' key tiles and staging buffers fit in one SM.
 inline bool mac_async_ok(uint32_t dnum) { return maca_smem((int)dnum) <= 113 * 1024; }

@@ -200,9 +200,10 @@ class Plan:
         return int(lib().gpufhe_plan_kernel_count(self.h))
 
     def schedule(self):
-        """Autotuner choice: {'p5_async', 'mixed_paths', 'tuned'}."""
+        """Autotuner choice: {'p5': form, 'mixed_paths': bool, 'tuned': bool}."""
         b = int(lib().gpufhe_plan_schedule(self.h))
-        return {"p5_async": bool(b & 1), "mixed_paths": bool(b & 2), "tuned": bool(b & 4)}
+        form = {0: "register-128x4", 1: "cp.async", 2: "register-256x2"}.get(b & 3, "?")
+        return {"p5": form, "mixed_paths": bool(b & 4), "tuned": bool(b & 8)}
 
     def launch_host(self, h_in, h_out, stream=None):
         """h_in: list of 4 host pointers per op (0 for unused); h_out: 2 per op."""

@@ -132,9 +132,11 @@ int  gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t st
 /* Number of kernels one gpufhe_plan_launch enqueues. */
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
 /* Launch schedule chosen by the autotuner (first gpufhe_plan_launch outside
- * graph capture, cached per context and batch shape): bit 0 = pipelined P5,
- * bit 1 = integer and FP64 transform jobs of a phase interleaved in one
- * launch (else two launches), bit 2 = tuned. */
+ * graph capture, cached per context and batch shape): bits 0-1 = P5 form
+ * (0 register prefetch, 128 threads x 4 words; 1 cp.async pipelined;
+ * 2 register prefetch, 256 threads x 2 words), bit 2 = integer and FP64
+ * transform jobs of a phase interleaved in one launch (else two launches),
+ * bit 3 = tuned. */
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan);
 /* Host-buffer form: copies h_in[4*i+k] (host, level*n words) into op i's
  * device inputs, launches the batch and copies each op's outputs back into
