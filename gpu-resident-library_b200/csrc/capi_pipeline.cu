@@ -78,6 +78,16 @@ uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan) {
     return (uint32_t)p.p5_form | (p.mix ? 4u : 0u) | (p.tuned ? 8u : 0u);
 }
 
+int gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule) {
+    if (!plan || (schedule & 3) > 2) { gfx::set_error("bad plan or schedule"); return GPUFHE_EINVAL; }
+    pl::Plan& p = *plan->p;
+    p.p5_form = (int)(schedule & 3);
+    if (p.p5_form == pl::P5_ASYNC && !pl::mac_async_ok(p.dc.dnum)) p.p5_form = pl::P5_REG128;
+    p.mix = (schedule & 4) != 0;
+    p.tuned = true;
+    return GPUFHE_OK;
+}
+
 uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     if (!plan) return 0;
     uint32_t k = 0;

@@ -51,7 +51,7 @@ __device__ __forceinline__ Job get_job(const Job* __restrict__ arr, const Job& o
 }
 
 template <int LOGN, bool SINGLE>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 4)
 k_fwd_col(const Job* __restrict__ arr, const Job one) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
@@ -67,7 +67,7 @@ k_fwd_col(const Job* __restrict__ arr, const Job one) {
 }
 
 template <int LOGN, bool SINGLE>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 4)
 k_fwd_row(const Job* __restrict__ arr, const Job one) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
@@ -87,7 +87,7 @@ k_fwd_row(const Job* __restrict__ arr, const Job one) {
 }
 
 template <int LOGN, bool SINGLE>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 4)
 k_inv_row(const Job* __restrict__ arr, const Job one) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
@@ -106,7 +106,7 @@ k_inv_row(const Job* __restrict__ arr, const Job one) {
 }
 
 template <int LOGN, bool SINGLE>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 4)
 k_inv_col(const Job* __restrict__ arr, const Job one) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];

@@ -55,6 +55,7 @@ _API: dict = {
     "gpufhe_plan_launch_phase": (I32, [VP, U32, VP]),
     "gpufhe_plan_kernel_count": (U32, [VP]),
     "gpufhe_plan_schedule": (U32, [VP]),
+    "gpufhe_plan_set_schedule": (I32, [VP, U32]),
     "gpufhe_plan_launch_host": (I32, [VP, VP, VP, VP]),
     "gpufhe_native_primes": (I32, [VP, U32, U32, U32, VP, U32]),
     "gpufhe_native_root": (U64, [U32, U64]),
@@ -192,6 +193,10 @@ class Plan:
 
     def launch(self, stream=None):
         check(lib().gpufhe_plan_launch(self.h, stream))
+
+    def set_schedule(self, bits):
+        """Fix the launch schedule (bits 0-1 P5 form, bit 2 interleaved paths); skips the autotuner."""
+        check(lib().gpufhe_plan_set_schedule(self.h, bits))
 
     def launch_phase(self, phase, stream=None):
         check(lib().gpufhe_plan_launch_phase(self.h, phase, stream))

@@ -138,6 +138,9 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
  * transform jobs of a phase interleaved in one launch (else two launches),
  * bit 3 = tuned. */
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan);
+/* Fixes the schedule (bits 0-2 as above) and skips the autotuner; every
+ * schedule computes the same bits. */
+int      gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule);
 /* Host-buffer form: copies h_in[4*i+k] (host, level*n words) into op i's
  * device inputs, launches the batch and copies each op's outputs back into
  * h_out[2*i+k]; synchronizes `stream`. NULL entries are skipped. Pinned host

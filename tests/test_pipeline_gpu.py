@@ -133,3 +133,36 @@ def test_rotate_hoisted_groups(G, S, gctx):
         sync()
         for j, (o0, o1, e0, e1) in enumerate(want):
             assert np.array_equal(host(o0), e0) and np.array_equal(host(o1), e1), (rep, j)
+
+
+@pytest.mark.parametrize("schedule", [0, 1, 2, 4, 5, 6])
+def test_every_schedule_same_bits(G, S, gctx, schedule):
+    """Each launch schedule the autotuner can pick (P5 form x interleaved or
+    separate integer / FP64 transform launches) gives the oracle's bits on a
+    mixed batch (EvalMult+Rescale at uneven levels, keyswitch, rotation)."""
+    rng = np.random.default_rng(900 + schedule)
+    n, k = S.n, list(S.rot)[0]
+    keep, specs, want = [], [], []
+    for L in (3, 7, 12):
+        c0a, c1a = S.rand_ct(rng, L)
+        c0b, c1b = S.rand_ct(rng, L)
+        ins = [dev(x) for x in (c0a, c1a, c0b, c1b)]
+        outs = [empty((L - 1) * n), empty((L - 1) * n)]
+        keep += ins + outs
+        specs.append(dict(level=L, inp=[ptr(x) for x in ins], out=[ptr(x) for x in outs]))
+        want.append((outs, S.octx.evalmult_rescale(L, c0a, c1a, c0b, c1b)))
+    c0, c1 = S.rand_ct(rng, 9)
+    d0, d1, o0, o1, k0, k1 = dev(c0), dev(c1), empty(9 * n), empty(9 * n), empty(9 * n), empty(9 * n)
+    keep += [d0, d1, o0, o1, k0, k1]
+    specs.append(dict(level=9, mode=G.ROTATE, key_id=k, galois=k, inp=[ptr(d0), ptr(d1)], out=[ptr(o0), ptr(o1)]))
+    want.append(([o0, o1], S.octx.rotate(9, k, c0, c1, k)))
+    specs.append(dict(level=9, mode=G.KEYSWITCH, inp=[ptr(d0)], out=[ptr(k0), ptr(k1)]))
+    want.append(([k0, k1], S.octx.keyswitch(9, c0)))
+    plan = G.Plan(gctx, specs)
+    plan.set_schedule(schedule)
+    plan.launch()
+    sync()
+    got = plan.schedule()
+    assert got["tuned"] and got["mixed_paths"] == bool(schedule & 4)
+    for outs, (e0, e1) in want:
+        assert np.array_equal(host(outs[0]), e0) and np.array_equal(host(outs[1]), e1)
