@@ -154,6 +154,7 @@ __device__ __forceinline__ void on_path(uint2& jb, F&& f) {
 // pairs t + k * COL_THREADS, k < PER; pair v sits at row v / (C/2), column
 // 2 * (v % (C/2)), so a warp reads whole 128-byte row segments.
 constexpr int CS_VB = 2;
+constexpr int P8_VB = 1;   // P8 carries more live state per pair (three modes inlined)
 
 template <int LOGN>
 struct ColStage {
@@ -224,7 +225,7 @@ __device__ __forceinline__ void p1_inv_row_body(const DevCtx& D, const PairDesc*
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
 p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
@@ -252,7 +253,7 @@ __device__ __forceinline__ void p2_inv_col_body(const DevCtx& D, const PairDesc*
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
 p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -295,9 +296,10 @@ __device__ __forceinline__ void p3_modup_fwd_col_body(const DevCtx& D, const Pai
         mac_terms<CS_VB>(lo, hi, X, (size_t)1 << LOGN, sp, cst, e);
 #pragma unroll
         for (int b = 0; b < CS_VB; ++b) {
-            u64* d = sm + r[b] * G::C + cl[b];
-            d[0] = barrett_lazy(lo[b][0], hi[b][0], m.q, m.mu_lo, m.mu_hi);
-            d[1] = barrett_lazy(lo[b][1], hi[b][1], m.q, m.mu_lo, m.mu_hi);
+            ulonglong2 v;
+            v.x = barrett_lazy(lo[b][0], hi[b][0], m.q, m.mu_lo, m.mu_hi);
+            v.y = barrett_lazy(lo[b][1], hi[b][1], m.q, m.mu_lo, m.mu_hi);
+            *reinterpret_cast<ulonglong2*>(sm + r[b] * G::C + cl[b]) = v;
         }
     }
     __syncthreads();
@@ -307,7 +309,7 @@ __device__ __forceinline__ void p3_modup_fwd_col_body(const DevCtx& D, const Pai
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
 p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -338,7 +340,7 @@ __device__ __forceinline__ void p4_modup_fwd_row_body(const DevCtx& D, const Pai
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
 p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
@@ -737,7 +739,7 @@ __device__ __forceinline__ void p6_moddown_inv_row_body(const DevCtx& D, const P
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
 p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
@@ -826,27 +828,28 @@ __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 
         return v;
     };
 #pragma unroll 1
-    for (int k0 = 0; k0 < CS::PER; k0 += CS_VB) {
-        int r[CS_VB], cl[CS_VB];
-        size_t e[CS_VB];
+    for (int k0 = 0; k0 < CS::PER; k0 += P8_VB) {
+        int r[P8_VB], cl[P8_VB];
+        size_t e[P8_VB];
 #pragma unroll
-        for (int b = 0; b < CS_VB; ++b) {
+        for (int b = 0; b < P8_VB; ++b) {
             CS::pos(k0 + b, r[b], cl[b]);
             e[b] = (size_t)r[b] * 256 + cl[b];
         }
-        ulonglong2 xr[CS_VB];
+        ulonglong2 xr[P8_VB];
         if constexpr (MODE == EMR || MODE == RESCALE) {
 #pragma unroll
-            for (int b = 0; b < CS_VB; ++b) xr[b] = ld2(R + e[b]);
+            for (int b = 0; b < P8_VB; ++b) xr[b] = ld2(R + e[b]);
         }
-        u64 lo[CS_VB][2] = {}, hi[CS_VB][2] = {};
-        if constexpr (MODE != RESCALE) mac_terms<CS_VB>(lo, hi, XP, (size_t)1 << LOGN, K, ci, e);
+        u64 lo[P8_VB][2] = {}, hi[P8_VB][2] = {};
+        if constexpr (MODE != RESCALE) mac_terms<P8_VB>(lo, hi, XP, (size_t)1 << LOGN, K, ci, e);
 #pragma unroll
-        for (int b = 0; b < CS_VB; ++b) {
-            u64* d = sm + r[b] * G::C + cl[b];
+        for (int b = 0; b < P8_VB; ++b) {
             const bool has_r = MODE == EMR || MODE == RESCALE;
-            d[0] = finish(has_r ? xr[b].x : 0, lo[b][0], hi[b][0]);
-            d[1] = finish(has_r ? xr[b].y : 0, lo[b][1], hi[b][1]);
+            ulonglong2 v;
+            v.x = finish(has_r ? xr[b].x : 0, lo[b][0], hi[b][0]);
+            v.y = finish(has_r ? xr[b].y : 0, lo[b][1], hi[b][1]);
+            *reinterpret_cast<ulonglong2*>(sm + r[b] * G::C + cl[b]) = v;
         }
     }
     __syncthreads();
@@ -871,7 +874,7 @@ __device__ __forceinline__ void p8_moddown_fwd_col_body(const DevCtx& D, const P
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 2)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
 p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -920,7 +923,7 @@ __device__ __forceinline__ void p9_final_fwd_row_body(const DevCtx& D, const Pai
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
 p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
