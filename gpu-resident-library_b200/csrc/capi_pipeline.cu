@@ -75,15 +75,21 @@ int gpufhe_plan_launch_phase(gpufhe_plan* plan, uint32_t phase, cudaStream_t s) 
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan) {
     if (!plan) return 0;
     const pl::Plan& p = *plan->p;
-    return (uint32_t)p.p5_form | (p.mix ? 4u : 0u) | (p.tuned ? 8u : 0u);
+    return (uint32_t)p.p5_form | ((p.mix & 0x1ffu) == 0x1ffu ? 4u : 0u) | ((uint32_t)p.p3_form << 3) |
+           (p.tuned ? 32u : 0u) | ((p.mix & 0x1ffu) << 8);
 }
 
 int gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule) {
-    if (!plan || (schedule & 3) > 2) { gfx::set_error("bad plan or schedule"); return GPUFHE_EINVAL; }
+    if (!plan || (schedule & 3) > 2 || ((schedule >> 3) & 3) > 2) {
+        gfx::set_error("bad plan or schedule");
+        return GPUFHE_EINVAL;
+    }
     pl::Plan& p = *plan->p;
     p.p5_form = (int)(schedule & 3);
     if (p.p5_form == pl::P5_ASYNC && !pl::mac_async_ok(p.dc.dnum)) p.p5_form = pl::P5_REG128;
-    p.mix = (schedule & 4) != 0;
+    p.mix = (schedule & 4) ? 0x1ffu : (schedule >> 8) & 0x1ffu;
+    p.p3_form = (int)((schedule >> 3) & 3);
+    if (p.p3_form > 2) { gfx::set_error("bad P3 form"); return GPUFHE_EINVAL; }
     p.tuned = true;
     return GPUFHE_OK;
 }
@@ -93,7 +99,7 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     uint32_t k = 0;
     const pl::Plan& p = *plan->p;
     for (int i = 0; i < pl::NPHASE; ++i) {
-        if (p.mix && p.job_cnt[i][2]) k += 1;
+        if ((p.mix >> i & 1) && p.job_cnt[i][2]) k += 1;
         else k += (p.job_cnt[i][0] ? 1 : 0) + (p.job_cnt[i][1] ? 1 : 0);
     }
     return k;

@@ -257,11 +257,19 @@ __device__ __forceinline__ void col_round(const AR& ar, const TW& tw, LD&& ld, S
 
 // Forward column pass: stages 0..A-1. First round loads via `ld`, last round
 // stores via `st`; intermediate rounds go through shared memory `sm`.
+// Barrier between rounds: the whole CTA by default; a warp-specialised
+// kernel passes a named barrier over its transform warps.
+struct CtaSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
 // `ld` returns u64 residues below 4q; `st` receives the policy's output
 // (IntAr: lazy [0,4q); FpAr: canonical [0,q)), or with RAW_OUT the policy's
 // own word (ar.to_raw), for a following row pass that reads it with RAW_IN.
-template <int A, int C, int NT, int J0, bool RAW_OUT = false, class AR, class TW, class LD, class ST>
-__device__ __forceinline__ void fwd_col_rounds(u64* sm, const TW& tw, const AR& ar, LD&& ld, ST&& st) {
+template <int A, int C, int NT, int J0, bool RAW_OUT = false, class AR, class TW, class LD, class ST,
+          class SY = CtaSync>
+__device__ __forceinline__ void fwd_col_rounds(u64* sm, const TW& tw, const AR& ar, LD&& ld, ST&& st,
+                                               const SY& sync = SY{}) {
     constexpr int K = cmin(4, A - J0);
     constexpr bool FIRST = (J0 == 0);
     constexpr bool LAST = (J0 + K == A);
@@ -278,8 +286,8 @@ __device__ __forceinline__ void fwd_col_rounds(u64* sm, const TW& tw, const AR& 
     else if constexpr (LAST) col_round<A, C, NT, J0, K, true>(ar, tw, sld, gst);
     else col_round<A, C, NT, J0, K, true>(ar, tw, sld, sst);
     if constexpr (!LAST) {
-        __syncthreads();
-        fwd_col_rounds<A, C, NT, J0 + K, RAW_OUT>(sm, tw, ar, ld, st);
+        sync();
+        fwd_col_rounds<A, C, NT, J0 + K, RAW_OUT>(sm, tw, ar, ld, st, sync);
     }
 }
 

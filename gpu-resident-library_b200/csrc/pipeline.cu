@@ -13,6 +13,16 @@ namespace pl {
 
 namespace {
 
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    }
+    return n;
+}
+
 // PATH 0 / 1: the integer / FP64 job segment of a phase; PATH 2: the mixed
 // segment (both kinds interleaved, one launch).
 template <int LOGN, int PATH>
@@ -59,6 +69,9 @@ struct Launcher {
             Variant<LOGN, 0>::attrs();
             Variant<LOGN, 1>::attrs();
             Variant<LOGN, 2>::attrs();
+            p3ws_attrs<0>();
+            p3ws_attrs<1>();
+            p3ws_attrs<2>();
             cudaFuncSetAttribute(p7_moddown_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
             done = true;
         }
@@ -69,6 +82,32 @@ struct Launcher {
                 cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      maca_smem((int)dnum));
             mac_dnum = dnum;
+        }
+    }
+    // persistent warp-specialised P3 over job segment PATH: form 1 = 128
+    // conversion threads, two CTAs per SM; form 2 = 256, one CTA per SM
+    template <int PATH>
+    static void p3ws_attrs() {
+        cudaFuncSetAttribute(p3ws_modup_fwd_col<LOGN, PATH, 128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             P3WS<LOGN, 128>::SMEM);
+        cudaFuncSetAttribute(p3ws_modup_fwd_col<LOGN, PATH, 256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             P3WS<LOGN, 256>::SMEM);
+    }
+    template <int PATH>
+    static void p3ws(const Plan& p, cudaStream_t s) {
+        using G = ntt::Geo<LOGN>;
+        const uint32_t cnt = p.job_cnt[2][PATH];
+        if (!cnt) return;
+        const u32 ntiles = cnt * G::COL_TILES;
+        const uint2* J = p.d_jobs + p.job_off[2][PATH];
+        if (p.p3_form == 1) {
+            const unsigned grid = std::min<unsigned>(ntiles, 2u * (unsigned)sm_count());
+            p3ws_modup_fwd_col<LOGN, PATH, 128, 2><<<grid, P3WS<LOGN, 128>::NT, P3WS<LOGN, 128>::SMEM, s>>>(
+                p.dc, p.d_pairs, J, ntiles);
+        } else {
+            const unsigned grid = std::min<unsigned>(ntiles, (unsigned)sm_count());
+            p3ws_modup_fwd_col<LOGN, PATH, 256, 1><<<grid, P3WS<LOGN, 256>::NT, P3WS<LOGN, 256>::SMEM, s>>>(
+                p.dc, p.d_pairs, J, ntiles);
         }
     }
     static void launch(const Plan& p, cudaStream_t s, unsigned mask) {
@@ -93,7 +132,10 @@ struct Launcher {
                 if (p.job_cnt[6][0])
                     p7_moddown_inv_col<LOGN><<<p.job_cnt[6][0] * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(
                         D, p.d_pairs, p.d_jobs + p.job_off[6][0]);
-            } else if (p.mix && p.job_cnt[k][0] && p.job_cnt[k][1]) {
+            } else if (k == 2 && p.p3_form) {
+                if ((p.mix >> 2 & 1) && p.job_cnt[2][0] && p.job_cnt[2][1]) p3ws<2>(p, s);
+                else { p3ws<0>(p, s); p3ws<1>(p, s); }
+            } else if ((p.mix >> k & 1) && p.job_cnt[k][0] && p.job_cnt[k][1]) {
                 Variant<LOGN, 2>::phase(k, p, s);
             } else {
                 Variant<LOGN, 0>::phase(k, p, s);
@@ -392,11 +434,15 @@ uint64_t tune_key(const Plan& p) {
     while ((1u << (cls + 1)) <= p.nops) ++cls;   // batch-size class: floor(log2(nops))
     return ((uint64_t)p.logn << 40) | ((uint64_t)p.dc.dnum << 32) | cls;
 }
-// choice: bits 0-1 = P5 form, bit 2 = interleaved integer / FP64 jobs
+// choice: bits 0-1 = P5 form, bits 3-4 = P3 form (0 plain, 1 and 2
+// warp-specialised), bits 8-16 = phases launched over their interleaved
+// integer / FP64 job list (else as two launches)
 void apply_choice(Plan& p, int choice) {
     p.p5_form = choice & 3;
     if (p.p5_form == P5_ASYNC && !mac_async_ok(p.dc.dnum)) p.p5_form = P5_REG128;
-    p.mix = (choice & 4) != 0;
+    p.mix = ((unsigned)choice >> 8) & 0x1ffu;
+    p.p3_form = (choice >> 3) & 3;
+    if (p.p3_form > 2) p.p3_form = 0;
 }
 }  // namespace
 
@@ -410,44 +456,57 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         p.tuned = true;
         return;
     }
-    constexpr int DEFAULT = P5_REG128 | 4;       // 4-word register P5, interleaved paths
+    constexpr int DEFAULT = P5_REG128 | (0x1ff << 8);   // 4-word register P5, plain P3, interleaved paths
     apply_choice(p, DEFAULT);
     if (!measure) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
     for (const Op& op : p.ops)
         if (op.mode == RESCALE) return;          // may be in place: re-running would change its input
-    std::vector<int> cands = {DEFAULT, P5_REG128, P5_REG256 | 4, P5_REG256};
-    if (mac_async_ok(p.dc.dnum)) { cands.push_back(P5_ASYNC | 4); cands.push_back(P5_ASYNC); }
-    std::vector<float> best(cands.size(), 1e30f);
     cudaEvent_t a, b;
     if (cudaEventCreate(&a) != cudaSuccess) return;
     if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
+    launch(p, s);                                // every workspace slot holds data of this batch
     bool ok = true;
-    // two interleaved passes, best of three timed launches per candidate and pass
-    for (int pass = 0; pass < 2 && ok; ++pass)
-        for (size_t ci = 0; ci < cands.size() && ok; ++ci) {
-            apply_choice(p, cands[ci]);
-            launch(p, s);
-            for (int r = 0; r < 3; ++r) {
-                cudaEventRecord(a, s);
-                launch(p, s);
-                cudaEventRecord(b, s);
-                if (cudaEventSynchronize(b) != cudaSuccess) { ok = false; break; }
-                float ms = 0;
-                cudaEventElapsedTime(&ms, a, b);
-                best[ci] = std::min(best[ci], ms);
+    // One decision per dimension, each timed on the phases it changes: two
+    // interleaved passes, best of three launches per candidate and pass; a
+    // candidate replaces the current value only if it is 1.5% faster.
+    auto pick = [&](unsigned mask, int field_mask, const std::vector<int>& values, int cur) {
+        std::vector<float> best(values.size(), 1e30f);
+        for (int pass = 0; pass < 2 && ok; ++pass)
+            for (size_t ci = 0; ci < values.size() && ok; ++ci) {
+                apply_choice(p, (cur & ~field_mask) | values[ci]);
+                launch(p, s, mask);
+                for (int r = 0; r < 3; ++r) {
+                    cudaEventRecord(a, s);
+                    launch(p, s, mask);
+                    cudaEventRecord(b, s);
+                    if (cudaEventSynchronize(b) != cudaSuccess) { ok = false; break; }
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, a, b);
+                    best[ci] = std::min(best[ci], ms);
+                }
             }
-        }
+        size_t win = 0;                          // values[0] is the current setting
+        for (size_t ci = 1; ci < values.size(); ++ci)
+            if (best[ci] < best[win]) win = ci;
+        if (!ok || best[win] > 0.985f * best[0]) win = 0;
+        return (cur & ~field_mask) | values[win];
+    };
+    int cur = DEFAULT;
+    for (int k : {0, 1, 2, 3, 5, 7, 8}) {                          // interleaved or separate, per phase
+        if (!p.job_cnt[k][0] || !p.job_cnt[k][1]) continue;
+        const int bit = 1 << (8 + k);
+        cur = pick(1u << k, bit, {bit, 0}, cur);
+    }
+    cur = pick(1u << 2, 24, {0, 8, 16}, cur);                      // P3 form
+    std::vector<int> p5v = {P5_REG128, P5_REG256};
+    if (mac_async_ok(p.dc.dnum)) p5v.push_back(P5_ASYNC);
+    cur = pick(1u << 4, 3, p5v, cur);                              // P5 form
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    size_t win = 0;
-    for (size_t ci = 1; ci < cands.size(); ++ci)
-        if (best[ci] < best[win]) win = ci;
-    // keep the default unless a candidate is clearly faster
-    if (!ok || best[win] > 0.985f * best[0]) win = 0;
-    apply_choice(p, cands[win]);
-    c.set_tuned_choice(key, cands[win]);
+    apply_choice(p, cur);
+    c.set_tuned_choice(key, cur);
     p.tuned = true;
 }
 

@@ -316,6 +316,114 @@ p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2
     on_path<PATH>(jb, [&](auto fp) { p3_modup_fwd_col_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
 }
 
+// P3, warp-specialised form: a persistent CTA of COL_THREADS transform threads
+// and NP conversion threads over a double-buffered tile ring (MINB CTAs per SM). While the
+// transform warps run the column NTT of tile k (FP64 or integer butterflies),
+// the NP conversion threads compute the ApproxSwitchCRTBasis prologue of tile k+1
+// (integer 128-bit MACs) into the other buffer, so the two pipes overlap.
+// Hand-over uses named barriers: FULL[b] (conversion -> transform) and
+// EMPTY[b] (transform -> conversion); both sides walk the same tile sequence,
+// and a transform warp releases a buffer only if a later tile will refill it.
+// Results equal p3_modup_fwd_col's word for word.
+constexpr unsigned BAR_FULL = 1, BAR_EMPTY = 3, BAR_XFORM = 5, BAR_CONV = 6;
+
+__device__ __forceinline__ void nb_sync(unsigned id, unsigned count) {
+    asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void nb_arrive(unsigned id, unsigned count) {
+    asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+
+template <int LOGN, int NP>
+struct P3WS {
+    using G = ntt::Geo<LOGN>;
+    static constexpr int NC = G::COL_THREADS;                // transform threads
+    static constexpr int NT = NC + NP;                       // NP conversion threads
+    static constexpr int SMEM = 2 * G::COL_SMEM;
+    static constexpr int VPR = G::C / 2;
+    static constexpr int PPER = G::R1 * VPR / NP;            // 16-byte pairs per conversion thread
+    static_assert(PPER * NP == G::R1 * VPR && PPER % CS_VB == 0, "conversion geometry");
+};
+
+struct XformSync {
+    unsigned count;
+    __device__ __forceinline__ void operator()() const { nb_sync(BAR_XFORM, count); }
+};
+
+template <int LOGN, int PATH, int NP, int MINB>
+__global__ void __launch_bounds__(P3WS<LOGN, NP>::NT, MINB)
+p3ws_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs,
+                   const u32 ntiles) {
+    using G = ntt::Geo<LOGN>;
+    using W = P3WS<LOGN, NP>;
+    extern __shared__ __align__(16) u64 sm[];   // [2][COL_TILE]
+    __shared__ u64 cst[2][MAXA];
+    const bool conv = threadIdx.x >= W::NC;
+    const u32 ctid = threadIdx.x - W::NC;
+    u32 k = 0;
+    for (u32 t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        const int b = (int)(k & 1);
+        uint2 jb = jobs[t / G::COL_TILES];
+        const int c0 = (int)(t % G::COL_TILES) * G::C;
+        bool fp = PATH == 1;
+        if constexpr (PATH == 2) {
+            fp = (jb.y & JOB_FP) != 0;
+            jb.y &= ~JOB_FP;
+        }
+        const PairDesc& P = pairs[jb.x];
+        const u32 L = P.L, K = D.K, QlP = L + K;
+        const u32 p = jb.y / QlP, i = jb.y % QlP;
+        const Level& lv = D.lvl[L];
+        const u32 st0 = lv.part_st[p], sp = lv.part_sp[p];
+        const u32 qp = qp_of(i, L, D.fullQ);
+        const ModC m = D.mod[qp];
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        u64* buf = sm + (size_t)b * G::COL_TILE;
+        if (conv) {
+            if (k >= 2) nb_sync(BAR_EMPTY + b, W::NT);      // transform warps released buffer b
+            const u64* pool = D.pool + lv.qmp_off + (size_t)st0 * QlP + i;
+            if (ctid < sp) cst[b][ctid] = pool[(size_t)ctid * QlP];
+            nb_sync(BAR_CONV, NP);
+            const u64* X = slot_ptr(P, w.X + st0, LOGN) + c0;
+#pragma unroll 1
+            for (int k0 = 0; k0 < W::PPER; k0 += CS_VB) {
+                int r[CS_VB], cl[CS_VB];
+                size_t e[CS_VB];
+                u64 lo[CS_VB][2] = {}, hi[CS_VB][2] = {};
+#pragma unroll
+                for (int bb = 0; bb < CS_VB; ++bb) {
+                    const int v = (int)ctid + (k0 + bb) * NP;
+                    r[bb] = v / W::VPR;
+                    cl[bb] = 2 * (v % W::VPR);
+                    e[bb] = (size_t)r[bb] * 256 + cl[bb];
+                }
+                mac_terms<CS_VB>(lo, hi, X, (size_t)1 << LOGN, sp, cst[b], e);
+#pragma unroll
+                for (int bb = 0; bb < CS_VB; ++bb) {
+                    ulonglong2 v;
+                    v.x = barrett_lazy(lo[bb][0], hi[bb][0], m.q, m.mu_lo, m.mu_hi);
+                    v.y = barrett_lazy(lo[bb][1], hi[bb][1], m.q, m.mu_lo, m.mu_hi);
+                    *reinterpret_cast<ulonglong2*>(buf + r[bb] * G::C + cl[bb]) = v;
+                }
+            }
+            nb_arrive(BAR_FULL + b, W::NT);                 // buffer b staged
+        } else {
+            nb_sync(BAR_FULL + b, W::NT);
+            u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + c0;
+            auto ld = [&](int r, int cl) { return buf[r * G::C + cl]; };
+            auto stf = [&](int r, int cl, u64 v) { Y[r * 256 + cl] = v; };
+            const XformSync xs{(unsigned)W::NC};
+            if (fp)
+                ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(buf, twf_of<true>(D, qp, LOGN),
+                                                                         ar_of<true>(m), ld, stf, xs);
+            else
+                ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(buf, twf_of<false>(D, qp, LOGN),
+                                                                         ar_of<false>(m), ld, stf, xs);
+            if (t + 2 * gridDim.x < ntiles) nb_arrive(BAR_EMPTY + b, W::NT);   // a later tile refills b
+        }
+    }
+}
+
 // ------------------------------------------------------------------ P4
 // NTT row stages of one digit tower; output reduced to [0, 2q).
 template <int LOGN, bool FP>

@@ -37,7 +37,8 @@ struct Plan {
     std::vector<PairDesc> pairs_host;
     // launch schedule (chosen by tune() or the context's tuning cache)
     int p5_form = 0;                   // P5_REG128, P5_ASYNC or P5_REG256
-    bool mix = true;                   // one launch per phase over the interleaved job list
+    unsigned mix = 0x1ff;              // bit k: phase k+1 as one launch over its interleaved job list
+    int p3_form = 0;                   // 0 plain P3; 1, 2 warp-specialised (128 x 2 CTAs, 256 x 1 CTA)
     bool tuned = false;
     const gfx::Context* ctx = nullptr;
     void* d_blob = nullptr;            // device tables (pairs, jobs, P5 groups, pair lists)
@@ -63,9 +64,9 @@ cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
 // Picks the launch schedule of `p` (P5 form; integer and FP64 transform
 // jobs as two launches or one interleaved launch): from the context's tuning cache when it holds
 // this shape (ring size, digits, batch-size class), else by timing every
-// candidate with CUDA events on `s` (two interleaved passes, best of three
-// launches each; the default stays unless another is 1.5% faster) and
-// caching the winner. Timing re-runs the batch, so it is skipped (defaults
+// candidate with CUDA events on `s` (one dimension at a time on the phases it
+// changes; two interleaved passes, best of three launches each; a candidate
+// wins only if 1.5% faster) and caching the winner. Timing re-runs the batch, so it is skipped (defaults
 // kept) when `measure` is false, while `s` is capturing a graph, or when an
 // operation writes over its own input (in-place rescale).
 void tune(Plan& p, cudaStream_t s, bool measure = true);

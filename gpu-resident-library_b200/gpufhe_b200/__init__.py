@@ -195,7 +195,7 @@ class Plan:
         check(lib().gpufhe_plan_launch(self.h, stream))
 
     def set_schedule(self, bits):
-        """Fix the launch schedule (bits 0-1 P5 form, bit 2 interleaved paths); skips the autotuner."""
+        """Fix the launch schedule (bits 0-1 P5 form, bit 2 interleaved paths, bits 3-4 P3 form)."""
         check(lib().gpufhe_plan_set_schedule(self.h, bits))
 
     def launch_phase(self, phase, stream=None):
@@ -208,7 +208,9 @@ class Plan:
         """Autotuner choice: {'p5': form, 'mixed_paths': bool, 'tuned': bool}."""
         b = int(lib().gpufhe_plan_schedule(self.h))
         form = {0: "register-128x4", 1: "cp.async", 2: "register-256x2"}.get(b & 3, "?")
-        return {"p5": form, "mixed_paths": bool(b & 4), "tuned": bool(b & 8)}
+        p3 = {0: "plain", 1: "warp-specialised-128x2", 2: "warp-specialised-256x1"}.get((b >> 3) & 3, "?")
+        mixed = [k + 1 for k in range(9) if b >> (8 + k) & 1]
+        return {"p5": form, "mixed_paths": bool(b & 4), "mixed_phases": mixed, "p3": p3, "tuned": bool(b & 32)}
 
     def launch_host(self, h_in, h_out, stream=None):
         """h_in: list of 4 host pointers per op (0 for unused); h_out: 2 per op."""

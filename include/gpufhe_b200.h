@@ -134,12 +134,15 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
 /* Launch schedule chosen by the autotuner (first gpufhe_plan_launch outside
  * graph capture, cached per context and batch shape): bits 0-1 = P5 form
  * (0 register prefetch, 128 threads x 4 words; 1 cp.async pipelined;
- * 2 register prefetch, 256 threads x 2 words), bit 2 = integer and FP64
- * transform jobs of a phase interleaved in one launch (else two launches),
- * bit 3 = tuned. */
+ * 2 register prefetch, 256 threads x 2 words), bit 2 = every phase launches
+ * its integer and FP64 transform jobs interleaved in one launch, bits 3-4 =
+ * P3 form (0 plain; 1 warp-specialised, 128 conversion threads, two CTAs per
+ * SM; 2 warp-specialised, 256 conversion threads, one CTA per SM: conversion
+ * warps overlap the transform warps), bit 5 = tuned, bits 8-16 = the phases
+ * (bit 8 + k for phase k+1) launched interleaved (the others as two launches). */
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan);
-/* Fixes the schedule (bits 0-2 as above) and skips the autotuner; every
- * schedule computes the same bits. */
+/* Fixes the schedule (bits 0-4 and 8-16 as above; bit 2 sets every phase
+ * interleaved) and skips the autotuner; every schedule computes the same bits. */
 int      gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule);
 /* Host-buffer form: copies h_in[4*i+k] (host, level*n words) into op i's
  * device inputs, launches the batch and copies each op's outputs back into

@@ -135,7 +135,7 @@ def test_rotate_hoisted_groups(G, S, gctx):
             assert np.array_equal(host(o0), e0) and np.array_equal(host(o1), e1), (rep, j)
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2, 4, 5, 6])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 4, 5, 6, 8, 12, 13, 16, 20])
 def test_every_schedule_same_bits(G, S, gctx, schedule):
     """Each launch schedule the autotuner can pick (P5 form x interleaved or
     separate integer / FP64 transform launches) gives the oracle's bits on a
@@ -164,5 +164,6 @@ def test_every_schedule_same_bits(G, S, gctx, schedule):
     sync()
     got = plan.schedule()
     assert got["tuned"] and got["mixed_paths"] == bool(schedule & 4)
+    assert got["p3"] == ("plain", "warp-specialised-128x2", "warp-specialised-256x1")[schedule >> 3]
     for outs, (e0, e1) in want:
         assert np.array_equal(host(outs[0]), e0) and np.array_equal(host(outs[1]), e1)
