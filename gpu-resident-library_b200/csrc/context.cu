@@ -175,6 +175,25 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
     dc_.lvl = upload(lv_host_);
     dc_.pool = upload(pool);
     dc_.pinv = upload(pinv);
+    // key storage scale (see Key): Montgomery when 2 * dnum * max(q) < 2^64
+    {
+        u64 qmax = 0;
+        for (u64 q : QPm) qmax = std::max(qmax, q);
+        const unsigned __int128 bound = (unsigned __int128)2 * dnum_ * qmax;
+        dc_.mont = bound < ((unsigned __int128)1 << 64) ? 1u : 0u;
+        key_scale_.resize(QP);
+        key_scale_p_.resize(QP);
+        for (uint32_t i = 0; i < QP; ++i) {
+            const u64 q = QPm[i];
+            const u64 r = dc_.mont ? hm::mulmod((1ull << 32) % q, (1ull << 32) % q, q) : 1;   // 2^64 mod q or 1
+            const u64 v = i < fullQ ? hm::mulmod(pinv[i], r, q) : r;
+            key_scale_[i] = v;
+            key_scale_p_[i] = hm::precon(v, q);
+        }
+        std::vector<u64> ks(key_scale_);
+        ks.insert(ks.end(), key_scale_p_.begin(), key_scale_p_.end());
+        d_key_scale_ = upload(ks);
+    }
     dc_.pinvp = upload(pinvp);
     dc_.pdn = upload(pdn);
     dc_.pdnp = upload(pdnp);
@@ -188,6 +207,27 @@ Context::~Context() {
     for (auto& kv : keys_) { cudaFree(kv.second.av); cudaFree(kv.second.bv); }
     for (void* p : allocs_) cudaFree(p);
     cudaSetDevice(prev);
+}
+
+namespace {
+// key[p][r][*] = key * scale[r] mod q_r (Shoup, canonical), every digit p.
+__global__ void k_scale_key_rows(u64* __restrict__ key, const ModC* __restrict__ mod, const u64* __restrict__ sc,
+                                 uint32_t QP, uint32_t n) {
+    const uint32_t row = blockIdx.y;               // p * QP + r
+    const uint32_t r = row % QP;
+    const u64 q = mod[r].q, c = sc[r], cp = sc[QP + r];
+    u64* x = key + (size_t)row * n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[i] = shoup(x[i], c, cp, q);
+}
+}  // namespace
+
+cudaError_t scale_key_rows(u64* key, const ModC* mod, const u64* scale, uint32_t dnum, uint32_t QP, uint32_t n) {
+    const dim3 g((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, dnum * QP);
+    k_scale_key_rows<<<g, 256>>>(key, mod, scale, QP, n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return e;
 }
 
 void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
@@ -204,6 +244,14 @@ void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
     };
     k.av = up(av);
     k.bv = up(bv);
+    for (u64* d : {k.av, k.bv}) {
+        const cudaError_t e = scale_key_rows(d, dc_.mod, d_key_scale_, dnum_, fullQ() + K(), n_);
+        if (e != cudaSuccess) {
+            cudaFree(k.av);
+            cudaFree(k.bv);
+            throw std::runtime_error(std::string("key scaling: ") + cudaGetErrorString(e));
+        }
+    }
     auto it = keys_.find(id);
     if (it != keys_.end()) { cudaFree(it->second.av); cudaFree(it->second.bv); }
     keys_[id] = k;

@@ -35,6 +35,7 @@ struct Level {
 
 struct DevCtx {
     u32 n, logn, fullQ, K, alpha, dnum, QP;
+    u32 mont;                 // keys are stored times 2^64 (Montgomery form), see Context::set_key
     const ModC* mod;          // [QP]: Q towers then P towers
     const Tw* twf;            // [QP][n]
     const Tw* twi;            // [QP][n]
@@ -51,8 +52,12 @@ struct DevCtx {
     const u64* phatmodq;      // [K][fullQ] (P/p_j) mod q_i
 };
 
-// A resident eval key: av/bv over full QP for every digit, canonical eval
-// form, layout [dnum][fullQ+K][n].
+// A resident eval key: av/bv over full QP for every digit, eval form, layout
+// [dnum][fullQ+K][n]. Stored scaled: row of Q modulus q_i times P^-1 * R,
+// row of P modulus p_j times R, canonical, with R = 2^64 when the key-switch
+// accumulator bound 2*dnum*max(q) < 2^64 allows Montgomery reduction (DevCtx
+// mont = 1), else R = 1. The inner product then yields res * P^-1 on Q rows
+// directly and needs one Montgomery (or Barrett) reduction per accumulator.
 struct Key {
     u64* av = nullptr;
     u64* bv = nullptr;
@@ -95,6 +100,8 @@ private:
     int device_;
     std::vector<u64> Q_, P_, roots_;
     std::vector<Level> lv_host_;
+    std::vector<u64> key_scale_, key_scale_p_;   // per QP row: P^-1 * R (Q) or R (P), Shoup precon
+    u64* d_key_scale_ = nullptr;                 // [2][QP] on the device
     DevCtx dc_{};
     std::vector<void*> allocs_;
     size_t table_bytes_ = 0;
@@ -105,6 +112,9 @@ private:
     template <class T>
     T* upload(const std::vector<T>& h);
 };
+
+// Applies the key storage scale of every row (Key) in place on the device.
+cudaError_t scale_key_rows(u64* key, const ModC* mod, const u64* scale, uint32_t dnum, uint32_t QP, uint32_t n);
 
 std::string last_error();
 void set_error(const std::string& s);

@@ -20,7 +20,18 @@ struct __align__(16) ModC {
     u64 mu_lo, mu_hi;   // floor(2^128 / q)
     u64 r64;            // floor(2^64 / q)
     u64 qinv_bits;      // bits of the double RN(1/q) (FP64 NTT path)
+    u64 qneg;           // -q^-1 mod 2^64 (Montgomery reduction)
+    u64 pad_;
 };
+
+// Montgomery reduction: T = hi*2^64 + lo < q*2^64 -> T * 2^-64 mod q in [0, q).
+// m = lo * (-q^-1) makes T + m*q divisible by 2^64; its low word sums to 0 or
+// 2^64, carrying 1 exactly when lo != 0.
+__device__ __forceinline__ u64 redc(u64 lo, u64 hi, const ModC& m) {
+    const u64 mm = lo * m.qneg;
+    const u64 t = hi + __umul64hi(mm, m.q) + (lo != 0 ? 1ull : 0ull);
+    return t >= m.q ? t - m.q : t;
+}
 
 // Towers whose transforms may take the FP64 path (4q < 2^52).
 __host__ __device__ __forceinline__ bool fp_tower(u64 q) { return q < (1ull << 50); }

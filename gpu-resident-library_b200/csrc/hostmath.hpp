@@ -36,6 +36,10 @@ inline ModC modc(u64 q) {
     m.r64 = (~0ull) / q;
     const double qinv = 1.0 / (double)q;   // RN(1/q), the FP64 NTT path's quotient scale
     std::memcpy(&m.qinv_bits, &qinv, 8);
+    u64 inv = q;                            // q^-1 mod 2^64 by Newton (q odd): 3 -> 6 -> ... -> 96 bits
+    for (int i = 0; i < 5; ++i) inv *= 2 - q * inv;
+    m.qneg = 0 - inv;
+    m.pad_ = 0;
     return m;
 }
 

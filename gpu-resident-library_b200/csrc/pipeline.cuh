@@ -470,6 +470,13 @@ constexpr int MAC_PCH = 4;
 __device__ __forceinline__ u64 v2get(const ulonglong2& v, int j) { return j ? v.y : v.x; }
 __device__ __forceinline__ void v2set(ulonglong2& v, int j, u64 x) { if (j) v.y = x; else v.x = x; }
 
+// One key-switch accumulator -> res (P rows) or res * P^-1 (Q rows), canonical:
+// the stored key carries P^-1 on Q rows and, with D.mont, the factor 2^64
+// that the Montgomery reduction removes.
+__device__ __forceinline__ u64 acc_reduce(u64 lo, u64 hi, const ModC& m, u32 mont) {
+    return mont ? redc(lo, hi, m) : barrett(lo, hi, m);
+}
+
 template <int LOGN, int NT>
 __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 3)
 p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
@@ -591,8 +598,8 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
         for (int k = 0; k < NV; ++k)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                v2set(r0[k], j, barrett(a0l[2 * k + j], a0h[2 * k + j], m));
-                v2set(r1[k], j, barrett(a1l[2 * k + j], a1h[2 * k + j], m));
+                v2set(r0[k], j, acc_reduce(a0l[2 * k + j], a0h[2 * k + j], m, D.mont));
+                v2set(r1[k], j, acc_reduce(a1l[2 * k + j], a1h[2 * k + j], m, D.mont));
             }
         u64 *d0, *d1;
         if (is_p) {
@@ -606,26 +613,19 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
             }
             continue;
         }
-        const u64 pv = D.pinv[i], pvp = D.pinvp[i];
-        if (!emr) {   // keyswitch / rotation: W = res * P^-1
+        if (!emr) {   // keyswitch / rotation: W = res * P^-1 (the reduced accumulator)
             d0 = slot_ptr(P, w.W + i, LOGN) + tile0;
             d1 = slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
             for (int k = 0; k < NV; ++k) {
                 const u32 e = 2 * (threadIdx.x + k * NT);
-                ulonglong2 o0, o1;
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    v2set(o0, j, shoup(v2get(r0[k], j), pv, pvp, q));
-                    v2set(o1, j, shoup(v2get(r1[k], j), pv, pvp, q));
-                }
-                *reinterpret_cast<ulonglong2*>(d0 + e) = o0;
-                *reinterpret_cast<ulonglong2*>(d1 + e) = o1;
+                *reinterpret_cast<ulonglong2*>(d0 + e) = r0[k];
+                *reinterpret_cast<ulonglong2*>(d1 + e) = r1[k];
             }
             continue;
         }
         const bool drop = i == L - 1;
-        const u64 s1 = lv.s1[i], s1p = lv.s1p[i], ps1 = lv.ps1[i], ps1p = lv.ps1p[i];
+        const u64 s1 = lv.s1[i], s1p = lv.s1p[i];
         d0 = drop ? slot_ptr(P, w.U, LOGN) + tile0 : slot_ptr(P, w.W + i, LOGN) + tile0;
         d1 = drop ? slot_ptr(P, w.U + 1, LOGN) + tile0 : slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
@@ -634,15 +634,11 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
             ulonglong2 o0, o1;
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const u64 ta = v2get(t0[k], j), tb = v2get(t1[k], j);
-                const u64 ra = v2get(r0[k], j), rb = v2get(r1[k], j);
-                if (drop) {   // u = t + res * P^-1 (eval), INTT'd in P6/P7
-                    v2set(o0, j, csub(ta + shoup(ra, pv, pvp, q), q));
-                    v2set(o1, j, csub(tb + shoup(rb, pv, pvp, q), q));
-                } else {      // W = t*s1 + res*P^-1*s1
-                    v2set(o0, j, csub(csub(shoup_lazy(ta, s1, s1p, q) + shoup_lazy(ra, ps1, ps1p, q), m.two_q), q));
-                    v2set(o1, j, csub(csub(shoup_lazy(tb, s1, s1p, q) + shoup_lazy(rb, ps1, ps1p, q), m.two_q), q));
-                }
+                // u = t + res * P^-1 (eval, INTT'd in P6/P7); W = (t + res * P^-1) * s1
+                const u64 ua = csub(v2get(t0[k], j) + v2get(r0[k], j), q);
+                const u64 ub = csub(v2get(t1[k], j) + v2get(r1[k], j), q);
+                v2set(o0, j, drop ? ua : shoup(ua, s1, s1p, q));
+                v2set(o1, j, drop ? ub : shoup(ub, s1, s1p, q));
             }
             *reinterpret_cast<ulonglong2*>(d0 + e) = o0;
             *reinterpret_cast<ulonglong2*>(d1 + e) = o1;
@@ -779,8 +775,8 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
         ulonglong2 r0, r1;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            v2set(r0, j, barrett(a0l[j], a0h[j], m));
-            v2set(r1, j, barrett(a1l[j], a1h[j], m));
+            v2set(r0, j, acc_reduce(a0l[j], a0h[j], m, D.mont));
+            v2set(r1, j, acc_reduce(a1l[j], a1h[j], m, D.mont));
         }
         const u64 q = m.q;
         if (is_p) {
@@ -788,32 +784,24 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
             *reinterpret_cast<ulonglong2*>(slot_ptr(P, w.RP + K + (i - L), LOGN) + tile0 + e) = r1;
             continue;
         }
-        const u64 pv = D.pinv[i], pvp = D.pinvp[i];
         ulonglong2 o0, o1;
         u64 *d0, *d1;
-        if (!emr) {   // keyswitch / rotation: W = res * P^-1
+        if (!emr) {   // keyswitch / rotation: W = res * P^-1 (the reduced accumulator)
             d0 = slot_ptr(P, w.W + i, LOGN);
             d1 = slot_ptr(P, w.W + L + i, LOGN);
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                v2set(o0, j, shoup(v2get(r0, j), pv, pvp, q));
-                v2set(o1, j, shoup(v2get(r1, j), pv, pvp, q));
-            }
+            o0 = r0;
+            o1 = r1;
         } else {
             const bool drop = i == L - 1;
-            const u64 s1 = lv.s1[i], s1p = lv.s1p[i], ps1 = lv.ps1[i], ps1p = lv.ps1p[i];
+            const u64 s1 = lv.s1[i], s1p = lv.s1p[i];
             d0 = drop ? slot_ptr(P, w.U, LOGN) : slot_ptr(P, w.W + i, LOGN);
             d1 = drop ? slot_ptr(P, w.U + 1, LOGN) : slot_ptr(P, w.W + L + i, LOGN);
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const u64 ta = v2get(t0, j), tb = v2get(t1, j), ra = v2get(r0, j), rb = v2get(r1, j);
-                if (drop) {
-                    v2set(o0, j, csub(ta + shoup(ra, pv, pvp, q), q));
-                    v2set(o1, j, csub(tb + shoup(rb, pv, pvp, q), q));
-                } else {
-                    v2set(o0, j, csub(csub(shoup_lazy(ta, s1, s1p, q) + shoup_lazy(ra, ps1, ps1p, q), m.two_q), q));
-                    v2set(o1, j, csub(csub(shoup_lazy(tb, s1, s1p, q) + shoup_lazy(rb, ps1, ps1p, q), m.two_q), q));
-                }
+                const u64 ua = csub(v2get(t0, j) + v2get(r0, j), q);
+                const u64 ub = csub(v2get(t1, j) + v2get(r1, j), q);
+                v2set(o0, j, drop ? ua : shoup(ua, s1, s1p, q));
+                v2set(o1, j, drop ? ub : shoup(ub, s1, s1p, q));
             }
         }
         *reinterpret_cast<ulonglong2*>(d0 + tile0 + e) = o0;

@@ -368,7 +368,7 @@ DeviceKSWork ks_work_create(const DeviceKSContext& C) {
         pl::Op op;
         op.L = L;
         op.mode = pl::KS;
-        static u64 dummy[2];
+        alignas(16) static u64 dummy[2];
         op.in[0] = dummy;   // rebound on every call
         op.out[0] = op.out[1] = dummy;
         wi->plan = pl::build_plan(*ctx, {op}, W.d_ws, words);
