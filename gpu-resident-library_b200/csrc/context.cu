@@ -106,6 +106,14 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
         for (uint32_t i = 0; i < fullQ; ++i) phatmodq[(size_t)j * fullQ + i] = hm::prod_mod(P.data(), K, Q[i], (int)j);
     }
 
+    // Montgomery conversions when the accumulated sums stay below q * 2^64
+    u64 qmaxQ = 0, qmaxP = 0;
+    for (u64 q : Q) qmaxQ = std::max(qmaxQ, q);
+    for (u64 p : P) qmaxP = std::max(qmaxP, p);
+    dc_.mont_up = ((unsigned __int128)alpha * qmaxQ < ((unsigned __int128)1 << 64)) ? 1u : 0u;
+    dc_.mont_down = ((unsigned __int128)K * qmaxP < ((unsigned __int128)1 << 64)) ? 1u : 0u;
+    auto r64mod = [](u64 m) { return hm::mulmod((1ull << 32) % m, (1ull << 32) % m, m); };
+
     // per-level constants
     lv_host_.assign(fullQ + 1, Level{});
     std::vector<u64> pool;
@@ -128,7 +136,8 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
             lv.up_scale_p[i] = hm::precon(lv.up_scale[i], q);
             for (uint32_t j = 0; j < QlP; ++j) {
                 const u64 m = j < L ? Q[j] : P[j - L];
-                pool.push_back(hm::prod_mod(Q.data() + st, sp, m, (int)(i - st)));
+                const u64 v = hm::prod_mod(Q.data() + st, sp, m, (int)(i - st));
+                pool.push_back(dc_.mont_up ? hm::mulmod(v, r64mod(m), m) : v);
             }
         }
         if (L >= 2) {

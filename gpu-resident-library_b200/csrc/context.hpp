@@ -36,6 +36,8 @@ struct Level {
 struct DevCtx {
     u32 n, logn, fullQ, K, alpha, dnum, QP;
     u32 mont;                 // keys are stored times 2^64 (Montgomery form), see Context::set_key
+    u32 mont_up;              // ModUp pool entries carry 2^64: P3 reduces with Montgomery (alpha * max q < 2^64)
+    u32 mont_down;            // P7 / P8 conversions reduce with Montgomery (K * max p < 2^64)
     const ModC* mod;          // [QP]: Q towers then P towers
     const Tw* twf;            // [QP][n]
     const Tw* twi;            // [QP][n]

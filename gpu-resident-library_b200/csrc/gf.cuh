@@ -27,11 +27,16 @@ struct __align__(16) ModC {
 // Montgomery reduction: T = hi*2^64 + lo < q*2^64 -> T * 2^-64 mod q in [0, q).
 // m = lo * (-q^-1) makes T + m*q divisible by 2^64; its low word sums to 0 or
 // 2^64, carrying 1 exactly when lo != 0.
-__device__ __forceinline__ u64 redc(u64 lo, u64 hi, const ModC& m) {
+__device__ __forceinline__ u64 redc_lazy(u64 lo, u64 hi, const ModC& m) {   // result in [0, 2q)
     const u64 mm = lo * m.qneg;
-    const u64 t = hi + __umul64hi(mm, m.q) + (lo != 0 ? 1ull : 0ull);
+    return hi + __umul64hi(mm, m.q) + (lo != 0 ? 1ull : 0ull);
+}
+__device__ __forceinline__ u64 redc(u64 lo, u64 hi, const ModC& m) {
+    const u64 t = redc_lazy(lo, hi, m);
     return t >= m.q ? t - m.q : t;
 }
+// 2^64 mod q from r64 = floor(2^64 / q): 2^64 - q * r64, computed mod 2^64.
+__device__ __forceinline__ u64 r_mod(const ModC& m) { return 0ull - m.q * m.r64; }
 
 // Towers whose transforms may take the FP64 path (4q < 2^52).
 __host__ __device__ __forceinline__ bool fp_tower(u64 q) { return q < (1ull << 50); }

@@ -171,6 +171,18 @@ struct ColStage {
 
 __device__ __forceinline__ ulonglong2 ld2(const u64* p) { return *reinterpret_cast<const ulonglong2*>(p); }
 
+// One key-switch accumulator -> res (P rows) or res * P^-1 (Q rows), canonical:
+// the stored key carries P^-1 on Q rows and, with D.mont, the factor 2^64
+// that the Montgomery reduction removes.
+__device__ __forceinline__ u64 acc_reduce(u64 lo, u64 hi, const ModC& m, u32 mont) {
+    return mont ? redc(lo, hi, m) : barrett(lo, hi, m);
+}
+// A basis-conversion sum whose constants carry 2^64 when `mont` (else plain):
+// lazy residue in [0, 4q).
+__device__ __forceinline__ u64 conv_reduce(u64 lo, u64 hi, const ModC& m, u32 mont) {
+    return mont ? redc_lazy(lo, hi, m) : barrett_lazy(lo, hi, m.q, m.mu_lo, m.mu_hi);
+}
+
 // lo/hi[b][j] += sum_{t < nterms} base[t * stride + e[b] + j] * coef[t] (128-bit).
 template <int VB>
 __device__ __forceinline__ void mac_terms(u64 (&lo)[VB][2], u64 (&hi)[VB][2], const u64* base, size_t stride,
@@ -297,8 +309,8 @@ __device__ __forceinline__ void p3_modup_fwd_col_body(const DevCtx& D, const Pai
 #pragma unroll
         for (int b = 0; b < CS_VB; ++b) {
             ulonglong2 v;
-            v.x = barrett_lazy(lo[b][0], hi[b][0], m.q, m.mu_lo, m.mu_hi);
-            v.y = barrett_lazy(lo[b][1], hi[b][1], m.q, m.mu_lo, m.mu_hi);
+            v.x = conv_reduce(lo[b][0], hi[b][0], m, D.mont_up);
+            v.y = conv_reduce(lo[b][1], hi[b][1], m, D.mont_up);
             *reinterpret_cast<ulonglong2*>(sm + r[b] * G::C + cl[b]) = v;
         }
     }
@@ -401,8 +413,8 @@ p3ws_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
 #pragma unroll
                 for (int bb = 0; bb < CS_VB; ++bb) {
                     ulonglong2 v;
-                    v.x = barrett_lazy(lo[bb][0], hi[bb][0], m.q, m.mu_lo, m.mu_hi);
-                    v.y = barrett_lazy(lo[bb][1], hi[bb][1], m.q, m.mu_lo, m.mu_hi);
+                    v.x = conv_reduce(lo[bb][0], hi[bb][0], m, D.mont_up);
+                    v.y = conv_reduce(lo[bb][1], hi[bb][1], m, D.mont_up);
                     *reinterpret_cast<ulonglong2*>(buf + r[bb] * G::C + cl[bb]) = v;
                 }
             }
@@ -470,12 +482,6 @@ constexpr int MAC_PCH = 4;
 __device__ __forceinline__ u64 v2get(const ulonglong2& v, int j) { return j ? v.y : v.x; }
 __device__ __forceinline__ void v2set(ulonglong2& v, int j, u64 x) { if (j) v.y = x; else v.x = x; }
 
-// One key-switch accumulator -> res (P rows) or res * P^-1 (Q rows), canonical:
-// the stored key carries P^-1 on Q rows and, with D.mont, the factor 2^64
-// that the Montgomery reduction removes.
-__device__ __forceinline__ u64 acc_reduce(u64 lo, u64 hi, const ModC& m, u32 mont) {
-    return mont ? redc(lo, hi, m) : barrett(lo, hi, m);
-}
 
 template <int LOGN, int NT>
 __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 3)
@@ -908,8 +914,7 @@ __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 
     const bool larger = q > ql;
     const u64 diff = larger ? q - ql : (ql - q) % q;
     const u64 s2 = lv.s2[i], s2p = lv.s2p[i];
-    const u64 cm = MODE == EMR ? lv.ps1[i] : D.pinv[i];
-    const u64 cmp = MODE == EMR ? lv.ps1p[i] : D.pinvp[i];
+
     // v = sw_i(r_l) * s2 - conv'_i * cm, lazy in [0, 4q)
     auto finish = [&](u64 x, u64 lo, u64 hi) -> u64 {
         u64 v = 0;
@@ -920,7 +925,11 @@ __device__ __forceinline__ void p8_body(const DevCtx& D, const PairDesc& P, u32 
             else { const u64 xm = reduce64(x, m); sw = xm >= d ? xm - d : xm + q - d; }
             v = shoup_lazy(sw, s2, s2p, q);
         }
-        if constexpr (MODE != RESCALE) v += 2 * q - shoup_lazy(barrett_lazy(lo, hi, q, m.mu_lo, m.mu_hi), cm, cmp, q);
+        if constexpr (MODE != RESCALE) {   // conv'_i * cm, folded into the constants
+            u64 c = conv_reduce(lo, hi, m, D.mont_down);   // [0, 4q)
+            c = csub(c, 2 * q);                            // [0, 2q)
+            v += 2 * q - c;
+        }
         return v;
     };
 #pragma unroll 1
@@ -962,7 +971,16 @@ __device__ __forceinline__ void p8_moddown_fwd_col_body(const DevCtx& D, const P
     const int c0 = tile * ntt::Geo<LOGN>::C;
     const PairDesc& P = pairs[jb.x];
     const u32 c = jb.y / P.L, i = jb.y % P.L;
-    if (threadIdx.x < D.K) ci[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + i];
+    if (threadIdx.x < D.K) {
+        // PHatModq[j][i] times the combine factor cm (P^-1 * s1 for EvalMult+Rescale,
+        // P^-1 otherwise) and, with mont_down, 2^64: the staged sum then reduces
+        // straight to conv'_i * cm
+        const ModC mi = D.mod[i];
+        const u64 cm = P.mode == EMR ? D.lvl[P.L].ps1[i] : D.pinv[i];
+        u64 v = mulmod(D.phatmodq[threadIdx.x * D.fullQ + i], cm, mi);
+        if (D.mont_down) v = mulmod(v, r_mod(mi), mi);
+        ci[threadIdx.x] = v;
+    }
     __syncthreads();
     if (P.mode == EMR) p8_body<LOGN, EMR, FP>(D, P, c, i, c0, sm, ci);
     else if (P.mode == RESCALE) p8_body<LOGN, RESCALE, FP>(D, P, c, i, c0, sm, ci);
