@@ -92,6 +92,14 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
         ninvp[i] = hm::precon(ninv[i], q);
     }
 
+    // Montgomery form of the keys when the key-switch sums stay below q * 2^64 (Key)
+    {
+        u64 qmax = 0;
+        for (u64 q : QPm) qmax = std::max(qmax, q);
+        dc_.mont = ((unsigned __int128)2 * dnum_ * qmax < ((unsigned __int128)1 << 64)) ? 1u : 0u;
+    }
+    auto rmod = [&](u64 m) { return dc_.mont ? hm::mulmod((1ull << 32) % m, (1ull << 32) % m, m) : (u64)1; };
+
     // level-independent ModDown constants
     std::vector<u64> pinv(fullQ), pinvp(fullQ), pdn(K), pdnp(K), phatmodq((size_t)K * fullQ);
     for (uint32_t i = 0; i < fullQ; ++i) {
@@ -156,6 +164,8 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
                 u128 pm1 = prod == 0 ? m2 - 1 : prod - 1;
                 lv.s2[i] = (u64)((pm1 / ql) % qi);
                 lv.s1p[i] = hm::precon(lv.s1[i], qi);
+                lv.s1r[i] = hm::mulmod(lv.s1[i], rmod(qi), qi);
+                lv.s1rp[i] = hm::precon(lv.s1r[i], qi);
                 lv.s2p[i] = hm::precon(lv.s2[i], qi);
                 lv.ps1[i] = hm::mulmod(pinv[i], lv.s1[i], qi);
                 lv.ps1p[i] = hm::precon(lv.ps1[i], qi);
@@ -184,24 +194,26 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
     dc_.lvl = upload(lv_host_);
     dc_.pool = upload(pool);
     dc_.pinv = upload(pinv);
-    // key storage scale (see Key): Montgomery when 2 * dnum * max(q) < 2^64
+    // key storage scale per (digit, row), see Key; n^-1 for U in P7
     {
-        u64 qmax = 0;
-        for (u64 q : QPm) qmax = std::max(qmax, q);
-        const unsigned __int128 bound = (unsigned __int128)2 * dnum_ * qmax;
-        dc_.mont = bound < ((unsigned __int128)1 << 64) ? 1u : 0u;
-        key_scale_.resize(QP);
-        key_scale_p_.resize(QP);
-        for (uint32_t i = 0; i < QP; ++i) {
-            const u64 q = QPm[i];
-            const u64 r = dc_.mont ? hm::mulmod((1ull << 32) % q, (1ull << 32) % q, q) : 1;   // 2^64 mod q or 1
-            const u64 v = i < fullQ ? hm::mulmod(pinv[i], r, q) : r;
-            key_scale_[i] = v;
-            key_scale_p_[i] = hm::precon(v, q);
-        }
-        std::vector<u64> ks(key_scale_);
-        ks.insert(ks.end(), key_scale_p_.begin(), key_scale_p_.end());
+        const size_t rows = (size_t)dnum_ * QP;
+        std::vector<u64> ks(2 * rows);
+        for (uint32_t p = 0; p < dnum_; ++p)
+            for (uint32_t i = 0; i < QP; ++i) {
+                const u64 q = QPm[i];
+                u64 v = rmod(q);
+                if (i < fullQ) v = hm::mulmod(pinv[i], i / alpha == p ? v : 1, q);
+                ks[(size_t)p * QP + i] = v;
+                ks[rows + (size_t)p * QP + i] = hm::precon(v, q);
+            }
         d_key_scale_ = upload(ks);
+        std::vector<u64> nu(fullQ), nup(fullQ);
+        for (uint32_t i = 0; i < fullQ; ++i) {
+            nu[i] = hm::mulmod(ninv[i], rmod(Q[i]), Q[i]);
+            nup[i] = hm::precon(nu[i], Q[i]);
+        }
+        dc_.ninvu = upload(nu);
+        dc_.ninvup = upload(nup);
     }
     dc_.pinvp = upload(pinvp);
     dc_.pdn = upload(pdn);
@@ -221,10 +233,10 @@ Context::~Context() {
 namespace {
 // key[p][r][*] = key * scale[r] mod q_r (Shoup, canonical), every digit p.
 __global__ void k_scale_key_rows(u64* __restrict__ key, const ModC* __restrict__ mod, const u64* __restrict__ sc,
-                                 uint32_t QP, uint32_t n) {
+                                 uint32_t QP, uint32_t rows, uint32_t n) {
     const uint32_t row = blockIdx.y;               // p * QP + r
     const uint32_t r = row % QP;
-    const u64 q = mod[r].q, c = sc[r], cp = sc[QP + r];
+    const u64 q = mod[r].q, c = sc[row], cp = sc[rows + row];
     u64* x = key + (size_t)row * n;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         x[i] = shoup(x[i], c, cp, q);
@@ -233,7 +245,7 @@ __global__ void k_scale_key_rows(u64* __restrict__ key, const ModC* __restrict__
 
 cudaError_t scale_key_rows(u64* key, const ModC* mod, const u64* scale, uint32_t dnum, uint32_t QP, uint32_t n) {
     const dim3 g((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, dnum * QP);
-    k_scale_key_rows<<<g, 256>>>(key, mod, scale, QP, n);
+    k_scale_key_rows<<<g, 256>>>(key, mod, scale, QP, dnum * QP, n);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return e;

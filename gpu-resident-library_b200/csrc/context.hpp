@@ -29,6 +29,7 @@ struct Level {
     u64 up_scale[MAXQ], up_scale_p[MAXQ];    // n^-1 * QHatInv_i (i's digit) mod q_i
     // rescale of tower L-1 onto i < L-1
     u64 s1[MAXQ], s1p[MAXQ];           // q_l^-1 mod q_i
+    u64 s1r[MAXQ], s1rp[MAXQ];         // s1 * 2^64 mod q_i with DevCtx mont, else s1 (P5 EvalMult epilogue)
     u64 s2[MAXQ], s2p[MAXQ];           // floor(Ql*(Ql^-1 mod q_l)/q_l) mod q_i
     u64 ps1[MAXQ], ps1p[MAXQ];         // P^-1 * s1 mod q_i
 };
@@ -45,6 +46,8 @@ struct DevCtx {
     const double* twid;       // [QP][n] inverse twiddles as doubles
     const u64* ninv;          // [QP] n^-1 mod q
     const u64* ninvp;
+    const u64* ninvu;         // [fullQ] n^-1 * 2^64 mod q with mont, else n^-1 (P7 scaling of U)
+    const u64* ninvup;
     const Level* lvl;         // [fullQ + 1]
     const u64* pool;          // qhatmodp pools
     const u64* pinv;          // [fullQ] P^-1 mod q_i
@@ -55,11 +58,15 @@ struct DevCtx {
 };
 
 // A resident eval key: av/bv over full QP for every digit, eval form, layout
-// [dnum][fullQ+K][n]. Stored scaled: row of Q modulus q_i times P^-1 * R,
-// row of P modulus p_j times R, canonical, with R = 2^64 when the key-switch
-// accumulator bound 2*dnum*max(q) < 2^64 allows Montgomery reduction (DevCtx
-// mont = 1), else R = 1. The inner product then yields res * P^-1 on Q rows
-// directly and needs one Montgomery (or Barrett) reduction per accumulator.
+// [dnum][fullQ+K][n]. Stored scaled, canonical, with R = 2^64 when the
+// key-switch accumulator bound 2*dnum*max(q) < 2^64 allows Montgomery
+// reduction (DevCtx mont = 1), else R = 1:
+//   P row j (every digit):                 key * R mod p_j
+//   Q row i, digit i / alpha (own digit):  key * P^-1 * R mod q_i
+//   Q row i, other digits:                 key * P^-1 mod q_i
+// With mont, the own-digit source enters the inner product as src * R^-1
+// (the EvalMult tensor products are Montgomery products), so every Q-row sum
+// is res * P^-1 exactly and every P-row sum is res * R.
 struct Key {
     u64* av = nullptr;
     u64* bv = nullptr;
@@ -102,8 +109,7 @@ private:
     int device_;
     std::vector<u64> Q_, P_, roots_;
     std::vector<Level> lv_host_;
-    std::vector<u64> key_scale_, key_scale_p_;   // per QP row: P^-1 * R (Q) or R (P), Shoup precon
-    u64* d_key_scale_ = nullptr;                 // [2][QP] on the device
+    u64* d_key_scale_ = nullptr;                 // [2][dnum * QP] row scale and Shoup precon (Key)
     DevCtx dc_{};
     std::vector<void*> allocs_;
     size_t table_bytes_ = 0;

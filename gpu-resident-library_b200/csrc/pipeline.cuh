@@ -533,27 +533,37 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
 #pragma unroll
                 for (int k = 0; k < NV; ++k)
 #pragma unroll
-                    for (int j = 0; j < 2; ++j) {
+                    for (int j = 0; j < 2; ++j) {   // tensor (Montgomery products with D.mont, see Key)
                         const u64 a0 = v2get(x0[k], j), a1 = v2get(x1[k], j);
                         const u64 b0 = v2get(y0[k], j), b1 = v2get(y1[k], j);
-                        v2set(s[k], j, mulmod(a1, b1, m));
-                        v2set(t0[k], j, mulmod(a0, b0, m));
                         u64 lo, hi;
+                        mul_wide(a1, b1, lo, hi);
+                        v2set(s[k], j, acc_reduce(lo, hi, m, D.mont));
+                        mul_wide(a0, b0, lo, hi);
+                        v2set(t0[k], j, acc_reduce(lo, hi, m, D.mont));
                         mul_wide(a0, b1, lo, hi);
                         mac_wide(lo, hi, a1, b0);
-                        v2set(t1[k], j, barrett(lo, hi, m));
+                        v2set(t1[k], j, acc_reduce(lo, hi, m, D.mont));
                     }
-            } else if (P.mode == ROT || P.mode == HROT) {
-                const u64* src = P.in[1] + ((size_t)i << LOGN);
-#pragma unroll
-                for (int k = 0; k < NV; ++k)
-#pragma unroll
-                    for (int j = 0; j < 2; ++j)
-                        v2set(s[k], j, src[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * NT) + j, P.galois)]);
             } else {
+                if (P.mode == ROT || P.mode == HROT) {
+                    const u64* src = P.in[1] + ((size_t)i << LOGN);
 #pragma unroll
-                for (int k = 0; k < NV; ++k)
-                    s[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + 2 * (threadIdx.x + k * NT));
+                    for (int k = 0; k < NV; ++k)
+#pragma unroll
+                        for (int j = 0; j < 2; ++j)
+                            v2set(s[k], j, src[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * NT) + j, P.galois)]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < NV; ++k)
+                        s[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + 2 * (threadIdx.x + k * NT));
+                }
+                if (D.mont) {   // own-digit source times R^-1 (Key)
+#pragma unroll
+                    for (int k = 0; k < NV; ++k)
+#pragma unroll
+                        for (int j = 0; j < 2; ++j) v2set(s[k], j, redc(v2get(s[k], j), 0, m));
+                }
             }
         }
         u64 a0l[2 * NV], a0h[2 * NV], a1l[2 * NV], a1h[2 * NV];
@@ -599,13 +609,16 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
                 }
             }
         }
+        // P rows and EvalMult Q rows carry R^-1 after Montgomery; keyswitch /
+        // rotation Q rows are plain sums (Key)
+        const u32 use_redc = D.mont && (is_p || emr);
         ulonglong2 r0[NV], r1[NV];
 #pragma unroll
         for (int k = 0; k < NV; ++k)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                v2set(r0[k], j, acc_reduce(a0l[2 * k + j], a0h[2 * k + j], m, D.mont));
-                v2set(r1[k], j, acc_reduce(a1l[2 * k + j], a1h[2 * k + j], m, D.mont));
+                v2set(r0[k], j, acc_reduce(a0l[2 * k + j], a0h[2 * k + j], m, use_redc));
+                v2set(r1[k], j, acc_reduce(a1l[2 * k + j], a1h[2 * k + j], m, use_redc));
             }
         u64 *d0, *d1;
         if (is_p) {
@@ -631,7 +644,7 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
             continue;
         }
         const bool drop = i == L - 1;
-        const u64 s1 = lv.s1[i], s1p = lv.s1p[i];
+        const u64 s1 = lv.s1r[i], s1p = lv.s1rp[i];
         d0 = drop ? slot_ptr(P, w.U, LOGN) + tile0 : slot_ptr(P, w.W + i, LOGN) + tile0;
         d1 = drop ? slot_ptr(P, w.U + 1, LOGN) + tile0 : slot_ptr(P, w.W + L + i, LOGN) + tile0;
 #pragma unroll
@@ -753,19 +766,27 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
                     const u64 a0 = v2get(x0, j), a1 = v2get(x1, j), b0 = v2get(y0, j), b1 = v2get(y1, j);
-                    v2set(s, j, mulmod(a1, b1, m));
-                    v2set(t0, j, mulmod(a0, b0, m));
                     u64 lo, hi;
+                    mul_wide(a1, b1, lo, hi);
+                    v2set(s, j, acc_reduce(lo, hi, m, D.mont));
+                    mul_wide(a0, b0, lo, hi);
+                    v2set(t0, j, acc_reduce(lo, hi, m, D.mont));
                     mul_wide(a0, b1, lo, hi);
                     mac_wide(lo, hi, a1, b0);
-                    v2set(t1, j, barrett(lo, hi, m));
+                    v2set(t1, j, acc_reduce(lo, hi, m, D.mont));
                 }
-            } else if (P.mode == ROT || P.mode == HROT) {
-                const u64* src = P.in[1] + ((size_t)i << LOGN);
-#pragma unroll
-                for (int j = 0; j < 2; ++j) v2set(s, j, src[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
             } else {
-                s = ld2(sb + MAC_TILE);
+                if (P.mode == ROT || P.mode == HROT) {
+                    const u64* src = P.in[1] + ((size_t)i << LOGN);
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) v2set(s, j, src[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
+                } else {
+                    s = ld2(sb + MAC_TILE);
+                }
+                if (D.mont) {
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) v2set(s, j, redc(v2get(s, j), 0, m));
+                }
             }
         }
         u64 a0l[2] = {0, 0}, a0h[2] = {0, 0}, a1l[2] = {0, 0}, a1h[2] = {0, 0};
@@ -778,11 +799,12 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
             mac_wide(a1l[0], a1h[0], dv.x, kav.x);
             mac_wide(a1l[1], a1h[1], dv.y, kav.y);
         }
+        const u32 use_redc = D.mont && (is_p || emr);
         ulonglong2 r0, r1;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            v2set(r0, j, acc_reduce(a0l[j], a0h[j], m, D.mont));
-            v2set(r1, j, acc_reduce(a1l[j], a1h[j], m, D.mont));
+            v2set(r0, j, acc_reduce(a0l[j], a0h[j], m, use_redc));
+            v2set(r1, j, acc_reduce(a1l[j], a1h[j], m, use_redc));
         }
         const u64 q = m.q;
         if (is_p) {
@@ -799,7 +821,7 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
             o1 = r1;
         } else {
             const bool drop = i == L - 1;
-            const u64 s1 = lv.s1[i], s1p = lv.s1p[i];
+            const u64 s1 = lv.s1r[i], s1p = lv.s1rp[i];
             d0 = drop ? slot_ptr(P, w.U, LOGN) : slot_ptr(P, w.W + i, LOGN);
             d1 = drop ? slot_ptr(P, w.U + 1, LOGN) : slot_ptr(P, w.W + L + i, LOGN);
 #pragma unroll
@@ -878,7 +900,8 @@ p7_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
     }
     if (P.mode != EMR) return;
     const ModC m = D.mod[l];
-    const u64 ni = D.ninv[l], nip = D.ninvp[l], pv = D.pinv[l], pvp = D.pinvp[l];
+    // U carries R^-1 from P5 with mont (Key): its n^-1 scale carries R
+    const u64 ni = D.ninvu[l], nip = D.ninvup[l], pv = D.pinv[l], pvp = D.pinvp[l];
     u64* U = slot_ptr(P, w.U + c, LOGN) + c0;
     const u64* XP = slot_ptr(P, w.RP + c * K, LOGN) + c0;
     auto ld = [&](int r, int cl) { return U[r * 256 + cl]; };
