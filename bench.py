@@ -225,6 +225,7 @@ def serving_trace(count, seed):
 
 def serve(G, ctxs, reqs, budget, plain):
     srv = G.Server(ctxs, budget, plain=plain)
+    tuned = srv.tune(512)                 # schedules per context and batch class, before the trace
     for i, (c, L, ops, t) in enumerate(reqs):
         srv.submit(c, L, ops, arrival_s=t, seed=SEED + i)
     srv.start()
@@ -244,7 +245,7 @@ def serve(G, ctxs, reqs, budget, plain):
         "steps": st["steps"], "ops": st["ops"], "evalmult_rescale_ops": st["emr_ops"],
         "completed": st["completed"], "peak_active": st["peak_active"], "max_batch": st["max_batch"],
         "peak_arena_bytes": st["peak_bytes"], "arena_bytes": st["arena_bytes"],
-        "resident_bytes": st["resident_bytes"],
+        "resident_bytes": st["resident_bytes"], "tuned_batch_shapes": tuned,
     }
 
 

@@ -183,6 +183,52 @@ uint64_t Server::submit(uint32_t ctx, uint32_t level, const std::vector<ReqOp>& 
     return id;
 }
 
+int Server::tune(uint32_t max_batch) {
+    ck(cudaSetDevice(device_), "cudaSetDevice");
+    if (!inflight_.empty() || !active_.empty())
+        throw std::invalid_argument("tune: the server must be idle");
+    int tuned = 0;
+    for (size_t c = 0; c < ctxs_.size(); ++c) {
+        const gfx::Context& ctx = *ctxs_[c];
+        cudaStream_t s = streams_[c];
+        // batches of EvalMult+Rescale over levels 2..fullQ, one per batch-size class
+        for (uint32_t nops = 1; nops <= max_batch; nops *= 2) {
+            std::vector<pl::Op> ops(nops);
+            std::vector<u64*> ws(nops);
+            std::vector<std::pair<size_t, size_t>> held;
+            bool fits = true;
+            for (uint32_t k = 0; k < nops && fits; ++k) {
+                const uint32_t L = 2 + (uint32_t)(((uint64_t)k * 7919u) % (ctx.fullQ() - 1));
+                const size_t bytes = request_bytes((uint32_t)c, L);
+                size_t off = 0;
+                if (!arena_->alloc(bytes, off)) { fits = false; break; }
+                held.push_back({off, bytes});
+                u64* base = arena_->base() + off / 8;
+                const size_t ctw = (size_t)L * ctx.n();
+                ck(cudaMemsetAsync(base, 0, 2 * ctw * 8, s), "tune inputs");
+                pl::Op& op = ops[k];
+                op.L = L;
+                op.mode = pl::EMR;
+                op.in[0] = op.in[2] = base;
+                op.in[1] = op.in[3] = base + ctw;
+                op.out[0] = base + 2 * ctw;
+                op.out[1] = base + 3 * ctw;
+                ws[k] = base + round_up(4 * ctw * 8) / 8;
+            }
+            if (fits && ctx.key(0)) {
+                pl::Plan& plan = *plans_[2 * c];
+                pl::build_plan_into(plan, ctx, ops, ws, s);
+                pl::tune(plan, s, true);
+                ck(cudaStreamSynchronize(s), "tune");
+                ++tuned;
+            }
+            for (auto& h : held) arena_->release(h.first, h.second);
+            if (!fits) break;
+        }
+    }
+    return tuned;
+}
+
 void Server::start() {
     cudaSetDevice(device_);
     ck(cudaEventRecord(epoch_ev_, streams_[0]), "cudaEventRecord");
@@ -434,6 +480,15 @@ int gpufhe_server_submit(gpufhe_server* h, uint32_t ctx, uint32_t level, const g
         for (uint32_t i = 0; i < nops; ++i) v[i] = {ops[i].mode, ops[i].galois};
         const uint64_t r = h->s->submit(ctx, level, v, arrival_s, seed, h_in, h_out);
         if (id) *id = r;
+        return GPUFHE_OK;
+    })
+}
+
+int gpufhe_server_tune(gpufhe_server* h, uint32_t max_batch, uint32_t* tuned) {
+    if (!h) return GPUFHE_EINVAL;
+    GPUFHE_TRY({
+        const int t = h->s->tune(max_batch ? max_batch : 256);
+        if (tuned) *tuned = (uint32_t)t;
         return GPUFHE_OK;
     })
 }

@@ -100,6 +100,12 @@ public:
     // Queues a request arriving arrival_s seconds after the epoch; returns its id.
     uint64_t submit(uint32_t ctx, uint32_t level, const std::vector<ReqOp>& ops, double arrival_s, uint64_t seed,
                     const u64* h_in, u64* h_out);
+    // Runs the autotuner for every context on EvalMult+Rescale batches of
+    // 1, 2, 4, ... max_batch operations (zero-filled buffers from the arena:
+    // timing does not depend on the residues), so that steps find their
+    // schedule in the cache; the server must be idle. Returns the number of
+    // batch shapes tuned.
+    int tune(uint32_t max_batch);
     // Resets the epoch to now (arrival times count from here).
     void start();
     // One scheduling step: retire completed steps, admit arrived requests,

@@ -67,6 +67,7 @@ _API: dict = {
     "gpufhe_server_request_bytes": (U64, [VP, U32, U32]),
     "gpufhe_server_submit": (I32, [VP, U32, U32, VP, U32, DBL, U64, VP, VP, C.POINTER(U64)]),
     "gpufhe_server_start": (I32, [VP]),
+    "gpufhe_server_tune": (I32, [VP, U32, C.POINTER(U32)]),
     "gpufhe_server_step": (I32, [VP, C.POINTER(U32)]),
     "gpufhe_server_drain": (I32, [VP, DBL]),
     "gpufhe_server_pending": (U64, [VP]),
@@ -280,6 +281,12 @@ class Server:
 
     def start(self):
         check(lib().gpufhe_server_start(self.h))
+
+    def tune(self, max_batch=256):
+        """Autotune every context's schedule on batches of 1..max_batch EvalMult+Rescale operations."""
+        t = U32()
+        check(lib().gpufhe_server_tune(self.h, max_batch, C.byref(t)))
+        return t.value
 
     def step(self):
         q = U32()

@@ -223,6 +223,11 @@ uint64_t gpufhe_server_request_bytes(gpufhe_server* srv, uint32_t ctx, uint32_t 
 int      gpufhe_server_submit(gpufhe_server* srv, uint32_t ctx, uint32_t level, const gpufhe_req_op* ops,
                               uint32_t nops, double arrival_s, uint64_t seed, const uint64_t* h_in, uint64_t* h_out,
                               uint64_t* id);
+/* Autotunes every context's launch schedule on EvalMult+Rescale batches of
+ * 1, 2, 4, ... max_batch (0 = 256) operations, on zero-filled arena buffers,
+ * so that serving steps (which only read the tuning cache) use measured
+ * schedules; call while the server is idle. *tuned = batch shapes tuned. */
+int      gpufhe_server_tune(gpufhe_server* srv, uint32_t max_batch, uint32_t* tuned);
 /* Sets the epoch to now. */
 int      gpufhe_server_start(gpufhe_server* srv);
 /* One scheduling step; *queued = operations queued (0 when idle). */

@@ -56,9 +56,11 @@ def final_level(r):
     return r["level"] - sum(1 for m, _ in r["ops"] if m == EMR)
 
 
-def run(G, gctxs, setups, reqs, plain=False, budget=None, seeded=False):
+def run(G, gctxs, setups, reqs, plain=False, budget=None, seeded=False, tune=0):
     resident = sum(g.resident_bytes() for g in gctxs)
     srv = G.Server(gctxs, budget or resident + (1 << 30), plain=plain)
+    if tune:
+        assert srv.tune(tune) > 0
     outs = []
     for i, r in enumerate(reqs):
         n = setups[r["ctx"]].n
@@ -143,3 +145,13 @@ def test_submit_errors(G, setups, gctxs):
     srv.close()
     with pytest.raises(G.GpuFheError):
         G.Server(gctxs, resident // 2)                  # budget below the resident tables
+
+
+def test_tuned_server_same_bits(G, setups, gctxs):
+    """Schedules picked by the server's autotuner give the same outputs."""
+    reqs = make_trace(setups, 10, seed=21)
+    base, _, _ = run(G, gctxs, setups, reqs)
+    tuned, st, _ = run(G, gctxs, setups, reqs, tune=16)
+    assert st["completed"] == len(reqs)
+    for i in range(len(reqs)):
+        assert np.array_equal(base[i], tuned[i]), i
