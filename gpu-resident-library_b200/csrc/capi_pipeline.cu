@@ -98,8 +98,9 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     if (!plan) return 0;
     uint32_t k = 0;
     const pl::Plan& p = *plan->p;
-    for (int i = 0; i < pl::NPHASE; ++i) {
-        if ((p.mix >> i & 1) && p.job_cnt[i][2]) k += 1;
+    for (int i = 0; i <= pl::NPHASE; ++i) {
+        const int bit = i == pl::NPHASE ? 6 : i;   // the second P7 launch follows phase 7's choice
+        if ((p.mix >> bit & 1) && p.job_cnt[i][2]) k += 1;
         else k += (p.job_cnt[i][0] ? 1 : 0) + (p.job_cnt[i][1] ? 1 : 0);
     }
     return k;

@@ -34,6 +34,8 @@ struct Variant {
         cudaFuncSetAttribute(p3_modup_fwd_col<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
         cudaFuncSetAttribute(p4_modup_fwd_row<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
         cudaFuncSetAttribute(p6_moddown_inv_row<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
+        cudaFuncSetAttribute(p7a_moddown_inv_col<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
+        cudaFuncSetAttribute(p7b_moddown_inv_col<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
         cudaFuncSetAttribute(p8_moddown_fwd_col<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
         cudaFuncSetAttribute(p9_final_fwd_row<LOGN, PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
     }
@@ -52,6 +54,8 @@ struct Variant {
             case 2: p3_modup_fwd_col<LOGN, PATH><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
             case 3: p4_modup_fwd_row<LOGN, PATH><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
             case 5: p6_moddown_inv_row<LOGN, PATH><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
+            case 6: p7a_moddown_inv_col<LOGN, PATH><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
+            case NPHASE: p7b_moddown_inv_col<LOGN, PATH><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
             case 7: p8_moddown_fwd_col<LOGN, PATH><<<cnt * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(D, pd, J); break;
             case 8: p9_final_fwd_row<LOGN, PATH><<<cnt * G::ROW_TILES, G::ROW_THREADS, G::ROW_SMEM, s>>>(D, pd, J); break;
             default: break;
@@ -72,7 +76,6 @@ struct Launcher {
             p3ws_attrs<0>();
             p3ws_attrs<1>();
             p3ws_attrs<2>();
-            cudaFuncSetAttribute(p7_moddown_inv_col<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
             done = true;
         }
         if (dnum > mac_dnum) {
@@ -128,10 +131,15 @@ struct Launcher {
                 else
                     p5_mac<LOGN, MAC_NT><<<grid, MAC_NT, mac_smem(D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
                                                                                p.d_plist);
-            } else if (k == 6) {
-                if (p.job_cnt[6][0])
-                    p7_moddown_inv_col<LOGN><<<p.job_cnt[6][0] * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(
-                        D, p.d_pairs, p.d_jobs + p.job_off[6][0]);
+            } else if (k == 6) {   // P7a then P7b (U and r_l need the P towers)
+                for (int kk : {6, (int)NPHASE}) {
+                    if ((p.mix >> 6 & 1) && p.job_cnt[kk][0] && p.job_cnt[kk][1]) {
+                        Variant<LOGN, 2>::phase(kk, p, s);
+                    } else {
+                        Variant<LOGN, 0>::phase(kk, p, s);
+                        Variant<LOGN, 1>::phase(kk, p, s);
+                    }
+                }
             } else if (k == 2 && p.p3_form) {
                 if ((p.mix >> 2 & 1) && p.job_cnt[2][0] && p.job_cnt[2][1]) p3ws<2>(p, s);
                 else { p3ws<0>(p, s); p3ws<1>(p, s); }
@@ -180,15 +188,15 @@ struct HostTables {
     std::vector<uint2> jobs;       // all phases, concatenated
     std::vector<uint4> mac_jobs;
     std::vector<uint32_t> plist;
-    size_t job_off[NPHASE][3] = {};     // [phase][integer, FP64, mixed]
-    uint32_t job_cnt[NPHASE][3] = {};
+    size_t job_off[NPHASE + 1][3] = {};     // [phase (+ the second P7 launch)][integer, FP64, mixed]
+    uint32_t job_cnt[NPHASE + 1][3] = {};
 };
 
 static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const std::vector<u64*>& ws_ptrs,
                         HostTables& T) {
     const uint32_t K = c.K();
     T.pairs.assign(ops.size(), PairDesc{});
-    std::vector<uint2> jobs[NPHASE];
+    std::vector<uint2> jobs[NPHASE + 1];   // index NPHASE: the second P7 launch (U and r_l)
     std::map<std::pair<uint64_t, uint32_t>, std::vector<uint32_t>> rows;
     std::map<std::pair<const u64*, uint32_t>, uint32_t> hoist_lead;   // (c1, level) -> first HROT op
     for (size_t pi = 0; pi < ops.size(); ++pi) {
@@ -240,7 +248,8 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
         const bool emr = op.mode == EMR;
         for (uint32_t cc = 0; cc < 2; ++cc) {
             for (uint32_t t = emr ? 0 : 1; t <= K; ++t) jobs[5].push_back({pu, cc * (K + 1) + t});
-            jobs[6].push_back({pu, cc});
+            for (uint32_t t = 1; t <= K; ++t) jobs[6].push_back({pu, cc * (K + 1) + t});
+            if (emr) jobs[NPHASE].push_back({pu, cc * (K + 1)});   // P7b: U of component cc
         }
         const uint32_t outL = emr ? L - 1 : L;
         for (uint32_t cc = 0; cc < 2; ++cc)
@@ -267,13 +276,13 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
         switch (k) {
             case 0: case 1: return j.y;
             case 2: case 3: return qp_of(j.y % (P.L + K), P.L, c.fullQ());
-            case 5: { const u32 t = j.y % (K + 1); return t == 0 ? P.L - 1 : c.fullQ() + t - 1; }
+            case 5: case 6: case NPHASE: { const u32 t = j.y % (K + 1); return t == 0 ? P.L - 1 : c.fullQ() + t - 1; }
             default: return j.y % P.L;   // 7, 8
         }
     };
     T.jobs.clear();
-    for (int k = 0; k < NPHASE; ++k) {
-        const bool split = k != 4 && k != 6;
+    for (int k = 0; k <= NPHASE; ++k) {
+        const bool split = k != 4;
         for (int v = 0; v < 2; ++v) {
             T.job_off[k][v] = T.jobs.size();
             for (const uint2& j : jobs[k]) {
@@ -346,7 +355,7 @@ static void commit(Plan& p, const HostTables& T, const std::vector<Op>& ops, cud
     p.d_jobs = reinterpret_cast<uint2*>(d + b_pairs);
     p.d_mac_jobs = reinterpret_cast<uint4*>(d + b_pairs + b_jobs);
     p.d_plist = reinterpret_cast<uint32_t*>(d + b_pairs + b_jobs + b_mac);
-    for (int k = 0; k < NPHASE; ++k)
+    for (int k = 0; k <= NPHASE; ++k)
         for (int v = 0; v < 3; ++v) { p.job_off[k][v] = T.job_off[k][v]; p.job_cnt[k][v] = T.job_cnt[k][v]; }
     p.nops = (uint32_t)ops.size();
     p.ops = ops;
@@ -494,8 +503,10 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         return (cur & ~field_mask) | values[win];
     };
     int cur = DEFAULT;
-    for (int k : {0, 1, 2, 3, 5, 7, 8}) {                          // interleaved or separate, per phase
-        if (!p.job_cnt[k][0] || !p.job_cnt[k][1]) continue;
+    for (int k : {0, 1, 2, 3, 5, 6, 7, 8}) {                       // interleaved or separate, per phase
+        const bool both = (p.job_cnt[k][0] && p.job_cnt[k][1]) ||
+                          (k == 6 && p.job_cnt[NPHASE][0] && p.job_cnt[NPHASE][1]);
+        if (!both) continue;
         const int bit = 1 << (8 + k);
         cur = pick(1u << k, bit, {bit, 0}, cur);
     }

@@ -27,7 +27,7 @@
 //                              one CTA keeps a key-row tile of every digit in
 //                              shared memory and streams all pairs using it -> W / U / RP
 //   P6 inv-row  (pair,c,t)     INTT row stages of U (dropped tower) and RP   -> U / RP
-//   P7 inv-col  (pair,c)       INTT columns of RP then U, scaled; r_l        -> RP / U
+//   P7 inv-col  (pair,c,t)     INTT columns of RP, scaled; then (pair,c) U and r_l -> RP / U
 //   P8 fwd-col  (pair,c,i)     ModDown conversion + SwitchModulus prologue   -> Z
 //   P9 fwd-row  (pair,c,i)     NTT row stages, final combine                -> out
 #pragma once
@@ -859,7 +859,7 @@ __device__ __forceinline__ void p6_moddown_inv_row_body(const DevCtx& D, const P
         [&](int rl, int cc, u64 v) { sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)] = ar.stage_in(v); });
     __syncthreads();
     auto st = [&](int rl, int cc, u64 v) { X[rl * 256 + cc] = v; };
-    ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8>(sm, twi_of<FP>(D, qp, LOGN), R0, ar, st);
+    ntt::inv_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 8, true>(sm, twi_of<FP>(D, qp, LOGN), R0, ar, st);
 }
 
 template <int LOGN, int PATH>
@@ -871,37 +871,57 @@ p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
 }
 
 // ------------------------------------------------------------------ P7
-// One CTA per (pair, component, column tile): INTT columns of the K P towers
-// (scaled by n^-1 * PHatInv), then of U[c] (scaled by n^-1) followed by
-// r_l = u - conv'_l * P^-1 mod q_l, written back into U[c]. The thread that
-// stores an element of each P tower is the one that reads it back for r_l.
-template <int LOGN>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
-p7_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+// Two launches. P7a (pair, c, t >= 1): INTT columns of P tower t-1 of RP[c],
+// scaled by n^-1 * PHatInv. P7b (pair, c), EvalMult+Rescale only, after P7a:
+// INTT columns of U[c] scaled by n^-1 (times R: U carries R^-1 from P5, see
+// Key), then r_l = u - conv'_l * P^-1 mod q_l into U[c], with the P->q_l
+// constants folding P^-1 (and 2^64 for a Montgomery reduction when
+// D.mont_down). Both read P6's output in the path's own word format.
+template <int LOGN, bool FP>
+__device__ __forceinline__ void p7a_moddown_inv_col_body(const DevCtx& D, const PairDesc* __restrict__ pairs,
+                                                         const uint2 jb, const u32 tile) {
+    using G = ntt::Geo<LOGN>;
+    extern __shared__ __align__(16) u64 sm[];
+    const int c0 = tile * G::C;
+    const PairDesc& P = pairs[jb.x];
+    const u32 L = P.L, K = D.K;
+    const u32 c = jb.y / (K + 1), t = jb.y % (K + 1);
+    const WsLayout w = ws_layout(L, K, D.alpha);
+    const u32 qp = D.fullQ + t - 1;
+    const ModC m = D.mod[qp];
+    const u64 sc = D.pdn[t - 1], scp = D.pdnp[t - 1];
+    u64* X = slot_ptr(P, w.RP + c * K + (t - 1), LOGN) + c0;
+    auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
+    auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
+    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, twi_of<FP>(D, qp, LOGN), ar_of<FP>(m), ld, st);
+}
+
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
+p7a_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p7a_moddown_inv_col_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
+}
+
+template <int LOGN, bool FP>
+__device__ __forceinline__ void p7b_moddown_inv_col_body(const DevCtx& D, const PairDesc* __restrict__ pairs,
+                                                         const uint2 jb, const u32 tile) {
     using G = ntt::Geo<LOGN>;
     extern __shared__ __align__(16) u64 sm[];
     __shared__ u64 cl_[gfx::MAXP];
-    const uint2 jb = jobs[blockIdx.x / G::COL_TILES];
-    const int c0 = (blockIdx.x % G::COL_TILES) * G::C;
+    const int c0 = tile * G::C;
     const PairDesc& P = pairs[jb.x];
-    const u32 L = P.L, K = D.K, c = jb.y, l = L - 1;
+    const u32 L = P.L, K = D.K, c = jb.y / (K + 1), l = L - 1;
     const WsLayout w = ws_layout(L, K, D.alpha);
-    if (threadIdx.x < K) cl_[threadIdx.x] = D.phatmodq[threadIdx.x * D.fullQ + l];
-    for (u32 t = 1; t <= K; ++t) {
-        const u32 qp = D.fullQ + t - 1;
-        const ModC m = D.mod[qp];
-        const u64 sc = D.pdn[t - 1], scp = D.pdnp[t - 1];
-        u64* X = slot_ptr(P, w.RP + c * K + (t - 1), LOGN) + c0;
-        auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
-        auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
-        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)qp << LOGN)},
-                                                              ntt::IntAr{m.q, m.two_q}, ld, st);
-        __syncthreads();
-    }
-    if (P.mode != EMR) return;
     const ModC m = D.mod[l];
-    // U carries R^-1 from P5 with mont (Key): its n^-1 scale carries R
-    const u64 ni = D.ninvu[l], nip = D.ninvup[l], pv = D.pinv[l], pvp = D.pinvp[l];
+    if (threadIdx.x < K) {   // PHatModq[j][l] * P^-1 (* 2^64 with mont_down)
+        u64 v = mulmod(D.phatmodq[threadIdx.x * D.fullQ + l], D.pinv[l], m);
+        if (D.mont_down) v = mulmod(v, r_mod(m), m);
+        cl_[threadIdx.x] = v;
+    }
+    __syncthreads();
+    const u64 ni = D.ninvu[l], nip = D.ninvup[l];
     u64* U = slot_ptr(P, w.U + c, LOGN) + c0;
     const u64* XP = slot_ptr(P, w.RP + c * K, LOGN) + c0;
     auto ld = [&](int r, int cl) { return U[r * 256 + cl]; };
@@ -910,11 +930,18 @@ p7_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uin
         const u64 u = shoup(v, ni, nip, m.q);
         u64 lo = 0, hi = 0;
         for (u32 j = 0; j < K; ++j) mac_wide(lo, hi, XP[((size_t)j << LOGN) + e], cl_[j]);
-        const u64 tmp = shoup(barrett_lazy(lo, hi, m.q, m.mu_lo, m.mu_hi), pv, pvp, m.q);
+        const u64 tmp = D.mont_down ? redc(lo, hi, m) : barrett(lo, hi, m);
         U[e] = u >= tmp ? u - tmp : u + m.q - tmp;
     };
-    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A>(sm, ntt::TwPacked{D.twi + ((size_t)l << LOGN)},
-                                                          ntt::IntAr{m.q, m.two_q}, ld, st);
+    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, twi_of<FP>(D, l, LOGN), ar_of<FP>(m), ld, st);
+}
+
+template <int LOGN, int PATH>
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
+p7b_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
+    uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
+    const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
+    on_path<PATH>(jb, [&](auto fp) { p7b_moddown_inv_col_body<LOGN, decltype(fp)::value>(D, pairs, jb, tile); });
 }
 
 // ------------------------------------------------------------------ P8

@@ -26,8 +26,9 @@ struct Plan {
     uint32_t logn = 0, nops = 0;
     PairDesc* d_pairs = nullptr;
     uint2* d_jobs = nullptr;
-    size_t job_off[NPHASE][3] = {};    // [phase][integer jobs, FP64 jobs, both interleaved]
-    uint32_t job_cnt[NPHASE][3] = {};
+    // [phase (index NPHASE: the second P7 launch)][integer jobs, FP64 jobs, both interleaved]
+    size_t job_off[NPHASE + 1][3] = {};
+    uint32_t job_cnt[NPHASE + 1][3] = {};
     uint4* d_mac_jobs = nullptr;
     uint32_t* d_plist = nullptr;
     u64* ws = nullptr;
