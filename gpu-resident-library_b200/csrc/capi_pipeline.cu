@@ -106,8 +106,8 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     return k;
 }
 
-int gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
-                            cudaStream_t s) {
+int gpufhe_plan_launch_host_async(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
+                                  cudaStream_t s) {
     if (!plan || !h_in || !h_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
     const pl::Plan& p = *plan->p;
     const size_t n = (size_t)1 << p.logn;
@@ -133,7 +133,14 @@ int gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint
             if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
         }
     }
-    e = cudaStreamSynchronize(s);
+    return GPUFHE_OK;
+}
+
+int gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
+                            cudaStream_t s) {
+    const int rc = gpufhe_plan_launch_host_async(plan, h_in, h_out, s);
+    if (rc) return rc;
+    const cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
     return GPUFHE_OK;
 }

@@ -57,6 +57,7 @@ _API: dict = {
     "gpufhe_plan_schedule": (U32, [VP]),
     "gpufhe_plan_set_schedule": (I32, [VP, U32]),
     "gpufhe_plan_launch_host": (I32, [VP, VP, VP, VP]),
+    "gpufhe_plan_launch_host_async": (I32, [VP, VP, VP, VP]),
     "gpufhe_native_primes": (I32, [VP, U32, U32, U32, VP, U32]),
     "gpufhe_native_root": (U64, [U32, U64]),
     "gpufhe_rescale_consts": (I32, [VP, VP, VP, U32]),
@@ -213,11 +214,13 @@ class Plan:
         mixed = [k + 1 for k in range(9) if b >> (8 + k) & 1]
         return {"p5": form, "mixed_paths": bool(b & 4), "mixed_phases": mixed, "p3": p3, "tuned": bool(b & 32)}
 
-    def launch_host(self, h_in, h_out, stream=None):
-        """h_in: list of 4 host pointers per op (0 for unused); h_out: 2 per op."""
+    def launch_host(self, h_in, h_out, stream=None, sync=True):
+        """h_in: list of 4 host pointers per op (0 for unused); h_out: 2 per op.
+        sync=False queues the copies and kernels only (pinned host buffers)."""
         ai = (VP * len(h_in))(*h_in)
         ao = (VP * len(h_out))(*h_out)
-        check(lib().gpufhe_plan_launch_host(self.h, ai, ao, stream))
+        f = lib().gpufhe_plan_launch_host if sync else lib().gpufhe_plan_launch_host_async
+        check(f(self.h, ai, ao, stream))
 
     def close(self):
         if getattr(self, "h", None):

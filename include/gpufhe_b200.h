@@ -150,6 +150,13 @@ int      gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule);
  * memory gives full PCIe bandwidth. */
 int  gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
                              cudaStream_t stream);
+/* The same without the final synchronisation: copies and kernels are queued
+ * on `stream`. Host buffers must be pinned and left untouched until the
+ * stream reaches this point; two plans over separate device buffers on two
+ * streams let one batch's host->device copies overlap another's transform
+ * and device->host copies. */
+int  gpufhe_plan_launch_host_async(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
+                                   cudaStream_t stream);
 /* create + launch + synchronize + destroy */
 int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaStream_t stream);
 
