@@ -167,3 +167,31 @@ def test_every_schedule_same_bits(G, S, gctx, schedule):
     assert got["p3"] == ("plain", "warp-specialised-128x2", "warp-specialised-256x1")[schedule >> 3]
     for outs, (e0, e1) in want:
         assert np.array_equal(host(outs[0]), e0) and np.array_equal(host(outs[1]), e1)
+
+
+def test_launch_host_sync_and_async(G, S, gctx):
+    """Host-buffer entry points: inputs copied in, the batch, outputs copied
+    out; the async form on pinned buffers after a stream synchronisation."""
+    import torch
+    rng = np.random.default_rng(77)
+    n, levels = S.n, [5, 9]
+    specs, keep, h_in, want, pins = [], [], [], [], []
+    for L in levels:
+        cts = [*S.rand_ct(rng, L), *S.rand_ct(rng, L)]
+        ins = [empty(L * n) for _ in range(4)]
+        outs = [empty((L - 1) * n), empty((L - 1) * n)]
+        keep += ins + outs
+        specs.append(dict(level=L, inp=[ptr(x) for x in ins], out=[ptr(x) for x in outs]))
+        for c in cts:
+            t = torch.from_numpy(c.view(np.int64).copy()).pin_memory()
+            pins.append(t)
+            h_in.append(t.data_ptr())
+        want.append(S.octx.evalmult_rescale(L, *cts))
+    plan = G.Plan(gctx, specs)
+    for sync in (True, False):
+        outs_h = [torch.zeros((L - 1) * n, dtype=torch.int64).pin_memory() for L in levels for _ in range(2)]
+        plan.launch_host(h_in, [t.data_ptr() for t in outs_h], None, sync=sync)
+        torch.cuda.synchronize()
+        for j, (e0, e1) in enumerate(want):
+            assert np.array_equal(outs_h[2 * j].numpy().view(np.uint64), e0), (sync, j)
+            assert np.array_equal(outs_h[2 * j + 1].numpy().view(np.uint64), e1), (sync, j)
