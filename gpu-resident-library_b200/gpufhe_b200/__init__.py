@@ -62,6 +62,7 @@ _API: dict = {
     "gpufhe_native_root": (U64, [U32, U64]),
     "gpufhe_rescale_consts": (I32, [VP, VP, VP, U32]),
     "gpufhe_rescale_noalloc": (I32, [VP, U32, VP, VP]),
+    "gpufhe_lintrans_bsgs": (I32, [VP, U32, VP, VP, U32, U32, VP, I32, VP, VP, VP]),
     "gpufhe_rescale_noalloc_max_words": (U64, []),
     "gpufhe_server_create": (I32, [VP, U32, U64, U32, U32, I32, C.POINTER(VP)]),
     "gpufhe_server_destroy": (None, [VP]),
@@ -325,6 +326,13 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def lintrans_bsgs(ctx, level, c0, c1, n1, n2, diags, out0, out1, hoisted=False, stream=None):
+    """Baby-step giant-step linear transform; diags: n1*n2 device pointers (or None), index g*n1+b."""
+    arr = (VP * len(diags))(*[d if d else None for d in diags])
+    check(lib().gpufhe_lintrans_bsgs(ctx.h, level, c0, c1, n1, n2, C.cast(arr, VP), 1 if hoisted else 0,
+                                     out0, out1, stream))
 
 
 def run_ops(ctx, specs, stream=None):

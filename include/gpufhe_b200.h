@@ -160,6 +160,24 @@ int  gpufhe_plan_launch_host_async(gpufhe_plan* plan, const uint64_t* const* h_i
 /* create + launch + synchronize + destroy */
 int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- linear transform
+ * Baby-step giant-step homomorphic linear transform of the ciphertext
+ * (d_c0, d_c1) at `level` (eval form, [level][n] each):
+ *   y = sum_{g<n2} rot_{g*n1}( sum_{b<n1} diag[g*n1+b] (.) rot_b(x) ),
+ * the sequence of the reference's tests/test_c2s_bsgs.cpp:129-151
+ * (rotate_ct per step, ct_mul_pt + ct_add_ct for the inner sums). diag: host
+ * array of n1*n2 device pointers to eval-form plaintext diagonals ([level][n])
+ * or NULL for a zero diagonal. Rotation by r slots uses Galois element
+ * 5^r mod 2n and needs the key stored under that element (baby steps
+ * r = 1..n1-1, giant steps r = g*n1). hoisted != 0 computes the baby
+ * rotations with one shared ModUp (GPUFHE_ROTATE_HOISTED; different bits from
+ * the reference's per-rotation ModUp). Allocates scratch, runs the baby
+ * rotations, the inner sums, the giant rotations and the final sum as four
+ * batched launches on `stream`, and synchronises it. */
+int gpufhe_lintrans_bsgs(gpufhe_ctx* ctx, uint32_t level, const uint64_t* d_c0, const uint64_t* d_c1, uint32_t n1,
+                         uint32_t n2, const uint64_t* const* diag, int hoisted, uint64_t* d_out0, uint64_t* d_out1,
+                         cudaStream_t stream);
+
 /* ---------------------------------------------------------------- no allocation
  * No counterpart in the reference. Rescale of one eval-form component
  * d_comp ([level][n], in place: the first level-1 towers receive the result)

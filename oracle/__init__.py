@@ -58,6 +58,7 @@ def lib():
             "orc_automorph": (None, [u64p, u64p, U32, U64, U64]),
             "orc_add_into": (None, [u64p, u64p, U64, U32]),
             "orc_ptmulacc": (None, [u64p, u64p, u64p, u64p, u64p, U64, U32]),
+            "orc_lintrans_bsgs": (None, [VP, U32, U32, U32, u64p, u64p, VP, I32, u64p, u64p]),
             "orc_ks_constants_size": (U64, [U32, U32, U32]),
             "orc_ks_constants": (None, [u64p, u64p, U32, u64p, U32, U32]),
             "orc_ctx_create": (VP, [U32, u64p, U32, u64p, U32, U32, VP]),
@@ -244,6 +245,14 @@ class Ctx:
         a, b = _u64(c0).copy(), _u64(c1).copy()
         lib().orc_rotate(self.h, key_id, L, k, a, b)
         return a, b
+
+    def lintrans_bsgs(self, L, n1, n2, c0, c1, diags, hoisted=False):
+        """diags: list of n2*n1 arrays ([L*n] eval form) or None, index g*n1+b."""
+        keep = [None if d is None else _u64(d) for d in diags]
+        arr = (C.c_void_p * len(keep))(*[None if d is None else d.ctypes.data for d in keep])
+        o0, o1 = np.zeros(L * self.n, np.uint64), np.zeros(L * self.n, np.uint64)
+        lib().orc_lintrans_bsgs(self.h, L, n1, n2, _u64(c0), _u64(c1), arr, 1 if hoisted else 0, o0, o1)
+        return o0, o1
 
     def rotate_hoisted(self, L, ks, key_ids, c0, c1):
         nr = len(ks)

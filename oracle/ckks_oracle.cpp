@@ -854,6 +854,49 @@ void orc_rotate_hoisted(const OrcCtx* c, uint32_t L, uint32_t nrot, const uint32
     }
 }
 
+void orc_lintrans_bsgs(const OrcCtx* c, uint32_t L, uint32_t n1, uint32_t n2, const u64* c0, const u64* c1,
+                       const u64* const* diag, int hoisted, u64* out0, u64* out1) {
+    /* Baby-step giant-step linear transform, the sequence of the reference's
+     * tests/test_c2s_bsgs.cpp:129-151: baby rotations rot_b(x), b < n1 (rot_0 = x);
+     * for every giant step g < n2: in_g = sum_b diag[g*n1+b] (.) rot_b(x)
+     * (ct_mul_pt_host then ct_add_ct_host, ptops.cpp:13-26), in_g rotated by
+     * g*n1 slots when g > 0 (rotate_ct_host), accumulated. Rotation by r slots
+     * uses Galois element 5^r mod 2n and the key stored under that element.
+     * hoisted != 0: the baby rotations share one ModUp (orc_rotate_hoisted). */
+    const uint32_t n = c->n, M = 2 * n;
+    const size_t T = (size_t)L * n;
+    auto gal = [&](uint32_t r) { u64 k = 1; for (uint32_t t = 0; t < r; ++t) k = (k * 5) % M; return (uint32_t)k; };
+    std::vector<vec> B0(n1, vec(c0, c0 + T)), B1(n1, vec(c1, c1 + T));
+    if (n1 > 1) {
+        if (hoisted) {
+            std::vector<uint32_t> ks(n1 - 1);
+            std::vector<u64*> o0(n1 - 1), o1(n1 - 1);
+            for (uint32_t b = 1; b < n1; ++b) { ks[b - 1] = gal(b); o0[b - 1] = B0[b].data(); o1[b - 1] = B1[b].data(); }
+            orc_rotate_hoisted(c, L, n1 - 1, ks.data(), ks.data(), c0, c1, o0.data(), o1.data());
+        } else {
+            for (uint32_t b = 1; b < n1; ++b) orc_rotate(c, gal(b), L, gal(b), B0[b].data(), B1[b].data());
+        }
+    }
+    vec acc0(T, 0), acc1(T, 0);
+    for (uint32_t g = 0; g < n2; ++g) {
+        vec in0(T, 0), in1(T, 0);
+        for (uint32_t b = 0; b < n1; ++b) {
+            const u64* d = diag[(size_t)g * n1 + b];
+            if (!d) continue;
+            for (uint32_t t = 0; t < L; ++t)
+                orc_ptmulacc(in0.data() + (size_t)t * n, in1.data() + (size_t)t * n, B0[b].data() + (size_t)t * n,
+                             B1[b].data() + (size_t)t * n, d + (size_t)t * n, c->Q[t], n);
+        }
+        if (g > 0) orc_rotate(c, gal(g * n1), L, gal(g * n1), in0.data(), in1.data());
+        for (uint32_t t = 0; t < L; ++t) {
+            orc_add_into(acc0.data() + (size_t)t * n, in0.data() + (size_t)t * n, c->Q[t], n);
+            orc_add_into(acc1.data() + (size_t)t * n, in1.data() + (size_t)t * n, c->Q[t], n);
+        }
+    }
+    std::memcpy(out0, acc0.data(), T * 8);
+    std::memcpy(out1, acc1.data(), T * 8);
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

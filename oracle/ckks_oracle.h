@@ -118,6 +118,8 @@ void orc_automorph_eval(const OrcCtx* c, uint32_t towers, uint32_t k, uint64_t* 
 /* rotate_ct_host: automorph c0,c1; keyswitch c1 with key_id; c0 += ba0; c1 = ba1 */
 void orc_rotate(const OrcCtx* c, uint32_t key_id, uint32_t L, uint32_t k, uint64_t* c0, uint64_t* c1);
 /* hoisted: one ModUp of c1 shared by nrot rotations (automorph the digits). */
+void orc_lintrans_bsgs(const OrcCtx* c, uint32_t L, uint32_t n1, uint32_t n2, const uint64_t* c0, const uint64_t* c1,
+                       const uint64_t* const* diag, int hoisted, uint64_t* out0, uint64_t* out1);
 void orc_rotate_hoisted(const OrcCtx* c, uint32_t L, uint32_t nrot, const uint32_t* ks,
                         const uint32_t* key_ids, const uint64_t* c0, const uint64_t* c1,
                         uint64_t* const* out0, uint64_t* const* out1);
