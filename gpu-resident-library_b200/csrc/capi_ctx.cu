@@ -48,6 +48,8 @@ __global__ void __launch_bounds__(MUL_NT) k_rns_mult_batch(const u64* __restrict
 #define GPUFHE_TRY(...)                                          \
     try { __VA_ARGS__ } catch (const std::invalid_argument& e) {        \
         gfx::set_error(e.what()); return GPUFHE_EINVAL;          \
+    } catch (const std::length_error& e) {                       \
+        gfx::set_error(e.what()); return GPUFHE_ENOMEM;          \
     } catch (const std::exception& e) {                          \
         gfx::set_error(e.what()); return GPUFHE_ECUDA;           \
     }
@@ -96,6 +98,26 @@ int gpufhe_ctx_set_key(gpufhe_ctx* h, uint64_t key_id, const uint64_t* av, const
 }
 
 uint64_t gpufhe_ctx_resident_bytes(const gpufhe_ctx* h) { return h ? h->c->resident_bytes() : 0; }
+
+int gpufhe_ctx_set_key_budget(gpufhe_ctx* h, uint64_t bytes) {
+    if (!h) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    GPUFHE_TRY({
+        h->c->set_key_budget(bytes);
+        return GPUFHE_OK;
+    })
+}
+
+int gpufhe_ctx_key_stats(const gpufhe_ctx* h, uint64_t* out) {
+    if (!h || !out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    const auto st = h->c->key_stats();
+    out[0] = st.known;
+    out[1] = st.resident;
+    out[2] = st.resident_bytes;
+    out[3] = st.uploads;
+    out[4] = st.evictions;
+    out[5] = st.budget;
+    return GPUFHE_OK;
+}
 
 int gpufhe_ntt_batch(gpufhe_ctx* h, uint64_t* d_data, uint32_t npolys, uint32_t towers, uint32_t first_tower,
                      int inverse, uint64_t* d_jobs, cudaStream_t s) {

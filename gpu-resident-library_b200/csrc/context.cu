@@ -225,7 +225,10 @@ Context::~Context() {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device_);
-    for (auto& kv : keys_) { cudaFree(kv.second.av); cudaFree(kv.second.bv); }
+    for (auto& kv : keys_) {
+        if (kv.second.dev.av) { cudaFree(kv.second.dev.av); cudaFree(kv.second.dev.bv); }
+        if (kv.second.host_av) { cudaFreeHost(kv.second.host_av); cudaFreeHost(kv.second.host_bv); }
+    }
     for (void* p : allocs_) cudaFree(p);
     cudaSetDevice(prev);
 }
@@ -254,6 +257,9 @@ cudaError_t scale_key_rows(u64* key, const ModC* mod, const u64* scale, uint32_t
 void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
     std::lock_guard<std::mutex> g(mu_);
     const size_t words = (size_t)dnum_ * (fullQ() + K()) * n_;
+    auto it0 = keys_.find(id);
+    if (it0 != keys_.end() && it0->second.pins) throw std::invalid_argument("set_key: key is in use by a plan");
+    if (key_budget_) evict_for(one_key_bytes(), id);
     Key k;
     auto up = [&](const u64* h) {
         u64* d = nullptr;
@@ -274,8 +280,106 @@ void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
         }
     }
     auto it = keys_.find(id);
-    if (it != keys_.end()) { cudaFree(it->second.av); cudaFree(it->second.bv); }
-    keys_[id] = k;
+    if (it != keys_.end()) {
+        KeySlot& old = it->second;
+        if (old.dev.av) { cudaFree(old.dev.av); cudaFree(old.dev.bv); key_dev_bytes_ -= one_key_bytes(); }
+        if (old.host_av) { cudaFreeHost(old.host_av); cudaFreeHost(old.host_bv); }
+        keys_.erase(it);
+    }
+    KeySlot& slot = keys_[id];
+    slot.dev = k;
+    slot.last_use = ++key_tick_;
+    key_dev_bytes_ += one_key_bytes();
+    if (key_budget_) host_copy(slot);
+}
+
+void Context::host_copy(KeySlot& k) const {
+    if (k.host_av || !k.dev.av) return;
+    const size_t bytes = one_key_bytes() / 2;
+    if (cudaMallocHost(&k.host_av, bytes) != cudaSuccess || cudaMallocHost(&k.host_bv, bytes) != cudaSuccess) {
+        if (k.host_av) cudaFreeHost(k.host_av);
+        k.host_av = k.host_bv = nullptr;
+        throw std::runtime_error("key host copy: pinned allocation failed");
+    }
+    if (cudaMemcpy(k.host_av, k.dev.av, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(k.host_bv, k.dev.bv, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("key host copy failed");
+}
+
+void Context::evict_for(size_t need, uint64_t keep) const {
+    if (!key_budget_) return;
+    while (key_dev_bytes_ + need > key_budget_) {
+        KeySlot* victim = nullptr;
+        for (auto& kv : keys_) {
+            KeySlot& k = kv.second;
+            if (kv.first == keep || !k.dev.av || k.pins) continue;
+            if (!victim || k.last_use < victim->last_use) victim = &k;
+        }
+        if (!victim) return;                       // everything resident is pinned
+        host_copy(*victim);
+        cudaFree(victim->dev.av);
+        cudaFree(victim->dev.bv);
+        victim->dev = Key{};
+        key_dev_bytes_ -= one_key_bytes();
+        ++key_evictions_;
+    }
+}
+
+void Context::set_key_budget(size_t bytes) {
+    std::lock_guard<std::mutex> g(mu_);
+    if (bytes && bytes < one_key_bytes()) throw std::invalid_argument("key budget below one key");
+    key_budget_ = bytes;
+    if (!bytes) return;
+    for (auto& kv : keys_) host_copy(kv.second);
+    evict_for(0, ~0ull);
+}
+
+const Key* Context::acquire(uint64_t id) const {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = keys_.find(id);
+    if (it == keys_.end()) return nullptr;
+    KeySlot& k = it->second;
+    if (!k.dev.av) {
+        evict_for(one_key_bytes(), id);
+        if (key_budget_ && key_dev_bytes_ + one_key_bytes() > key_budget_)
+            throw std::length_error("key budget too small for the keys one batch needs at once");
+        const size_t bytes = one_key_bytes() / 2;
+        Key d;
+        if (cudaMalloc(&d.av, bytes) != cudaSuccess || cudaMalloc(&d.bv, bytes) != cudaSuccess) {
+            if (d.av) cudaFree(d.av);
+            throw std::length_error("key upload: cudaMalloc failed");
+        }
+        if (cudaMemcpy(d.av, k.host_av, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(d.bv, k.host_bv, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(d.av);
+            cudaFree(d.bv);
+            throw std::runtime_error("key upload failed");
+        }
+        k.dev = d;
+        key_dev_bytes_ += one_key_bytes();
+        ++key_uploads_;
+    }
+    ++k.pins;
+    k.last_use = ++key_tick_;
+    return &k.dev;
+}
+
+void Context::release(uint64_t id) const {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = keys_.find(id);
+    if (it != keys_.end() && it->second.pins) --it->second.pins;
+}
+
+Context::KeyStats Context::key_stats() const {
+    std::lock_guard<std::mutex> g(mu_);
+    KeyStats s{};
+    s.known = keys_.size();
+    for (auto& kv : keys_) s.resident += kv.second.dev.av != nullptr;
+    s.resident_bytes = key_dev_bytes_;
+    s.uploads = key_uploads_;
+    s.evictions = key_evictions_;
+    s.budget = key_budget_;
+    return s;
 }
 
 bool Context::tuned_choice(uint64_t key, int& choice) const {
@@ -294,12 +398,12 @@ void Context::set_tuned_choice(uint64_t key, int choice) const {
 const Key* Context::key(uint64_t id) const {
     std::lock_guard<std::mutex> g(mu_);
     auto it = keys_.find(id);
-    return it == keys_.end() ? nullptr : &it->second;
+    return it == keys_.end() ? nullptr : &it->second.dev;
 }
 
 size_t Context::key_bytes() const {
     std::lock_guard<std::mutex> g(mu_);
-    return keys_.size() * 2 * (size_t)dnum_ * (fullQ() + K()) * n_ * 8;
+    return key_dev_bytes_;
 }
 
 }  // namespace gfx

@@ -96,9 +96,23 @@ public:
     // Upload a key (host [dnum][fullQ+K][n] canonical). id 0 = relinearisation;
     // rotation keys are stored under their Galois element.
     void set_key(uint64_t id, const u64* av, const u64* bv);
+    // The key stored under `id` (its device pointers are null while it is
+    // evicted), or nullptr for an unknown id.
     const Key* key(uint64_t id) const;
-    size_t key_bytes() const;
+    size_t key_bytes() const;              // device bytes of the resident keys
     size_t resident_bytes() const { return table_bytes_ + key_bytes(); }
+
+    // Key residency. With a budget (bytes, 0 = unlimited) every key keeps a
+    // pinned host copy of its stored form and at most `budget` bytes of keys
+    // stay on the device; acquire() makes a key resident (uploading it and
+    // evicting least recently used unpinned keys) and pins it until release().
+    // A batch that needs more pinned keys than the budget holds throws
+    // std::length_error.
+    void set_key_budget(size_t bytes);
+    const Key* acquire(uint64_t id) const;
+    void release(uint64_t id) const;
+    struct KeyStats { uint64_t known, resident, resident_bytes, uploads, evictions, budget; };
+    KeyStats key_stats() const;
 
     // Autotuner cache: launch-schedule choice per batch shape key.
     bool tuned_choice(uint64_t key, int& choice) const;
@@ -113,7 +127,20 @@ private:
     DevCtx dc_{};
     std::vector<void*> allocs_;
     size_t table_bytes_ = 0;
-    std::map<uint64_t, Key> keys_;
+    struct KeySlot {
+        Key dev;                       // device copy (null while evicted)
+        u64* host_av = nullptr;        // pinned host copy of the stored form (with a budget)
+        u64* host_bv = nullptr;
+        uint64_t last_use = 0;
+        uint32_t pins = 0;
+    };
+    mutable std::map<uint64_t, KeySlot> keys_;
+    size_t key_budget_ = 0;
+    mutable size_t key_dev_bytes_ = 0;
+    mutable uint64_t key_tick_ = 0, key_uploads_ = 0, key_evictions_ = 0;
+    size_t one_key_bytes() const { return 2 * (size_t)dnum_ * (fullQ() + K()) * n_ * 8; }
+    void host_copy(KeySlot& k) const;              // device -> pinned host (caller holds mu_)
+    void evict_for(size_t need, uint64_t keep) const;   // caller holds mu_
     mutable std::map<uint64_t, int> tune_;
     mutable std::mutex mu_;
     void* dalloc(size_t bytes);

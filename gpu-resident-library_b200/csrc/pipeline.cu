@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <set>
 #include <stdexcept>
 
 namespace pl {
@@ -222,6 +223,7 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
         if (op.mode != RESCALE) {
             const gfx::Key* key = c.key(op.key_id);
             if (!key) throw std::invalid_argument("missing eval key");
+            if (!key->av) throw std::logic_error("eval key not resident (not pinned by the plan)");
             P.kav = key->av;
             P.kbv = key->bv;
         }
@@ -313,6 +315,8 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
 Plan::Plan() : staging(std::make_unique<HostTables>()) {}
 
 Plan::~Plan() {
+    if (ctx)
+        for (uint64_t id : key_pins) ctx->release(id);
     if (d_blob) cudaFree(d_blob);
     if (h_blob) cudaFreeHost(h_blob);
     if (own_ws && ws) cudaFree(ws);
@@ -362,6 +366,28 @@ static void commit(Plan& p, const HostTables& T, const std::vector<Op>& ops, cud
     p.pairs_host = T.pairs;
 }
 
+// Makes every key the batch uses resident and pinned for the plan's lifetime
+// (releasing the keys of the plan's previous batch).
+static void pin_keys(Plan& p, const gfx::Context& c, const std::vector<Op>& ops) {
+    std::set<uint64_t> ids;
+    for (const Op& op : ops)
+        if (op.mode != RESCALE) ids.insert(op.key_id);
+    if (p.ctx)
+        for (uint64_t id : p.key_pins) p.ctx->release(id);
+    p.key_pins.clear();
+    p.ctx = &c;
+    try {
+        for (uint64_t id : ids) {
+            if (!c.acquire(id)) throw std::invalid_argument("missing eval key");
+            p.key_pins.push_back(id);
+        }
+    } catch (...) {
+        for (uint64_t id : p.key_pins) c.release(id);
+        p.key_pins.clear();
+        throw;
+    }
+}
+
 std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words) {
     if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
     auto plan = std::make_unique<Plan>();
@@ -381,6 +407,7 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
         throw std::invalid_argument("workspace must be 16-byte aligned");
     }
     plan->ws_words = need;
+    pin_keys(*plan, c, ops);
     std::vector<u64*> wsp(ops.size());
     size_t off = 0;
     for (size_t i = 0; i < ops.size(); ++i) { wsp[i] = ws + off; off += op_workspace_words(c, ops[i].L); }
@@ -397,7 +424,7 @@ void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops,
     for (u64* w : ws_ptrs)
         if (!w || (reinterpret_cast<uintptr_t>(w) & 15)) throw std::invalid_argument("workspace must be 16-byte aligned");
     for (const Op& op : ops) validate(c, op);
-    p.ctx = &c;
+    pin_keys(p, c, ops);
     p.dc = c.dev();
     p.logn = c.logn();
     p.tuned = false;
@@ -420,6 +447,11 @@ void rebind(Plan& p, uint32_t idx, const Op& op, const gfx::Context& c, cudaStre
     if (!same_shape) throw std::invalid_argument("rebind: level or job shape differs");
     if (op.key_id != old.key_id && p.ops.size() > 1)
         throw std::invalid_argument("rebind: changing the key of one operation of a shared batch");
+    if (op.mode != RESCALE && op.key_id != old.key_id) {   // single-op plan: move the pin
+        if (!c.acquire(op.key_id)) throw std::invalid_argument("missing eval key");
+        for (auto& id : p.key_pins)
+            if (id == old.key_id) { c.release(id); id = op.key_id; break; }
+    }
     PairDesc P = p.pairs_host[idx];
     P.mode = op.mode;
     P.galois = op.galois;

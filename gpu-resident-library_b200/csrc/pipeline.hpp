@@ -42,6 +42,7 @@ struct Plan {
     int p3_form = 0;                   // 0 plain P3; 1, 2 warp-specialised (128 x 2 CTAs, 256 x 1 CTA)
     bool tuned = false;
     const gfx::Context* ctx = nullptr;
+    std::vector<uint64_t> key_pins;    // keys this plan holds resident (Context::acquire)
     void* d_blob = nullptr;            // device tables (pairs, jobs, P5 groups, pair lists)
     void* h_blob = nullptr;            // pinned host mirror of d_blob
     size_t blob_cap = 0;

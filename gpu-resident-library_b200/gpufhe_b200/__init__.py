@@ -43,6 +43,8 @@ _API: dict = {
     "gpufhe_ctx_roots": (I32, [VP, VP]),
     "gpufhe_ctx_set_key": (I32, [VP, U64, VP, VP]),
     "gpufhe_ctx_resident_bytes": (U64, [VP]),
+    "gpufhe_ctx_set_key_budget": (I32, [VP, U64]),
+    "gpufhe_ctx_key_stats": (I32, [VP, VP]),
     "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
     "gpufhe_ntt_job_bytes": (U64, []),
     "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),
@@ -168,6 +170,21 @@ class Context:
 
     def resident_bytes(self):
         return int(lib().gpufhe_ctx_resident_bytes(self.h))
+
+    def set_key_budget(self, nbytes):
+        """Caps the device bytes of resident keys (0 = no cap); evicted keys
+        live in pinned host copies and come back when a plan needs them."""
+        check(lib().gpufhe_ctx_set_key_budget(self.h, int(nbytes)))
+
+    def key_stats(self):
+        out = (C.c_uint64 * 6)()
+        check(lib().gpufhe_ctx_key_stats(self.h, out))
+        return dict(zip(("known", "resident", "resident_bytes", "uploads", "evictions", "budget"), map(int, out)))
+
+    def key_bytes(self):
+        """Device bytes of one key: 2 * dnum * (fullQ + K) * n words."""
+        dnum = -(-self.fullQ // self.alpha)
+        return 2 * dnum * (self.fullQ + self.K) * self.n * 8
 
 
 def make_ops(specs):

@@ -49,6 +49,19 @@ int  gpufhe_ctx_roots(const gpufhe_ctx* ctx, uint64_t* roots_qp);
  * key_id 0 = relinearisation key; rotation keys use their Galois element. */
 int  gpufhe_ctx_set_key(gpufhe_ctx* ctx, uint64_t key_id, const uint64_t* av, const uint64_t* bv);
 uint64_t gpufhe_ctx_resident_bytes(const gpufhe_ctx* ctx);
+/* Rotation-key residency (the key management the reference leaves to its
+ * caller: every ks_context_create uploads one key per call, reference
+ * keyswitch_resident.cpp:32-101). bytes = 0 (the default) keeps every key
+ * resident. Otherwise the device holds at most `bytes` of keys: each key set
+ * after the budget keeps a pinned host copy, the least recently used key no
+ * plan holds is evicted to make room, and a plan built over a batch uploads
+ * the batch's evicted keys and pins them for its lifetime. A batch whose keys
+ * do not fit returns GPUFHE_ENOMEM from plan creation. A budget below one
+ * key's bytes is GPUFHE_EINVAL. */
+int  gpufhe_ctx_set_key_budget(gpufhe_ctx* ctx, uint64_t bytes);
+/* out[6] = {keys known, keys resident, resident key bytes, uploads from host
+ * copies, evictions, budget}. */
+int  gpufhe_ctx_key_stats(const gpufhe_ctx* ctx, uint64_t* out);
 
 /* ---------------------------------------------------------------- parameters
  * C forms of the reference's native parameter routines (include/params.h;
