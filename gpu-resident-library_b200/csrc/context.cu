@@ -181,9 +181,13 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
         std::vector<double> fd((size_t)QP * n, 0.0), id((size_t)QP * n, 0.0);
         for (uint32_t i = 0; i < QP; ++i) {
             if (!fp_tower(mc[i].q)) continue;
+            // signed representatives in (-q/2, q/2): the FP64 butterflies'
+            // bounds (one normalisation per round) rely on |w| <= (q-1)/2
+            const u64 q = mc[i].q;
+            auto sgn = [q](u64 w) { return w > q / 2 ? -(double)(q - w) : (double)w; };
             for (uint32_t k = 0; k < n; ++k) {
-                fd[(size_t)i * n + k] = (double)twf[(size_t)i * n + k].w;
-                id[(size_t)i * n + k] = (double)twi[(size_t)i * n + k].w;
+                fd[(size_t)i * n + k] = sgn(twf[(size_t)i * n + k].w);
+                id[(size_t)i * n + k] = sgn(twi[(size_t)i * n + k].w);
             }
         }
         dc_.twfd = upload(fd);

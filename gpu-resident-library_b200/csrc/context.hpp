@@ -42,8 +42,8 @@ struct DevCtx {
     const ModC* mod;          // [QP]: Q towers then P towers
     const Tw* twf;            // [QP][n]
     const Tw* twi;            // [QP][n]
-    const double* twfd;       // [QP][n] forward twiddles as doubles (towers with q < 2^50; else 0)
-    const double* twid;       // [QP][n] inverse twiddles as doubles
+    const double* twfd;       // [QP][n] forward twiddles as signed doubles in (-q/2, q/2) (towers with q < 2^50; else 0)
+    const double* twid;       // [QP][n] inverse twiddles, same form
     const u64* ninv;          // [QP] n^-1 mod q
     const u64* ninvp;
     const u64* ninvu;         // [fullQ] n^-1 * 2^64 mod q with mont, else n^-1 (P7 scaling of U)

@@ -94,35 +94,57 @@ __device__ __forceinline__ void gs_reg(u64 (&v)[1 << K], const TW& tw, u32 B, u6
 }
 
 // ------------------------------------------------------------------ FP64 arithmetic
-// Residues as FP64 integers for q < 2^50 (so 4q < 2^52). With
+// Residues as FP64 integers for q < 2^50 (so 8q < 2^53). With
 // M2 = 1.5*2^53 and M1 = 1.5*2^52 ("magic" constants whose addition rounds
-// to the nearest even / nearest integer):
-//   mul(y, w), |y| <= 4q, 0 <= w < q:
-//     h = RN(y*w); l = y*w - h exactly (FMA); k = RN2(h * qinv) (even);
-//     r = (h - k*q) + l, every step an exact integer below 2^53,
-//     r = y*w (mod q) and |r| <= 2q   (|k - h/q| <= 1.5, |l| <= q/2).
-//   norm(z), |z| < 2^51 q: k = RN(z * qinv); z - k*q in [-q/2 - 1, q/2 + 1].
-// A round keeps every value normalised at its start and end and normalises
-// after every second stage: forward (CT) values stay below 4.5q + 1 in
-// magnitude and every multiplier input below 2.5q + 1; inverse (GS) values
-// below 3q + 2, multiplier inputs below 3q + 2. All intermediate values are
-// exact integers, so results equal the integer path's canonical residues.
+// to the nearest even / nearest integer) and qinv = RN(1/q) (relative error
+// at most 2^-53):
+//   mul(y, w): h = RN(y*w); l = y*w - h exactly (FMA); k = RN(h*qinv) by M1
+//     or RN2(h*qinv) (even) by M2; r = (h - k*q) + l. h, l, h - k*q and r are
+//     exact integers (|h| >= 2^53 makes h an integer, h - k*q and r are
+//     integers below 2^52), so r = y*w (mod q). With |h| <= c*q*|w|:
+//     |l| <= |h| 2^-53 and |k - h/q| <= e + |h/q| 2^-53, e = 1/2 (M1) or 1 (M2).
+//   norm(z), |z| < 2^53: k = RN(z*qinv) by M1; z - k*q in [-q/2 - 1, q/2 + 1].
+//
+// Unsigned twiddles 0 <= w < q (FpArT<false>, tables converted on load): mul
+// by M2 for |y| <= 4q gives |r| <= 2q. A round keeps every value normalised
+// at its start and end and normalises after every second stage: forward (CT)
+// values stay below 4.5q + 1 and multiplier inputs below 2.5q + 1; inverse
+// (GS) values below 3q + 2, multiplier inputs below 3q + 2.
+//
+// Signed twiddles |w| <= (q-1)/2 (FpArT<true>, the library's double tables):
+// |h/q| <= |y|/2, so with c = |y|/q and q < 2^50, |l| <= (c/16) q and
+//   M1 (needs |y| < 2^52):  |r| <= (1/2 + c/8) q,
+//   M2 (needs |y| < 2^53):  |r| <= (1 + c/8) q,
+// and a round of up to four stages needs one normalisation, at its end:
+//   CT from |x| <= q/2 + 1, M1 in every stage: stage outputs below 1.07q,
+//     1.70q, 2.41q, 3.21q; multiplier inputs below 2.41q < 4q.
+//   GS from |x| <= q/2 + 1: stages one to three by M1 (multiplier inputs
+//     below q + 2, 2q + 4, 4q + 8 < 2^52, since an NTT prime below 2^50 has
+//     q = 1 mod 2n with n >= 2^9, so q <= 2^50 - 2^10 + 1), values below
+//     q + 2, 2q + 4, 4q + 8; stage four
+//     by M2 (input below 8q + 16 < 2^53, |r| <= 2q + 2), sums below 8q + 16.
+// Every value stays an exact integer below 2^53, so the results equal the
+// integer path's canonical residues.
 constexpr double FP_M1 = 6755399441055744.0;    // 1.5 * 2^52
 constexpr double FP_M2 = 13510798882111488.0;   // 1.5 * 2^53
 
-struct FpAr {
+template <bool SIGNED_TW>
+struct FpArT {
     using T = double;
     double q, qinv;
     __device__ __forceinline__ double norm(double z) const {
         const double k = __dsub_rn(__fma_rn(z, qinv, FP_M1), FP_M1);
         return __fma_rn(-k, q, z);
     }
-    __device__ __forceinline__ double mul(double y, double w) const {
+    template <bool EVEN = true>
+    __device__ __forceinline__ double mulq(double y, double w) const {
+        constexpr double M = EVEN ? FP_M2 : FP_M1;
         const double h = __dmul_rn(y, w);
         const double l = __fma_rn(y, w, -h);
-        const double k = __dsub_rn(__fma_rn(h, qinv, FP_M2), FP_M2);
+        const double k = __dsub_rn(__fma_rn(h, qinv, M), M);
         return __dadd_rn(__fma_rn(-k, q, h), l);
     }
+    __device__ __forceinline__ double mul(double y, double w) const { return mulq<true>(y, w); }
     // x < 4q (any lazy residue of the integer kernels)
     __device__ __forceinline__ double in(u64 x) const { return norm(u2d(x)); }
     // normalised z -> canonical [0, q)
@@ -137,6 +159,7 @@ struct FpAr {
 
     template <int K, int L, class TW>
     __device__ __forceinline__ void ct_stage(double (&v)[1 << K], const TW& tw, u32 B) const {
+        static_assert(K <= 4, "bounds are proven for rounds of at most four stages");
         constexpr int half = 1 << (K - 1 - L);
 #pragma unroll
         for (int g = 0; g < (1 << L); ++g) {
@@ -145,12 +168,12 @@ struct FpAr {
             for (int o = 0; o < half; ++o) {
                 double& x = v[g * 2 * half + o];
                 double& y = v[g * 2 * half + o + half];
-                const double r = mul(y, w), xx = x;
+                const double r = mulq<!SIGNED_TW>(y, w), xx = x;
                 x = __dadd_rn(xx, r);
                 y = __dsub_rn(xx, r);
             }
         }
-        if constexpr (L % 2 == 1 || L == K - 1) {
+        if constexpr ((!SIGNED_TW && L % 2 == 1) || L == K - 1) {
 #pragma unroll
             for (int u = 0; u < (1 << K); ++u) v[u] = norm(v[u]);
         }
@@ -158,7 +181,9 @@ struct FpAr {
     }
     template <int K, int L, class TW>
     __device__ __forceinline__ void gs_stage(double (&v)[1 << K], const TW& tw, u32 B) const {
+        static_assert(K <= 4, "bounds are proven for rounds of at most four stages");
         constexpr int half = 1 << (K - 1 - L);
+        constexpr bool EVEN = !SIGNED_TW || (K - 1 - L) >= 3;
 #pragma unroll
         for (int g = 0; g < (1 << L); ++g) {
             const double w = tw((B << L) + g);
@@ -168,10 +193,10 @@ struct FpAr {
                 double& y = v[g * 2 * half + o + half];
                 const double xx = x, yy = y;
                 x = __dadd_rn(xx, yy);
-                y = mul(__dsub_rn(xx, yy), w);
+                y = mulq<EVEN>(__dsub_rn(xx, yy), w);
             }
         }
-        if constexpr ((K - L) % 2 == 0 || L == 0) {
+        if constexpr ((!SIGNED_TW && (K - L) % 2 == 0) || L == 0) {
 #pragma unroll
             for (int u = 0; u < (1 << K); ++u) v[u] = norm(v[u]);
         }
@@ -182,6 +207,10 @@ struct FpAr {
     template <int K, class TW>
     __device__ __forceinline__ void inv(double (&v)[1 << K], const TW& tw, u32 B) const { gs_stage<K, K - 1>(v, tw, B); }
 };
+// Unsigned twiddles (the reference's u64 tables converted on load).
+using FpAr = FpArT<false>;
+// Signed twiddles in (-q/2, q/2) (the library's double tables).
+using FpArS = FpArT<true>;
 
 // Integer path: the lazy Harvey/Shoup butterflies above, values as-is.
 struct IntAr {

@@ -117,7 +117,7 @@ __device__ __forceinline__ u64* slot_ptr(const PairDesc& P, u32 slot, int logn) 
 // FP64 (FP = true, towers with q < 2^50) instantiation of a phase kernel.
 template <bool FP>
 __device__ __forceinline__ auto ar_of(const ModC& m) {
-    if constexpr (FP) return ntt::FpAr{ntt::u2d(m.q), qinv_of(m)};
+    if constexpr (FP) return ntt::FpArS{ntt::u2d(m.q), qinv_of(m)};
     else return ntt::IntAr{m.q, m.two_q};
 }
 template <bool FP>

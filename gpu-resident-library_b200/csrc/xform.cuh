@@ -12,9 +12,10 @@ namespace xf {
 
 // One tower to transform in place. Twiddles either packed {w, wp} (library
 // tables) or split (two arrays, the reference's table layout). fp != 0 (only
-// for q < 2^50) selects the FP64 arithmetic, with the double table twd or,
-// when twd is null, the split w table converted on load. Fields after
-// scale_p default to zero (integer path) in brace initialisation.
+// for q < 2^50) selects the FP64 arithmetic, with the signed double table twd
+// (twiddles in (-q/2, q/2)) or, when twd is null, the split w table converted
+// on load. Fields after scale_p default to zero (integer path) in brace
+// initialisation.
 struct Job {
     u64* x;
     const Tw* tw;        // packed tables, or nullptr when split
@@ -32,9 +33,9 @@ template <class F>
 __device__ __forceinline__ void with_path(const Job& j, F&& f) {
     if (j.fp) {
         const double qd = ntt::u2d(j.q);
-        const ntt::FpAr ar{qd, __ddiv_rn(1.0, qd)};
-        if (j.twd) f(ar, ntt::TwD{j.twd});
-        else f(ar, ntt::TwDConv{j.w});
+        const double qi = __ddiv_rn(1.0, qd);
+        if (j.twd) f(ntt::FpArS{qd, qi}, ntt::TwD{j.twd});
+        else f(ntt::FpAr{qd, qi}, ntt::TwDConv{j.w});
         return;
     }
     const ntt::IntAr ar{j.q, 2 * j.q};

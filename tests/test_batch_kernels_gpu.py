@@ -52,6 +52,53 @@ def test_ntt_batch(G, n, npolys, towers):
     assert np.array_equal(host(dx), x)
 
 
+@pytest.mark.parametrize("n,npolys,q_towers", [(65536, 26, 3), (32768, 41, 4)])
+def test_ntt_batch_large(G, n, npolys, q_towers):
+    """A batch larger than 48 MiB that mixes 50-bit (FP64 path, signed twiddle
+    tables) and 60-bit (integer path) towers, transformed once and three times
+    in a row from a prepared job list."""
+    ctx, Q = make_ctx(G, n, q_towers)
+    mods = [int(q) for q in Q] + [int(ctx._P[0])]
+    towers = len(mods)
+    assert npolys * towers * n * 8 > 48 << 20
+    roots = ctx.roots()
+    rng = np.random.default_rng(n + npolys)
+    x = np.concatenate([rng.integers(0, int(mods[t]), n, dtype=np.uint64)
+                        for _ in range(npolys) for t in range(towers)])
+    dx = dev(x)
+    jb = int(G.lib().gpufhe_ntt_job_bytes())
+    jf = empty(npolys * towers * jb // 8)
+    ji = empty(npolys * towers * jb // 8)
+    G.check(G.lib().gpufhe_ntt_batch(ctx.h, ptr(dx), npolys, towers, 0, 0, ptr(jf), None))
+    sync()
+    y = host(dx)
+    for p in range(npolys):
+        for t in range(towers):
+            q = int(mods[t])
+            fr, fp, ir, ip, ni, nip = O.root_tables(n, q, int(roots[t]))
+            seg = slice((p * towers + t) * n, (p * towers + t + 1) * n)
+            assert np.array_equal(y[seg], O.ntt(x[seg], n, q, fr, fp)), (p, t)
+    G.check(G.lib().gpufhe_ntt_batch(ctx.h, ptr(dx), npolys, towers, 0, 1, ptr(ji), None))
+    sync()
+    assert np.array_equal(host(dx), x)
+    for _ in range(3):
+        G.check(G.lib().gpufhe_ntt_run_jobs(ctx.h, ptr(jf), npolys * towers, 0, None))
+    sync()
+    y3 = host(dx)
+    for p, t in ((0, 0), (npolys - 1, towers - 1)):   # an FP64 tower and the 60-bit tower
+        q = int(mods[t])
+        fr, fp = O.root_tables(n, q, int(roots[t]))[:2]
+        seg = slice((p * towers + t) * n, (p * towers + t + 1) * n)
+        want = x[seg]
+        for _ in range(3):
+            want = O.ntt(want, n, q, fr, fp)
+        assert np.array_equal(y3[seg], want), (p, t)
+    for _ in range(3):
+        G.check(G.lib().gpufhe_ntt_run_jobs(ctx.h, ptr(ji), npolys * towers, 1, None))
+    sync()
+    assert np.array_equal(host(dx), x)
+
+
 @pytest.mark.parametrize("n,npolys,towers", [(2048, 2, 3), (65536, 3, 4)])
 def test_rns_mult_batch(G, n, npolys, towers):
     ctx, Q = make_ctx(G, n, towers)
