@@ -258,7 +258,7 @@ cudaError_t scale_key_rows(u64* key, const ModC* mod, const u64* scale, uint32_t
     return e;
 }
 
-void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
+void Context::set_key(uint64_t id, const u64* av, const u64* bv, bool device_src) {
     std::lock_guard<std::mutex> g(mu_);
     const size_t words = (size_t)dnum_ * (fullQ() + K()) * n_;
     auto it0 = keys_.find(id);
@@ -269,7 +269,7 @@ void Context::set_key(uint64_t id, const u64* av, const u64* bv) {
         u64* d = nullptr;
         cudaError_t e = cudaMalloc(&d, words * 8);
         if (e != cudaSuccess) throw std::runtime_error(std::string("key cudaMalloc: ") + cudaGetErrorString(e));
-        e = cudaMemcpy(d, h, words * 8, cudaMemcpyHostToDevice);
+        e = cudaMemcpy(d, h, words * 8, device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
         if (e != cudaSuccess) { cudaFree(d); throw std::runtime_error("key upload failed"); }
         return d;
     };

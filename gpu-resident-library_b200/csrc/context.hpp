@@ -93,9 +93,10 @@ public:
     const Level& level_host(uint32_t L) const { return lv_host_[L]; }
     int device() const { return device_; }
 
-    // Upload a key (host [dnum][fullQ+K][n] canonical). id 0 = relinearisation;
-    // rotation keys are stored under their Galois element.
-    void set_key(uint64_t id, const u64* av, const u64* bv);
+    // Upload a key ([dnum][fullQ+K][n] canonical; host arrays, or device
+    // arrays with device_src). id 0 = relinearisation; rotation keys are
+    // stored under their Galois element.
+    void set_key(uint64_t id, const u64* av, const u64* bv, bool device_src = false);
     // The key stored under `id` (its device pointers are null while it is
     // evicted), or nullptr for an unknown id.
     const Key* key(uint64_t id) const;

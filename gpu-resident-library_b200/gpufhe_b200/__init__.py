@@ -45,6 +45,12 @@ _API: dict = {
     "gpufhe_ctx_resident_bytes": (U64, [VP]),
     "gpufhe_ctx_set_key_budget": (I32, [VP, U64]),
     "gpufhe_ctx_key_stats": (I32, [VP, VP]),
+    "gpufhe_keygen": (I32, [VP, U32, U32, U64, C.c_double, U64, VP, VP, VP, VP]),
+    "gpufhe_evalkeygen": (I32, [VP, U32, VP, VP, VP, VP, VP, VP, U64, C.c_double, VP, VP, VP]),
+    "gpufhe_ctx_set_key_device": (I32, [VP, U64, VP, VP]),
+    "gpufhe_encrypt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, U64, C.c_double, VP, VP, VP]),
+    "gpufhe_decrypt_batch": (I32, [VP, U32, VP, VP, VP, VP, VP]),
+    "gpufhe_decrypt_crt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
     "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
     "gpufhe_ntt_job_bytes": (U64, []),
     "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),

@@ -63,6 +63,55 @@ int  gpufhe_ctx_set_key_budget(gpufhe_ctx* ctx, uint64_t bytes);
  * copies, evictions, budget}. */
 int  gpufhe_ctx_key_stats(const gpufhe_ctx* ctx, uint64_t* out);
 
+/* ---------------------------------------------------------------- keys and encryption
+ * Seeded key generation, eval-key generation, encryption and decryption on
+ * the device. The random draws are the reference's (std::mt19937_64,
+ * std::normal_distribution + lround, in its order), made on the host; the
+ * same seed gives the same keys and ciphertexts, bit for bit. Embedding into
+ * the towers, the NTTs and the products run as batched launches. Every call
+ * returns after its work on `stream` has completed. Tower t uses QP modulus t
+ * (Q towers, then P). */
+/* Secret s, public key (pkA, pkB) over the first `towers` QP moduli, eval
+ * form, device [towers][n] each; hw = 0: uniform ternary secret, else exactly
+ * hw nonzero coefficients (reference keygen_host, src/keygen.cpp:55-112, with
+ * set_secret_hamming_weight). */
+int gpufhe_keygen(gpufhe_ctx* ctx, uint32_t towers, uint32_t hw, uint64_t ns, double sigma, uint64_t seed,
+                  uint64_t* d_s, uint64_t* d_pkA, uint64_t* d_pkB, cudaStream_t stream);
+/* `count` eval keys over the full QP basis, key i switching sOld -> s with
+ * sOld = s^2 (galois[i] = 0, relinearisation) or sigma_galois[i](s), drawn
+ * from seeds[i] and installed in the context under key_ids[i] (reference
+ * evalkeygen_host / evalkeygen_host_sold, src/evalkeygen.cpp:42-113, followed
+ * by the key upload of ks_context_create, keyswitch_resident.cpp:32-101).
+ * d_sQP, d_pkA, d_pkB: device [fullQ+K][n] from gpufhe_keygen over all QP
+ * towers. d_av_out / d_bv_out: optional host arrays of count device pointers
+ * ([dnum][fullQ+K][n] each, may be null) that receive the canonical keys. */
+int gpufhe_evalkeygen(gpufhe_ctx* ctx, uint32_t count, const uint64_t* key_ids, const uint64_t* galois,
+                      const uint64_t* seeds, const uint64_t* d_sQP, const uint64_t* d_pkA, const uint64_t* d_pkB,
+                      uint64_t ns, double sigma, uint64_t* const* d_av_out, uint64_t* const* d_bv_out,
+                      cudaStream_t stream);
+/* gpufhe_ctx_set_key from device arrays. */
+int gpufhe_ctx_set_key_device(gpufhe_ctx* ctx, uint64_t key_id, const uint64_t* d_av, const uint64_t* d_bv);
+/* Encrypts `count` integer-coefficient messages m (host [count][n]) under
+ * (d_pkA, d_pkB) ([towers][n] eval form), message i with seeds[i], into the
+ * device buffers d_c0[i], d_c1[i] ([towers][n] each; host arrays of device
+ * pointers) (reference encrypt_host, src/encdec.cpp:41-64). */
+int gpufhe_encrypt_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, const int64_t* m, const uint64_t* seeds,
+                         const uint64_t* d_pkA, const uint64_t* d_pkB, uint64_t ns, double sigma,
+                         uint64_t* const* d_c0, uint64_t* const* d_c1, cudaStream_t stream);
+/* Decrypts `count` ciphertexts with the secret d_s, the reference's way: the
+ * phase c0 + c1*s in tower 0 only, centred mod q0 (reference decrypt_host,
+ * src/encdec.cpp:68-81); m_out host [count][n]. */
+int gpufhe_decrypt_batch(gpufhe_ctx* ctx, uint32_t count, const uint64_t* const* d_c0, const uint64_t* const* d_c1,
+                         const uint64_t* d_s, int64_t* m_out, cudaStream_t stream);
+/* Exact decryption over the first `towers` Q towers: the phase in every
+ * tower, centred CRT reconstruction (Garner) of each coefficient as a
+ * two's-complement 128-bit integer, out128 host [count][n][2] = {low, high}
+ * words; exact while |coefficient| < 2^127. No counterpart in the reference
+ * (which recovers from tower 0 only). */
+int gpufhe_decrypt_crt_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, const uint64_t* const* d_c0,
+                             const uint64_t* const* d_c1, const uint64_t* d_s, uint64_t* out128,
+                             cudaStream_t stream);
+
 /* ---------------------------------------------------------------- parameters
  * C forms of the reference's native parameter routines (include/params.h;
  * reference src/params.cpp:29-75). */
