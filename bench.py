@@ -341,6 +341,39 @@ def cpu_port_rate(levels, n, nthreads, budget_s=20.0):
                       f"OpenMP over pairs"}
 
 
+def cpu_keys_rate(n):
+    """Oracle keygen, relinearisation key and encryption at the rotation
+    workload's parameters, one host thread each (the reference's routines are
+    single-threaded host loops): a bounded sample for the keys_and_encryption
+    figures of the GPU arm."""
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    q0 = O.native_primes(1, 60, n)
+    Q = np.concatenate([q0, O.native_primes(ROT_TOWERS - 1, 50, n, avoid=list(q0))])
+    P = O.native_primes(K_SPECIAL, 60, n, avoid=list(Q))
+    ctx = O.Ctx(n, Q, P, ALPHA)
+    T, L = ROT_TOWERS + K_SPECIAL, ROT_TOWERS
+    t0 = time.perf_counter()
+    s, a, b = ctx.keygen(T, seed=SEED)
+    t1 = time.perf_counter()
+    s2 = np.empty_like(s)
+    for t, q in enumerate(ctx.QP):   # s^2 per tower (not timed)
+        seg = s[t * n:(t + 1) * n]
+        s2[t * n:(t + 1) * n] = [(int(x) * int(x)) % int(q) for x in seg]
+    t2 = time.perf_counter()
+    ctx.evalkeygen(s, s2, a, b, seed=SEED + 1)
+    t3 = time.perf_counter()
+    m = np.random.default_rng(SEED + 47).integers(-(1 << 40), 1 << 40, size=n, dtype=np.int64)
+    reps = 4
+    for i in range(reps):
+        ctx.encrypt(L, m, a[:L * n], b[:L * n], seed=SEED + 1000 + i)
+    t4 = time.perf_counter()
+    return {"keygen_ms": (t1 - t0) * 1e3, "relin_key_ms": (t3 - t2) * 1e3,
+            "encryptions_per_s": reps / (t4 - t3), "cores": 1, "kind": "port",
+            "sample": f"one keygen over {T} towers, one relinearisation key, {reps} encryptions at {L} towers, "
+                      f"N=2^{N_LOG}, one host thread"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -439,6 +472,60 @@ def ntt_isolation(G, torch, dev, local, cur, gen):
 ROT_TOWERS, ROT_COUNT, ROT_HOIST = 10, 256, 16
 
 
+def keys_and_encryption(G, torch, dev, ctx, galois, cts):
+    """Secret and public key over all QP towers, the relinearisation key, one
+    rotation key per Galois element (installed in ctx), encryption of one
+    seeded message per ciphertext of cts ([2][L][n] device tensors), then
+    decryption: tower 0 (the reference's) and exact CRT. Each call is
+    synchronous and includes the host random draws, so it is timed by the host
+    clock."""
+    import ctypes as C
+    n, T, L = ctx.n, ctx.fullQ + ctx.K, cts[0].shape[1]
+    lib = G.lib()
+    buf = lambda words: torch.empty(words, dtype=torch.int64, device=dev)
+    ds, da, db = buf(T * n), buf(T * n), buf(T * n)
+    arr = lambda xs: (C.c_uint64 * len(xs))(*xs)
+    parr = lambda ps: (C.c_void_p * len(ps))(*ps)
+    clock = time.perf_counter
+    torch.cuda.synchronize()
+    t0 = clock()
+    G.check(lib.gpufhe_keygen(ctx.h, T, 0, 1, 3.19, SEED, ds.data_ptr(), da.data_ptr(), db.data_ptr(), None))
+    t1 = clock()
+    G.check(lib.gpufhe_evalkeygen(ctx.h, 1, arr([0]), arr([0]), arr([SEED + 1]), ds.data_ptr(), da.data_ptr(),
+                                  db.data_ptr(), 1, 3.19, None, None, None))
+    t2 = clock()
+    G.check(lib.gpufhe_evalkeygen(ctx.h, len(galois), arr(galois), arr(galois),
+                                  arr([SEED + 100 + j for j in range(len(galois))]), ds.data_ptr(), da.data_ptr(),
+                                  db.data_ptr(), 1, 3.19, None, None, None))
+    t3 = clock()
+    count = len(cts)
+    msgs = np.random.default_rng(SEED + 47).integers(-(1 << 40), 1 << 40, size=(count, n), dtype=np.int64)
+    c0 = parr([c[0].data_ptr() for c in cts])
+    c1 = parr([c[1].data_ptr() for c in cts])
+    t4 = clock()
+    G.check(lib.gpufhe_encrypt_batch(ctx.h, count, L, msgs.ctypes.data, arr([SEED + 1000 + i for i in range(count)]),
+                                     da.data_ptr(), db.data_ptr(), 1, 3.19, c0, c1, None))
+    t5 = clock()
+    dec = np.zeros((count, n), np.int64)
+    G.check(lib.gpufhe_decrypt_batch(ctx.h, count, c0, c1, ds.data_ptr(), dec.ctypes.data, None))
+    t6 = clock()
+    crt = np.zeros((count, n, 2), np.uint64)
+    G.check(lib.gpufhe_decrypt_crt_batch(ctx.h, count, L, c0, c1, ds.data_ptr(), crt.ctypes.data, None))
+    t7 = clock()
+    # noise of the exact decryption (message + ns * noise terms)
+    v = crt[..., 0].view(np.int64)   # |coefficient| < 2^63 here: the low word is the value
+    noise_bits = float(np.log2(np.abs(v - msgs).max() + 1))
+    del ds, da, db
+    return {"params": f"N=2^{N_LOG}, {L}+{ctx.K} towers, dnum={-(-ctx.fullQ // ctx.alpha)}, sigma=3.19, "
+                      f"uniform ternary secret",
+            "timer": "host clock around synchronous calls (host random draws included)",
+            "keygen_ms": (t1 - t0) * 1e3, "relin_key_ms": (t2 - t1) * 1e3,
+            "rotation_keys": len(galois), "rotation_keys_ms": (t3 - t2) * 1e3,
+            "encryptions": count, "encrypt_ms": (t5 - t4) * 1e3, "encryptions_per_s": count / (t5 - t4),
+            "decrypt_tower0_ms": (t6 - t5) * 1e3, "decrypt_crt_ms": (t7 - t6) * 1e3,
+            "decryption_noise_bits": noise_bits}
+
+
 def rotation_batch(G, torch, dev, local, gen, steps):
     """256 ciphertexts at N=2^16, 10 towers, each rotated by a seeded index from
     {+-1, +-2, ..., +-2^14} with its own resident key; then hoisted: 16
@@ -452,19 +539,12 @@ def rotation_batch(G, torch, dev, local, gen, steps):
     steps_r = [s * (1 << j) for j in range(15) for s in (1, -1)]
     gal = [galois_element(r, n) for r in steps_r]
     rows = -(-ROT_TOWERS // ALPHA) * (ROT_TOWERS + K_SPECIAL)
-    rng = np.random.default_rng(SEED + 44)
-    pool = rng.integers(0, 1 << 49, 2 * rows * n, dtype=np.uint64)
-    for j, k in enumerate(gal):
-        key = np.roll(pool, 104729 * (j + 1))
-        ctx.set_key(k, key[: rows * n], key[rows * n:])
-    evk_bytes = ctx.resident_bytes()
     L = ROT_TOWERS
-
-    def ct():
-        t = torch.empty((2, L, n), dtype=torch.int64, device=dev)
-        for i in range(L):
-            t[:, i].random_(0, int(Q[i]), generator=gen)
-        return t
+    # real keys and encryptions, made on the GPU (timed: key generation and
+    # encryption at this workload's parameters)
+    cts = [torch.empty((2, L, n), dtype=torch.int64, device=dev) for _ in range(ROT_COUNT)]
+    keys = keys_and_encryption(G, torch, dev, ctx, sorted(set(gal)), cts)
+    evk_bytes = ctx.resident_bytes()
 
     def timed(specs):
         wsb = sum(ctx.workspace_bytes(sp["level"]) for sp in specs)
@@ -491,15 +571,13 @@ def rotation_batch(G, torch, dev, local, gen, steps):
         return ms, sched
 
     idx = np.random.default_rng(SEED + 45).integers(0, len(gal), ROT_COUNT)
-    cts = [ct() for _ in range(ROT_COUNT)]
     outs = [torch.empty((2, L, n), dtype=torch.int64, device=dev) for _ in range(ROT_COUNT)]
     specs = [dict(level=L, mode=G.ROTATE, key_id=gal[k], galois=gal[k],
                   inp=[c[0].data_ptr(), c[1].data_ptr()], out=[o[0].data_ptr(), o[1].data_ptr()])
              for c, o, k in zip(cts, outs, idx)]
     ms_plain, sched_plain = timed(specs)
-    del cts
     hrng = np.random.default_rng(SEED + 46)
-    hcts = [ct() for _ in range(ROT_COUNT // ROT_HOIST)]
+    hcts = cts[:ROT_COUNT // ROT_HOIST]
     hspecs = []
     for g, c in enumerate(hcts):
         for k in hrng.choice(len(gal), ROT_HOIST, replace=False):
@@ -507,10 +585,12 @@ def rotation_batch(G, torch, dev, local, gen, steps):
             hspecs.append(dict(level=L, mode=G.ROTATE_HOISTED, key_id=gal[k], galois=gal[k],
                                inp=[c[0].data_ptr(), c[1].data_ptr()], out=[o[0].data_ptr(), o[1].data_ptr()]))
     ms_hoist, sched_hoist = timed(hspecs)
-    del hcts, outs
+    del hcts, outs, cts
     ctx.close()
     return {"workload": "256 ciphertexts, N=2^16, 10 towers (1x60+9x50), P=3x60, alpha=3, index from "
-                        "{+-1,...,+-2^14} with resident keys; hoisted: 16 ciphertexts x 16 rotations",
+                        "{+-1,...,+-2^14} with resident keys; hoisted: 16 ciphertexts x 16 rotations; keys and "
+                        "ciphertexts are real (generated and encrypted on the GPU, seeded)",
+            "keys_and_encryption": keys,
             "rotations_per_s": ROT_COUNT / (ms_plain * 1e-3), "ms_per_batch": ms_plain, "schedule": sched_plain,
             "hoisted_rotations_per_s": ROT_COUNT / (ms_hoist * 1e-3), "hoisted_ms_per_batch": ms_hoist,
             "hoisted_schedule": sched_hoist, "resident_bytes": evk_bytes,
@@ -747,6 +827,8 @@ def run_gpu(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_port_rate(levels, n, 0)
+        if not args.no_rot:
+            cpu["keys_and_encryption"] = cpu_keys_rate(n)
 
     if dist is not None:
         dist.barrier()
