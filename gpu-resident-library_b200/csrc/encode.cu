@@ -1,0 +1,198 @@
+// Canonical CKKS encode / decode on the device (include/gpufhe_b200.h).
+//
+// The reference's encode_host / decode_host (src/encode.cpp:13-44) are O(N^2)
+// host loops in double precision:
+//   encode: m_j = llround((2 Delta / N) * sum_k (Re z_k Re tw[t] - Im z_k Im tw[t])),
+//   decode: z_k = (sum_j m_j tw[t]) / Delta,     t = j * r_k mod 2N, r_k = 5^k mod 2N,
+// with tw[t] = polar(1, -+pi t / N) from the host's libm. Here every output
+// index is one thread that runs the same sum in the same order, with
+// separately rounded products and sums (no fused multiply-add) and the
+// twiddle table computed on the host by the same expression, so encodings and
+// decodings equal the reference's bit for bit. A thread carries up to MB
+// messages of a batch, so each twiddle gather (from the 2N-entry table in L2)
+// serves MB sums.
+#include <cmath>
+#include <complex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "context.hpp"
+#include "gpufhe_b200.h"
+
+struct gpufhe_encoder {
+    uint32_t n = 0;
+    int device = 0;
+    double2* tw_enc = nullptr;   // [2n] polar(1, -pi t / n)
+    double2* tw_dec = nullptr;   // [2n] polar(1, +pi t / n)
+    uint32_t* r = nullptr;       // [n/2] 5^k mod 2n
+};
+
+namespace {
+
+constexpr int ENT = 128;   // threads per block
+constexpr int MB = 4;      // messages per thread
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// m[b][j], one thread per j, messages b0..b0+MB-1 of the batch.
+__global__ void __launch_bounds__(ENT) k_encode(const double2* __restrict__ tw, const uint32_t* __restrict__ r,
+                                                const double2* __restrict__ z, int64_t* __restrict__ m,
+                                                uint32_t n, uint32_t count, double sc) {
+    const uint32_t j = blockIdx.x * ENT + threadIdx.x;
+    const uint32_t b0 = blockIdx.y * MB;
+    if (j >= n) return;
+    const uint32_t S = n / 2, mask = 2 * n - 1;
+    const uint32_t nb = min((uint32_t)MB, count - b0);
+    double acc[MB] = {0.0, 0.0, 0.0, 0.0};
+    const double2* zb = z + (size_t)b0 * S;
+#pragma unroll 4
+    for (uint32_t k = 0; k < S; ++k) {
+        const uint32_t t = (j * __ldg(r + k)) & mask;   // j * r_k mod 2n (2n divides 2^32)
+        const double2 w = __ldg(tw + t);
+#pragma unroll
+        for (int b = 0; b < MB; ++b) {
+            if (b < (int)nb) {
+                const double2 v = __ldg(zb + (size_t)b * S + k);
+                acc[b] = __dadd_rn(acc[b], __dsub_rn(__dmul_rn(v.x, w.x), __dmul_rn(v.y, w.y)));
+            }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < MB; ++b)
+        if (b < (int)nb) m[(size_t)(b0 + b) * n + j] = llround(__dmul_rn(sc, acc[b]));
+}
+
+// z[b][k], one thread per slot k.
+__global__ void __launch_bounds__(ENT) k_decode(const double2* __restrict__ tw, const uint32_t* __restrict__ r,
+                                                const int64_t* __restrict__ m, double2* __restrict__ z,
+                                                uint32_t n, uint32_t count, double delta) {
+    const uint32_t S = n / 2, mask = 2 * n - 1;
+    const uint32_t k = blockIdx.x * ENT + threadIdx.x;
+    const uint32_t b0 = blockIdx.y * MB;
+    if (k >= S) return;
+    const uint32_t nb = min((uint32_t)MB, count - b0);
+    const uint32_t rk = __ldg(r + k);
+    double ar[MB] = {0.0, 0.0, 0.0, 0.0}, ai[MB] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t* mb = m + (size_t)b0 * n;
+#pragma unroll 4
+    for (uint32_t j = 0; j < n; ++j) {
+        const double2 w = __ldg(tw + ((j * rk) & mask));
+#pragma unroll
+        for (int b = 0; b < MB; ++b) {
+            if (b < (int)nb) {
+                const double mj = __ll2double_rn(__ldg(reinterpret_cast<const long long*>(mb) + (size_t)b * n + j));
+                ar[b] = __dadd_rn(ar[b], __dmul_rn(mj, w.x));
+                ai[b] = __dadd_rn(ai[b], __dmul_rn(mj, w.y));
+            }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < MB; ++b)
+        if (b < (int)nb) z[(size_t)(b0 + b) * S + k] = make_double2(__ddiv_rn(ar[b], delta), __ddiv_rn(ai[b], delta));
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpufhe_encoder_create(uint32_t n, int device, gpufhe_encoder** out) {
+    if (!out || n < 4 || (n & (n - 1)) || n > (1u << 17)) {
+        gfx::set_error("gpufhe_encoder_create: n must be a power of two in [4, 2^17]");
+        return GPUFHE_EINVAL;
+    }
+    *out = nullptr;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    auto* E = new gpufhe_encoder;
+    try {
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        E->n = n;
+        E->device = device;
+        const uint32_t M = 2 * n, S = n / 2;
+        std::vector<double2> te(M), td(M);
+        for (uint32_t t = 0; t < M; ++t) {
+            // the reference's table expressions (encode.cpp:18, 35), host libm
+            const std::complex<double> a = std::polar(1.0, -M_PI * (double)t / (double)n);
+            const std::complex<double> b = std::polar(1.0, +M_PI * (double)t / (double)n);
+            te[t] = make_double2(a.real(), a.imag());
+            td[t] = make_double2(b.real(), b.imag());
+        }
+        std::vector<uint32_t> r(S);
+        uint64_t rk = 1;
+        for (uint32_t k = 0; k < S; ++k) { r[k] = (uint32_t)rk; rk = (rk * 5) % M; }
+        ck(cudaMalloc(&E->tw_enc, M * sizeof(double2)), "cudaMalloc");
+        ck(cudaMalloc(&E->tw_dec, M * sizeof(double2)), "cudaMalloc");
+        ck(cudaMalloc(&E->r, S * sizeof(uint32_t)), "cudaMalloc");
+        ck(cudaMemcpy(E->tw_enc, te.data(), M * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+        ck(cudaMemcpy(E->tw_dec, td.data(), M * sizeof(double2), cudaMemcpyHostToDevice), "upload");
+        ck(cudaMemcpy(E->r, r.data(), S * sizeof(uint32_t), cudaMemcpyHostToDevice), "upload");
+    } catch (const std::exception& e) {
+        gpufhe_encoder_destroy(E);
+        cudaSetDevice(prev);
+        gfx::set_error(e.what());
+        return GPUFHE_ECUDA;
+    }
+    cudaSetDevice(prev);
+    *out = E;
+    return GPUFHE_OK;
+}
+
+void gpufhe_encoder_destroy(gpufhe_encoder* E) {
+    if (!E) return;
+    cudaFree(E->tw_enc);
+    cudaFree(E->tw_dec);
+    cudaFree(E->r);
+    delete E;
+}
+
+int gpufhe_encode_batch(gpufhe_encoder* E, uint32_t count, const double* z, double delta, int64_t* m,
+                        cudaStream_t s) {
+    if (!E || !z || !m) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    if (!count) return GPUFHE_OK;
+    const uint32_t n = E->n, S = n / 2;
+    double2* dz = nullptr;
+    int64_t* dm = nullptr;
+    cudaError_t e = cudaMallocAsync(&dz, (size_t)count * S * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dm, (size_t)count * n * 8, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dz, z, (size_t)count * S * sizeof(double2), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        const double sc = 2.0 * delta / (double)n;   // encode.cpp:22
+        k_encode<<<dim3((n + ENT - 1) / ENT, (count + MB - 1) / MB), ENT, 0, s>>>(E->tw_enc, E->r, dz, dm, n, count,
+                                                                                 sc);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m, dm, (size_t)count * n * 8, cudaMemcpyDeviceToHost, s);
+    if (dz) cudaFreeAsync(dz, s);
+    if (dm) cudaFreeAsync(dm, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
+}
+
+int gpufhe_decode_batch(gpufhe_encoder* E, uint32_t count, const int64_t* m, double delta, double* z,
+                        cudaStream_t s) {
+    if (!E || !z || !m) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    if (!count) return GPUFHE_OK;
+    const uint32_t n = E->n, S = n / 2;
+    double2* dz = nullptr;
+    int64_t* dm = nullptr;
+    cudaError_t e = cudaMallocAsync(&dz, (size_t)count * S * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dm, (size_t)count * n * 8, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dm, m, (size_t)count * n * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        k_decode<<<dim3((S + ENT - 1) / ENT, (count + MB - 1) / MB), ENT, 0, s>>>(E->tw_dec, E->r, dm, dz, n, count,
+                                                                                 delta);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(z, dz, (size_t)count * S * sizeof(double2), cudaMemcpyDeviceToHost, s);
+    if (dz) cudaFreeAsync(dz, s);
+    if (dm) cudaFreeAsync(dm, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
+}
+
+}  // extern "C"

@@ -51,6 +51,10 @@ _API: dict = {
     "gpufhe_encrypt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, U64, C.c_double, VP, VP, VP]),
     "gpufhe_decrypt_batch": (I32, [VP, U32, VP, VP, VP, VP, VP]),
     "gpufhe_decrypt_crt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
+    "gpufhe_encoder_create": (I32, [U32, I32, C.POINTER(VP)]),
+    "gpufhe_encoder_destroy": (None, [VP]),
+    "gpufhe_encode_batch": (I32, [VP, U32, VP, C.c_double, VP, VP]),
+    "gpufhe_decode_batch": (I32, [VP, U32, VP, C.c_double, VP, VP]),
     "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
     "gpufhe_ntt_job_bytes": (U64, []),
     "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),
@@ -136,6 +140,46 @@ def api_symbols():
 def _np_u64(a):
     import numpy as np
     return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+class Encoder:
+    """Canonical encode / decode (the reference's encode_host / decode_host)
+    on the device, numpy in and out."""
+
+    def __init__(self, n, device=0):
+        h = VP()
+        check(lib().gpufhe_encoder_create(n, device, C.byref(h)))
+        self.h, self.n = h, n
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpufhe_encoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def encode(self, z, delta):
+        """z: [count][n/2] or [n/2] complex -> int64 [count][n] (or [n])."""
+        import numpy as np
+        z = np.asarray(z, dtype=np.complex128)
+        one = z.ndim == 1
+        z = np.ascontiguousarray(z.reshape(-1, self.n // 2))
+        m = np.zeros((z.shape[0], self.n), np.int64)
+        check(lib().gpufhe_encode_batch(self.h, z.shape[0], z.ctypes.data, float(delta), m.ctypes.data, None))
+        return m[0] if one else m
+
+    def decode(self, m, delta):
+        import numpy as np
+        m = np.asarray(m, dtype=np.int64)
+        one = m.ndim == 1
+        m = np.ascontiguousarray(m.reshape(-1, self.n))
+        z = np.zeros((m.shape[0], self.n // 2), np.complex128)
+        check(lib().gpufhe_decode_batch(self.h, m.shape[0], m.ctypes.data, float(delta), z.ctypes.data, None))
+        return z[0] if one else z
 
 
 class Context:

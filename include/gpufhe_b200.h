@@ -112,6 +112,24 @@ int gpufhe_decrypt_crt_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, c
                              const uint64_t* const* d_c1, const uint64_t* d_s, uint64_t* out128,
                              cudaStream_t stream);
 
+/* ---------------------------------------------------------------- canonical encode / decode
+ * The reference's encode_host / decode_host (src/encode.cpp:13-44): slots
+ * z_0..z_{n/2-1} (complex, interleaved re/im doubles) <-> n integer
+ * coefficients at scale delta, with the same summation order, rounding and
+ * twiddle table, so results equal the reference's bit for bit; one thread
+ * per output index, a batch of messages per launch. The encoder holds the
+ * twiddle table (32n bytes) and the rotation-group exponents on `device`;
+ * calls must run with that device current. Buffers are host memory; each
+ * call returns after its work on `stream` has completed. */
+typedef struct gpufhe_encoder gpufhe_encoder;
+int  gpufhe_encoder_create(uint32_t n, int device, gpufhe_encoder** out);
+void gpufhe_encoder_destroy(gpufhe_encoder* enc);
+/* z: [count][n/2][2] doubles; m: [count][n] */
+int  gpufhe_encode_batch(gpufhe_encoder* enc, uint32_t count, const double* z, double delta, int64_t* m,
+                         cudaStream_t stream);
+int  gpufhe_decode_batch(gpufhe_encoder* enc, uint32_t count, const int64_t* m, double delta, double* z,
+                         cudaStream_t stream);
+
 /* ---------------------------------------------------------------- parameters
  * C forms of the reference's native parameter routines (include/params.h;
  * reference src/params.cpp:29-75). */

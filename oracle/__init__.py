@@ -21,6 +21,7 @@ _REF_GPU = os.path.join(HERE, "_ref", "libref_gpu.so")
 
 u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 VP = C.c_void_p
 U32, U64, I32, DBL = C.c_uint32, C.c_uint64, C.c_int, C.c_double
@@ -79,6 +80,8 @@ def lib():
             "orc_rotate": (None, [VP, U32, U32, U32, u64p, u64p]),
             "orc_rotate_hoisted": (None, [VP, U32, U32, u32p, u32p, u64p, u64p, VP, VP]),
             "orc_num_threads": (I32, []),
+            "orc_encode": (None, [i64p, f64p, f64p, U32, DBL]),
+            "orc_decode": (None, [f64p, f64p, i64p, U32, DBL]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -273,6 +276,21 @@ def num_threads():
     return int(lib().orc_num_threads())
 
 
+def encode(z, n, delta):
+    """Canonical encode of n/2 complex slots (reference encode.cpp:13-28)."""
+    z = np.asarray(z, dtype=np.complex128)
+    m = np.zeros(n, np.int64)
+    lib().orc_encode(m, np.ascontiguousarray(z.real), np.ascontiguousarray(z.imag), n, float(delta))
+    return m
+
+
+def decode(m, n, delta):
+    """Canonical decode of n integer coefficients (reference encode.cpp:30-44)."""
+    zr, zi = np.zeros(n // 2), np.zeros(n // 2)
+    lib().orc_decode(zr, zi, np.ascontiguousarray(m, np.int64), n, float(delta))
+    return zr + 1j * zi
+
+
 def galois_element(r, n):
     """k = 5^r mod 2n; negative r uses the inverse (5^-r), conjugation is 2n-1."""
     M = 2 * n
@@ -293,7 +311,9 @@ def load_ref_host():
     L.ref_ks_constants.restype = U32
     L.ref_ks_constants.argtypes = [u64p, u64p, U32, u64p, U32, U32]
     L.ref_encode.restype = None
-    L.ref_encode.argtypes = [i64p, np.ctypeslib.ndpointer(np.float64), np.ctypeslib.ndpointer(np.float64), U32, DBL]
+    L.ref_encode.argtypes = [i64p, f64p, f64p, U32, DBL]
+    L.ref_decode.restype = None
+    L.ref_decode.argtypes = [f64p, f64p, i64p, U32, DBL]
     return L
 
 

@@ -14,6 +14,7 @@
 #include "ckks_oracle.h"
 
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <random>
 #include <stdexcept>
@@ -903,6 +904,60 @@ int orc_num_threads(void) {
 #else
     return 1;
 #endif
+}
+
+/* Canonical encode / decode (reference src/encode.cpp:13-44): slots
+ * z_0..z_{N/2-1} <-> integer coefficients at scale Delta with
+ * r_k = 5^k mod 2N and the twiddle table tw[t] = polar(1, -+pi t / N).
+ *   encode: m_j = llround((2 Delta / N) * sum_k (Re z_k Re tw[j r_k] - Im z_k Im tw[j r_k]))
+ *   decode: z_k = (sum_j m_j tw[j r_k]) / Delta
+ * Sums run in index order with separate products and sums (no fused
+ * multiply-add), so the doubles equal the reference's. */
+void orc_encode(int64_t* m, const double* zre, const double* zim, uint32_t N, double Delta) {
+    const uint32_t M = 2 * N, S = N / 2;
+    std::vector<double> twr(M), twi(M);
+    for (uint32_t t = 0; t < M; ++t) {
+        const std::complex<double> w = std::polar(1.0, -M_PI * (double)t / (double)N);
+        twr[t] = w.real();
+        twi[t] = w.imag();
+    }
+    std::vector<uint64_t> r(S);
+    uint64_t rk = 1;
+    for (uint32_t k = 0; k < S; ++k) { r[k] = rk; rk = (rk * 5) % M; }
+    const double sc = 2.0 * Delta / (double)N;
+    for (uint32_t j = 0; j < N; ++j) {
+        double acc = 0;
+        for (uint32_t k = 0; k < S; ++k) {
+            const uint64_t t = ((uint64_t)j * r[k]) % M;
+            const double a = zre[k] * twr[t];
+            const double b = zim[k] * twi[t];
+            acc += a - b;
+        }
+        m[j] = (int64_t)llround(sc * acc);
+    }
+}
+
+void orc_decode(double* zre, double* zim, const int64_t* m, uint32_t N, double Delta) {
+    const uint32_t M = 2 * N, S = N / 2;
+    std::vector<double> twr(M), twi(M);
+    for (uint32_t t = 0; t < M; ++t) {
+        const std::complex<double> w = std::polar(1.0, +M_PI * (double)t / (double)N);
+        twr[t] = w.real();
+        twi[t] = w.imag();
+    }
+    uint64_t rk = 1;
+    for (uint32_t k = 0; k < S; ++k) {
+        double ar = 0, ai = 0;
+        for (uint32_t j = 0; j < N; ++j) {
+            const uint64_t t = ((uint64_t)j * rk) % M;
+            const double mj = (double)m[j];
+            ar += mj * twr[t];
+            ai += mj * twi[t];
+        }
+        zre[k] = ar / Delta;
+        zim[k] = ai / Delta;
+        rk = (rk * 5) % M;
+    }
 }
 
 }  // extern "C"

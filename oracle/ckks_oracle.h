@@ -125,6 +125,11 @@ void orc_rotate_hoisted(const OrcCtx* c, uint32_t L, uint32_t nrot, const uint32
                         uint64_t* const* out0, uint64_t* const* out1);
 int orc_num_threads(void);
 
+/* Canonical encode / decode (reference src/encode.cpp:13-44): z as separate
+ * real / imaginary arrays of N/2 slots, m of N coefficients. */
+void orc_encode(int64_t* m, const double* zre, const double* zim, uint32_t N, double Delta);
+void orc_decode(double* zre, double* zim, const int64_t* m, uint32_t N, double Delta);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,7 +7,8 @@ EvalMult+Rescale, keyswitch and rotation runs. tests/test_golden.py then
 regenerates the same arrays with the CPU oracle and compares digests, which
 pins the oracle to the reference without shipping megabytes of residues.
 
-  python tests/golden/make_golden.py        (needs a CUDA GPU)
+  python tests/golden/make_golden.py          (needs a CUDA GPU)
+  python tests/golden/make_golden.py encode   (canonical encode / decode; host only)
 
 Config-1 parameters: N = 2^15, Q = one 60-bit + three 50-bit primes,
 P = two 60-bit primes, dnum = 2, scale 2^50, ternary secret, sigma 3.2,
@@ -28,7 +29,8 @@ import oracle as O  # noqa: E402
 
 def digest(a):
     a = np.ascontiguousarray(a)
-    return {"sha256": hashlib.sha256(a.tobytes()).hexdigest(), "head": [int(x) for x in a.ravel()[:6]],
+    conv = float if a.dtype.kind == "f" else int
+    return {"sha256": hashlib.sha256(a.tobytes()).hexdigest(), "head": [conv(x) for x in a.ravel()[:6]],
             "words": int(a.size)}
 
 
@@ -114,7 +116,43 @@ def rotation(R):
     return out
 
 
+def slots(seed, n, real_only=False):
+    g = np.random.default_rng(seed)
+    re = g.uniform(-1.0, 1.0, n // 2)
+    im = np.zeros(n // 2) if real_only else g.uniform(-1.0, 1.0, n // 2)
+    return re, im
+
+
+# (n, seed, delta bits, real-only slots): canonical encode / decode cases
+ENCODE_CASES = [(1 << 10, 11, 40, False), (1 << 12, 12, 40, False), (1 << 12, 13, 50, True),
+                (1 << 13, 14, 30, False)]
+
+
+def encode_cases(H):
+    """The reference's encode_host / decode_host (encode.cpp:13-44, host-only
+    code, oracle/_ref/libref_host.so) on seeded slots: digests of the
+    coefficients and of the decoded slots."""
+    out = {"cases": []}
+    for n, seed, dbits, real in ENCODE_CASES:
+        re, im = slots(seed, n, real)
+        m = np.zeros(n, np.int64)
+        H.ref_encode(m, re, im, n, float(2.0 ** dbits))
+        zr, zi = np.zeros(n // 2), np.zeros(n // 2)
+        H.ref_decode(zr, zi, m, n, float(2.0 ** dbits))
+        out["cases"].append({"n": n, "seed": seed, "delta_bits": dbits, "real_only": real, "m": digest(m),
+                             "dec_re": digest(zr), "dec_im": digest(zi)})
+    return out
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "encode":   # host-only code, no GPU needed
+        H = O.load_ref_host()
+        if H is None:
+            raise SystemExit("oracle/_ref/libref_host.so missing: run oracle/build_ref.sh")
+        with open(os.path.join(HERE, "encode_golden.json"), "w") as f:
+            json.dump(encode_cases(H), f, indent=1)
+        print("encode golden vectors written")
+        return
     R = O.load_ref_gpu()
     if R is None:
         raise SystemExit("oracle/_ref/libref_gpu.so missing: run oracle/build_ref.sh")

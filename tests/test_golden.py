@@ -90,3 +90,17 @@ def test_rotation_golden():
         ctx.set_key(k, av, bv)
         r0, r1 = ctx.rotate(L, k, c0, c1, k)
         assert same(r0, d["rot0"]) and same(r1, d["rot1"])
+
+
+def test_encode_golden():
+    """Canonical encode / decode (reference encode.cpp:13-44): the oracle's
+    coefficients and decoded doubles equal the reference's, bit for bit."""
+    from golden.make_golden import slots
+    g = load("encode_golden.json")
+    for c in g["cases"]:
+        n, d = c["n"], float(2.0 ** c["delta_bits"])
+        re, im = slots(c["seed"], n, c["real_only"])
+        m = O.encode(re + 1j * im, n, d)
+        assert same(m, c["m"]), c
+        z = O.decode(m, n, d)
+        assert same(np.ascontiguousarray(z.real), c["dec_re"]) and same(np.ascontiguousarray(z.imag), c["dec_im"]), c
