@@ -368,10 +368,16 @@ def cpu_keys_rate(n):
     for i in range(reps):
         ctx.encrypt(L, m, a[:L * n], b[:L * n], seed=SEED + 1000 + i)
     t4 = time.perf_counter()
+    z = np.random.default_rng(SEED + 48).uniform(-1, 1, n // 2) + 0j
+    em = O.encode(z, n, 2.0 ** 40)
+    t5 = time.perf_counter()
+    O.decode(em, n, 2.0 ** 40)
+    t6 = time.perf_counter()
     return {"keygen_ms": (t1 - t0) * 1e3, "relin_key_ms": (t3 - t2) * 1e3,
-            "encryptions_per_s": reps / (t4 - t3), "cores": 1, "kind": "port",
+            "encryptions_per_s": reps / (t4 - t3), "encodes_per_s": 1 / (t5 - t4), "decodes_per_s": 1 / (t6 - t5),
+            "cores": 1, "kind": "port",
             "sample": f"one keygen over {T} towers, one relinearisation key, {reps} encryptions at {L} towers, "
-                      f"N=2^{N_LOG}, one host thread"}
+                      f"one canonical encode and decode, N=2^{N_LOG}, one host thread"}
 
 
 def run_reference(args):
@@ -470,6 +476,7 @@ def ntt_isolation(G, torch, dev, local, cur, gen):
 
 # ---------------------------------------------------------------- rotation batch
 ROT_TOWERS, ROT_COUNT, ROT_HOIST = 10, 256, 16
+ENC_COUNT = 16
 
 
 def keys_and_encryption(G, torch, dev, ctx, galois, cts):
@@ -516,6 +523,17 @@ def keys_and_encryption(G, torch, dev, ctx, galois, cts):
     v = crt[..., 0].view(np.int64)   # |coefficient| < 2^63 here: the low word is the value
     noise_bits = float(np.log2(np.abs(v - msgs).max() + 1))
     del ds, da, db
+    # canonical encode / decode of 16 slot vectors at scale 2^40
+    enc = G.Encoder(n, device=torch.cuda.current_device())
+    zr = np.random.default_rng(SEED + 48)
+    z = zr.uniform(-1, 1, (ENC_COUNT, n // 2)) + 1j * zr.uniform(-1, 1, (ENC_COUNT, n // 2))
+    enc.encode(z[:1], 2.0 ** 40)   # first call: allocator pools
+    t8 = clock()
+    em = enc.encode(z, 2.0 ** 40)
+    t9 = clock()
+    zd = enc.decode(em, 2.0 ** 40)
+    t10 = clock()
+    enc.close()
     return {"params": f"N=2^{N_LOG}, {L}+{ctx.K} towers, dnum={-(-ctx.fullQ // ctx.alpha)}, sigma=3.19, "
                       f"uniform ternary secret",
             "timer": "host clock around synchronous calls (host random draws included)",
@@ -523,7 +541,12 @@ def keys_and_encryption(G, torch, dev, ctx, galois, cts):
             "rotation_keys": len(galois), "rotation_keys_ms": (t3 - t2) * 1e3,
             "encryptions": count, "encrypt_ms": (t5 - t4) * 1e3, "encryptions_per_s": count / (t5 - t4),
             "decrypt_tower0_ms": (t6 - t5) * 1e3, "decrypt_crt_ms": (t7 - t6) * 1e3,
-            "decryption_noise_bits": noise_bits}
+            "decryption_noise_bits": noise_bits,
+            "encode": {"messages": ENC_COUNT, "encode_ms": (t9 - t8) * 1e3, "decode_ms": (t10 - t9) * 1e3,
+                       "encodes_per_s": ENC_COUNT / (t9 - t8), "decodes_per_s": ENC_COUNT / (t10 - t9),
+                       "round_trip_max_err": float(np.abs(zd - z).max()),
+                       "form": "the reference's O(N^2) sums in its order, bit-identical, one thread per "
+                               "output index, 4 messages per thread"}}
 
 
 def rotation_batch(G, torch, dev, local, gen, steps):
@@ -596,6 +619,31 @@ def rotation_batch(G, torch, dev, local, gen, steps):
             "hoisted_schedule": sched_hoist, "resident_bytes": evk_bytes,
             "distinct_keys": len(set(gal)), "evk_bytes": len(set(gal)) * 2 * rows * n * 8,
             "note": "rotations by +2^14 and -2^14 share one Galois element at N=2^16 (2^15 slots)"}
+
+
+def plain_driver(levels, n, reps, local):
+    """The plain per-chain resident form as the reference defines it: its
+    bench_evalmult_resident driver (one CUDA graph per chain of LaunchTensor ->
+    keyswitch_resident -> LaunchCombine -> rescale_resident_raw x2) run on this
+    library's drop-in API (drivers/plain_chain), one chain after the other on
+    one stream and spread over 16 streams; device time by CUDA events."""
+    from gpufhe_b200 import build as B
+    exe = B.build_driver()
+    env = dict(os.environ)
+    vis = env.get("CUDA_VISIBLE_DEVICES")
+    env["CUDA_VISIBLE_DEVICES"] = vis.split(",")[local] if vis else str(local)
+    r = subprocess.run([exe, str(n), str(FULLQ), str(K_SPECIAL), str(ALPHA), str(max(2, reps)), "-",
+                        *map(str, levels)], capture_output=True, text=True, timeout=900, env=env)
+    if r.returncode != 0:
+        raise RuntimeError("plain_chain driver failed: " + r.stderr[-2000:])
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    ops = len(levels)
+    return {"value": ops / (d["one_stream_ms"] * 1e-3), "unit": "ops/s", "ms_per_step": d["one_stream_ms"],
+            "form": "the reference's per-chain driver (bench_evalmult_resident.cpp:80-109) on this library's "
+                    "drop-in API: a CUDA graph per chain of LaunchTensor -> keyswitch_resident -> LaunchCombine "
+                    "-> rescale_resident_raw x2, chains in turn on one stream",
+            "streams16": {"value": ops / (d["streams16_ms"] * 1e-3), "ms_per_step": d["streams16_ms"],
+                          "form": "the same per-chain graphs spread over 16 streams (the reference's N-stream run)"}}
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -799,12 +847,14 @@ def run_gpu(args):
         b.record(g1)
         torch.cuda.synchronize()
         p1ms = a.elapsed_time(b) / reps
-        plain = {"value": pairs / (p1ms * 1e-3), "unit": "ops/s", "ms_per_step": p1ms,
-                 "form": "one chain at a time: one pair per launch set (9 kernels), a CUDA graph per chain, "
-                         "replayed in turn on one stream",
-                 "streams16": {"value": pairs / (pms * 1e-3), "ms_per_step": pms,
-                               "form": "the same per-chain graphs spread over 16 streams"}}
+        plain_fused = {"value": pairs / (p1ms * 1e-3), "unit": "ops/s", "ms_per_step": p1ms,
+                       "form": "this library's fused plan for one pair (9 kernels), a CUDA graph per chain, "
+                               "replayed in turn on one stream",
+                       "streams16": {"value": pairs / (pms * 1e-3), "ms_per_step": pms,
+                                     "form": "the same per-chain graphs spread over 16 streams"}}
         del pgraphs, pplans
+        plain = plain_driver(levels, n, reps, local)
+        plain["fused_single_pair"] = plain_fused
 
     # kernel isolation: 64 polys x 12 towers x 2^16
     ntt = None if args.no_ntt else ntt_isolation(G, torch, dev, local, cur, gen)
@@ -867,6 +917,7 @@ def run_gpu(args):
         "plain": plain,
         "served_vs_plain": (value / world / plain["value"]) if plain else None,
         "served_vs_plain_16streams": (value / world / plain["streams16"]["value"]) if plain else None,
+        "served_vs_plain_fused": (value / world / plain["fused_single_pair"]["value"]) if plain else None,
         "latency_ms": (dict(serving["served"]["latency_ms"], source="serving trace, served form") if serving
                        else {"p50": ms_step, "p99": ms_step, "source": "whole batch per step"}),
         "ntt_kernel_isolation": ntt,

@@ -325,7 +325,8 @@ DeviceKSContext ks_context_create(const KeySwitchConstants& K) {
     };
     for (u64 q : K.qMod) { roots.push_back(root_of(q)); C.modList.push_back(q); }
     for (u64 p : K.pMod) { roots.push_back(root_of(p)); C.modList.push_back(p); }
-    const uint32_t alpha = K.alpha ? K.alpha : (K.sizeQl + K.numPart - 1) / K.numPart;
+    // a digit wider than the level covers all of it: the same partition as alpha = sizeQl
+    const uint32_t alpha = std::min(K.alpha ? K.alpha : (K.sizeQl + K.numPart - 1) / K.numPart, K.sizeQl);
     int dev = 0;
     cudaGetDevice(&dev);
     auto* ctx = new gfx::Context(K.n, K.qMod, K.pMod, alpha, roots, dev);
@@ -406,10 +407,13 @@ void rescale_resident_raw(uint64_t* d_c, uint32_t towers, const DeviceKSContext&
     if (towers > ctx->fullQ()) throw std::runtime_error("rescale_resident_raw: more towers than the context");
     const auto& D = ctx->dev();
     const uint32_t n = C.n;
-    std::vector<u64> ninv(towers), ninvp(towers);
-    ck(cudaMemcpy(ninv.data(), D.ninv, towers * 8, cudaMemcpyDeviceToHost), "ninv");
-    ck(cudaMemcpy(ninvp.data(), D.ninvp, towers * 8, cudaMemcpyDeviceToHost), "ninvp");
     const std::vector<u64>& q = ctx->Q();
+    // n^-1 from the host moduli: no device read, so the call stays capturable
+    std::vector<u64> ninv(towers), ninvp(towers);
+    for (uint32_t t = 0; t < towers; ++t) {
+        ninv[t] = hm::invmod(n, q[t]);
+        ninvp[t] = hm::precon(ninv[t], q[t]);
+    }
     auto fwd = [&](uint32_t t) { return xf::Job{nullptr, D.twf + (size_t)t * n, nullptr, nullptr, q[t], 0, 0}; };
     auto inv = [&](uint32_t t) { return xf::Job{nullptr, D.twi + (size_t)t * n, nullptr, nullptr, q[t], ninv[t], ninvp[t]}; };
     rescale_component(d_c, towers, n, q, s1, s2, d_scratch, d_drop, s, fwd, inv);

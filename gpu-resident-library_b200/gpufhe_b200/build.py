@@ -65,7 +65,28 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
         os.replace(LIB + ".tmp", LIB)
+    build_driver()
     return LIB
+
+
+DRIVER_SRC = os.path.join(PKG, "drivers", "plain_chain.cpp")
+DRIVER = os.path.join(PKG, "drivers", "_build", "plain_chain")
+
+
+def build_driver() -> str:
+    """drivers/plain_chain: the reference's per-chain EvalMult+Rescale driver
+    linked against libgpufhe_b200.so (host code only; rpath to the package)."""
+    if os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(os.path.getmtime(DRIVER_SRC),
+                                                                 os.path.getmtime(LIB)):
+        return DRIVER
+    os.makedirs(os.path.dirname(DRIVER), exist_ok=True)
+    cmd = [NVCC, "-std=c++17", "-O2", "-ccbin", HOSTCXX, f"-I{INCLUDE}", DRIVER_SRC, "-o", DRIVER + ".tmp",
+           f"-L{HERE}", "-lgpufhe_b200", "-Xlinker", "-rpath", "-Xlinker", HERE, "-Wno-deprecated-gpu-targets"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stderr}")
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
 
 
 if __name__ == "__main__":
