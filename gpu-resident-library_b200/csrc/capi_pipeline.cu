@@ -1,4 +1,6 @@
 // extern "C" batched-operation entry points (include/gpufhe_b200.h).
+#include <cuda.h>
+
 #include <memory>
 #include <stdexcept>
 #include <vector>
@@ -106,34 +108,88 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     return k;
 }
 
-int gpufhe_plan_launch_host_async(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
-                                  cudaStream_t s) {
-    if (!plan || !h_in || !h_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+}  // extern "C"
+
+namespace {
+struct Copy {
+    char* dst;
+    const char* src;
+    size_t bytes;
+};
+// Issues the copies in order. With `merge` (the host side is one buffer,
+// walked in order), a copy joins the previous one when both its source and
+// its destination continue the previous ranges and the device side stays
+// inside one device allocation (cuMemGetAddressRange): a batch laid out
+// contiguously on both sides moves in one large copy, which PCIe serves
+// faster than many small ones.
+cudaError_t issue(const std::vector<Copy>& v, cudaMemcpyKind kind, bool merge, cudaStream_t s) {
+    const bool dev_dst = kind == cudaMemcpyHostToDevice;
+    size_t i = 0;
+    while (i < v.size()) {
+        Copy c = v[i++];
+        if (merge) {
+            CUdeviceptr base = 0;
+            size_t size = 0;
+            const char* d0 = dev_dst ? c.dst : c.src;
+            if (cuMemGetAddressRange(&base, &size, (CUdeviceptr)d0) == CUDA_SUCCESS) {
+                const char* dend = (const char*)base + size;
+                while (i < v.size() && v[i].dst == c.dst + c.bytes && v[i].src == c.src + c.bytes &&
+                       (dev_dst ? v[i].dst : v[i].src) + v[i].bytes <= dend)
+                    c.bytes += v[i++].bytes;
+            }
+        }
+        const cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.bytes, kind, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out, const uint64_t* in_buf,
+                uint64_t* out_buf, cudaStream_t s) {
     const pl::Plan& p = *plan->p;
     const size_t n = (size_t)1 << p.logn;
+    const bool batch = in_buf != nullptr;
+    std::vector<Copy> in, out;
+    const char* hin = (const char*)in_buf;
+    char* hout = (char*)out_buf;
     for (size_t i = 0; i < p.ops.size(); ++i) {
         const pl::Op& op = p.ops[i];
         for (int k = 0; k < pl::input_count(op.mode); ++k) {
-            const uint64_t* src = h_in[4 * i + k];
-            if (!src) continue;
-            cudaError_t e = cudaMemcpyAsync((void*)op.in[k], src, op.L * n * 8, cudaMemcpyHostToDevice, s);
-            if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+            const size_t b = op.L * n * 8;
+            const char* src = batch ? hin : (const char*)h_in[4 * i + k];
+            if (batch) hin += b;
+            if (src) in.push_back({(char*)op.in[k], src, b});
         }
-    }
-    pl::tune(*plan->p, s);
-    cudaError_t e = pl::launch(p, s);
-    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
-    for (size_t i = 0; i < p.ops.size(); ++i) {
-        const pl::Op& op = p.ops[i];
         const int nout = op.mode == pl::RESCALE ? 1 : 2;
         for (int k = 0; k < nout; ++k) {
-            uint64_t* dst = h_out[2 * i + k];
-            if (!dst) continue;
-            e = cudaMemcpyAsync(dst, op.out[k], pl::output_towers(op) * n * 8, cudaMemcpyDeviceToHost, s);
-            if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+            const size_t b = pl::output_towers(op) * n * 8;
+            char* dst = batch ? hout : (char*)h_out[2 * i + k];
+            if (batch) hout += b;
+            if (dst) out.push_back({dst, (const char*)op.out[k], b});
         }
     }
+    cudaError_t e = issue(in, cudaMemcpyHostToDevice, batch, s);
+    if (e == cudaSuccess) {
+        pl::tune(*plan->p, s);
+        e = pl::launch(p, s);
+    }
+    if (e == cudaSuccess) e = issue(out, cudaMemcpyDeviceToHost, batch, s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
     return GPUFHE_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int gpufhe_plan_launch_host_async(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
+                                  cudaStream_t s) {
+    if (!plan || !h_in || !h_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    return launch_host(plan, h_in, h_out, nullptr, nullptr, s);
+}
+
+int gpufhe_plan_launch_host_batch_async(gpufhe_plan* plan, const uint64_t* h_in, uint64_t* h_out, cudaStream_t s) {
+    if (!plan || !h_in || !h_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    return launch_host(plan, nullptr, nullptr, h_in, h_out, s);
 }
 
 int gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,

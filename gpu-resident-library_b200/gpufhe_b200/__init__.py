@@ -64,6 +64,7 @@ _API: dict = {
     "gpufhe_plan_launch": (I32, [VP, VP]),
     "gpufhe_plan_destroy": (None, [VP]),
     "gpufhe_run_ops": (I32, [VP, U32, VP, VP]),
+    "gpufhe_plan_launch_host_batch_async": (I32, [VP, VP, VP, VP]),
     "gpufhe_plan_launch_phase": (I32, [VP, U32, VP]),
     "gpufhe_plan_kernel_count": (U32, [VP]),
     "gpufhe_plan_schedule": (U32, [VP]),
@@ -289,6 +290,14 @@ class Plan:
         ao = (VP * len(h_out))(*h_out)
         f = lib().gpufhe_plan_launch_host if sync else lib().gpufhe_plan_launch_host_async
         check(f(self.h, ai, ao, stream))
+
+    def launch_host_batch(self, h_in, h_out, stream=None, sync=True):
+        """h_in / h_out: one pinned host buffer each, all ops' inputs / outputs
+        back to back in op order (gpufhe_plan_launch_host_batch_async)."""
+        check(lib().gpufhe_plan_launch_host_batch_async(self.h, h_in, h_out, stream))
+        if sync:
+            import torch
+            torch.cuda.synchronize()
 
     def close(self):
         if getattr(self, "h", None):

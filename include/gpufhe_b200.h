@@ -237,6 +237,15 @@ int  gpufhe_plan_launch_host(gpufhe_plan* plan, const uint64_t* const* h_in, uin
  * and device->host copies. */
 int  gpufhe_plan_launch_host_async(gpufhe_plan* plan, const uint64_t* const* h_in, uint64_t* const* h_out,
                                    cudaStream_t stream);
+/* Batch form of the above: h_in is one pinned host buffer holding every op's
+ * inputs back to back in op order (each op's input components, level*n words
+ * each), h_out one pinned buffer for all outputs in op order. Where the ops'
+ * device buffers continue each other inside one device allocation, the
+ * copies merge into one transfer each way (large copies reach PCIe's full
+ * rate; a batch of 2-6 MB copies does not). No counterpart in the
+ * reference. */
+int  gpufhe_plan_launch_host_batch_async(gpufhe_plan* plan, const uint64_t* h_in, uint64_t* h_out,
+                                         cudaStream_t stream);
 /* create + launch + synchronize + destroy */
 int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaStream_t stream);
 

@@ -195,3 +195,42 @@ def test_launch_host_sync_and_async(G, S, gctx):
         for j, (e0, e1) in enumerate(want):
             assert np.array_equal(outs_h[2 * j].numpy().view(np.uint64), e0), (sync, j)
             assert np.array_equal(outs_h[2 * j + 1].numpy().view(np.uint64), e1), (sync, j)
+
+
+def test_launch_host_contiguous_batch(G, S, gctx):
+    """gpufhe_plan_launch_host_batch_async: one host buffer per direction,
+    every op's inputs / outputs back to back in op order. With device buffers
+    in the same layout inside one allocation the copies merge (one transfer
+    each way); with separate device allocations they stay piecewise. Both give
+    the oracle's results."""
+    import torch
+    rng = np.random.default_rng(78)
+    n, levels = S.n, [4, 7, 6]
+    cts = [[*S.rand_ct(rng, L), *S.rand_ct(rng, L)] for L in levels]
+    want = [S.octx.evalmult_rescale(L, *c) for L, c in zip(levels, cts)]
+    in_words = [L * n for L in levels for _ in range(4)]
+    out_words = [(L - 1) * n for L in levels for _ in range(2)]
+    offs = lambda ws: [int(o) for o in np.cumsum([0] + ws[:-1])]
+    h_in_buf = torch.from_numpy(np.concatenate([x for c in cts for x in c]).view(np.int64).copy()).pin_memory()
+    h_out_buf = torch.zeros(sum(out_words), dtype=torch.int64).pin_memory()
+    for contiguous in (True, False):
+        if contiguous:
+            d_in, d_out = empty(sum(in_words)), empty(sum(out_words))
+            keep = [d_in, d_out]
+            ip = [ptr(d_in) + 8 * o for o in offs(in_words)]
+            op = [ptr(d_out) + 8 * o for o in offs(out_words)]
+        else:
+            keep = [empty(w) for w in in_words] + [empty(w) for w in out_words]
+            ip = [ptr(t) for t in keep[:len(in_words)]]
+            op = [ptr(t) for t in keep[len(in_words):]]
+        specs = [dict(level=L, inp=ip[4 * j:4 * j + 4], out=op[2 * j:2 * j + 2]) for j, L in enumerate(levels)]
+        plan = G.Plan(gctx, specs)
+        h_out_buf.zero_()
+        plan.launch_host_batch(h_in_buf.data_ptr(), h_out_buf.data_ptr(), None, sync=True)
+        got = h_out_buf.numpy().view(np.uint64)
+        o = offs(out_words)
+        for j, (e0, e1) in enumerate(want):
+            assert np.array_equal(got[o[2 * j]:o[2 * j] + out_words[2 * j]], e0), (contiguous, j)
+            assert np.array_equal(got[o[2 * j + 1]:o[2 * j + 1] + out_words[2 * j + 1]], e1), (contiguous, j)
+        plan.close()
+        del keep
