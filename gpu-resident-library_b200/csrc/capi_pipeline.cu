@@ -122,16 +122,34 @@ struct Copy {
 // inside one device allocation (cuMemGetAddressRange): a batch laid out
 // contiguously on both sides moves in one large copy, which PCIe serves
 // faster than many small ones.
+// cuMemGetAddressRange through the runtime's driver entry point, so that the
+// library carries no link-time dependency on the driver library; null when
+// the entry point is unavailable (copies then stay piecewise).
+using AddrRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+AddrRangeFn addr_range() {
+    static const AddrRangeFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &p, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (AddrRangeFn) nullptr;
+        return (AddrRangeFn)p;
+    }();
+    return fn;
+}
+
 cudaError_t issue(const std::vector<Copy>& v, cudaMemcpyKind kind, bool merge, cudaStream_t s) {
     const bool dev_dst = kind == cudaMemcpyHostToDevice;
+    const AddrRangeFn range = merge ? addr_range() : nullptr;
     size_t i = 0;
     while (i < v.size()) {
         Copy c = v[i++];
-        if (merge) {
+        if (range) {
             CUdeviceptr base = 0;
             size_t size = 0;
             const char* d0 = dev_dst ? c.dst : c.src;
-            if (cuMemGetAddressRange(&base, &size, (CUdeviceptr)d0) == CUDA_SUCCESS) {
+            if (range(&base, &size, (CUdeviceptr)d0) == CUDA_SUCCESS) {
                 const char* dend = (const char*)base + size;
                 while (i < v.size() && v[i].dst == c.dst + c.bytes && v[i].src == c.src + c.bytes &&
                        (dev_dst ? v[i].dst : v[i].src) + v[i].bytes <= dend)

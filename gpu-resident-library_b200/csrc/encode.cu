@@ -13,11 +13,15 @@
 // serves MB sums.
 #include <cmath>
 #include <complex>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "context.hpp"
+#include "encode.h"
 #include "gpufhe_b200.h"
 
 struct gpufhe_encoder {
@@ -196,3 +200,43 @@ int gpufhe_decode_batch(gpufhe_encoder* E, uint32_t count, const int64_t* m, dou
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- reference C++ API
+namespace {
+// One encoder per (device, N) for the process; never freed (the reference's
+// host functions hold no state, so callers expect none to manage).
+gpufhe_encoder* encoder_for(uint32_t N) {
+    static std::mutex mu;
+    static std::map<std::pair<int, uint32_t>, gpufhe_encoder*> cache;
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> g(mu);
+    auto& e = cache[{dev, N}];
+    if (!e && gpufhe_encoder_create(N, dev, &e) != GPUFHE_OK) {
+        e = nullptr;
+        throw std::runtime_error("encode_host: " + gfx::last_error());
+    }
+    return e;
+}
+}  // namespace
+
+namespace gpufhe {
+
+void encode_host(std::vector<int64_t>& m, const std::vector<std::complex<double>>& z, uint32_t N, double Delta) {
+    if (z.size() < N / 2) throw std::invalid_argument("encode_host: z needs N/2 slots");
+    m.assign(N, 0);
+    // std::complex<double> is laid out as two doubles (re, im)
+    if (gpufhe_encode_batch(encoder_for(N), 1, reinterpret_cast<const double*>(z.data()), Delta, m.data(), 0) !=
+        GPUFHE_OK)
+        throw std::runtime_error("encode_host: " + gfx::last_error());
+}
+
+void decode_host(std::vector<std::complex<double>>& z, const std::vector<int64_t>& m, uint32_t N, double Delta) {
+    if (m.size() < N) throw std::invalid_argument("decode_host: m needs N coefficients");
+    z.assign(N / 2, {0.0, 0.0});
+    if (gpufhe_decode_batch(encoder_for(N), 1, m.data(), Delta, reinterpret_cast<double*>(z.data()), 0) !=
+        GPUFHE_OK)
+        throw std::runtime_error("decode_host: " + gfx::last_error());
+}
+
+}  // namespace gpufhe

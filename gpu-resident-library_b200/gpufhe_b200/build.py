@@ -60,7 +60,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [NVCC, *ARCH, "-shared", "-ccbin", HOSTCXX, "-o", LIB + ".tmp", *objs,
-               "-Xlinker", "-Bsymbolic", "-lcuda"]
+               "-Xlinker", "-Bsymbolic"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -5,15 +5,19 @@
 // EvalMult+Rescale output and the keyswitch output to argv[1] (binary) so the
 // Python test can compare them with the CPU oracle bit for bit.
 #include <cuda_runtime.h>
+#include <algorithm>
 
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
+#include <random>
 #include <stdexcept>
 #include <vector>
 
 #include "ckks_ops.h"
 #include "device_ciphertext.h"
+#include "encode.h"
 #include "keygen.h"
 #include "keyswitch.h"
 #include "keyswitch_resident.h"
@@ -192,12 +196,33 @@ int main(int argc, char** argv) {
         gate(thrown, "DeviceCiphertext::upload throws on size mismatch");
     }
 
+    // canonical encode / decode as the reference's tests call them
+    // (test_alpha10.cpp:52-82): seeded slots at scale 2^40
+    std::vector<int64_t> em;
+    std::vector<std::complex<double>> ez(n / 2), dz;
+    {
+        std::mt19937_64 zr(11);
+        std::uniform_real_distribution<double> u(-1.0, 1.0);
+        for (auto& v : ez) {
+            const double re = u(zr);
+            v = {re, u(zr)};
+        }
+        gpufhe::encode_host(em, ez, n, 1099511627776.0);
+        gpufhe::decode_host(dz, em, n, 1099511627776.0);
+        double err = 0;
+        for (uint32_t k = 0; k < n / 2; ++k) err = std::max(err, std::abs(dz[k] - ez[k]));
+        gate(em.size() == n && dz.size() == n / 2 && err < 1e-6, "encode_host / decode_host round trip");
+    }
+
     if (argc > 1) {
         FILE* f = std::fopen(argv[1], "wb");
         std::fwrite(h0.data(), 8, (size_t)(sizeQ - 1) * n, f);
         std::fwrite(h1.data(), 8, (size_t)(sizeQ - 1) * n, f);
         std::fwrite(ks0.data(), 8, T, f);
         std::fwrite(ks1.data(), 8, T, f);
+        std::fwrite(ez.data(), 16, n / 2, f);
+        std::fwrite(em.data(), 8, n, f);
+        std::fwrite(dz.data(), 16, n / 2, f);
         std::fclose(f);
     }
     gpufhe::ks_work_destroy(W);

@@ -48,7 +48,14 @@ def test_cpp_api(tmp_path):
     c0b, c1b = octx.encrypt(L, m2, qA, qB, seed=304)
     data = np.fromfile(out, dtype=np.uint64)
     T1, T = (L - 1) * n, L * n
-    r0, r1, k0, k1 = data[:T1], data[T1:2 * T1], data[2 * T1:2 * T1 + T], data[2 * T1 + T:]
+    r0, r1, k0, k1 = data[:T1], data[T1:2 * T1], data[2 * T1:2 * T1 + T], data[2 * T1 + T:2 * T1 + 2 * T]
+    rest = data[2 * T1 + 2 * T:]
+    ez = rest[:n].view(np.float64).view(np.complex128)
+    em = rest[n:2 * n].view(np.int64)
+    dz = rest[2 * n:3 * n].view(np.float64).view(np.complex128)
+    assert np.array_equal(em, O.encode(ez, n, 2.0 ** 40))         # the reference's encode_host, bit for bit
+    want = O.decode(em, n, 2.0 ** 40)
+    assert np.array_equal(dz.real, want.real) and np.array_equal(dz.imag, want.imag)
     e0, e1 = octx.evalmult_rescale(L, c0a, c1a, c0b, c1b)
     assert np.array_equal(r0, e0) and np.array_equal(r1, e1)
     t2 = np.zeros(T, np.uint64)
