@@ -76,6 +76,9 @@ _API: dict = {
     "gpufhe_rescale_consts": (I32, [VP, VP, VP, U32]),
     "gpufhe_rescale_noalloc": (I32, [VP, U32, VP, VP]),
     "gpufhe_lintrans_bsgs": (I32, [VP, U32, VP, VP, U32, U32, VP, I32, VP, VP, VP]),
+    "gpufhe_lintrans_plan_create": (I32, [VP, U32, VP, VP, U32, U32, VP, I32, VP, VP, C.POINTER(VP)]),
+    "gpufhe_lintrans_plan_launch": (I32, [VP, VP]),
+    "gpufhe_lintrans_plan_destroy": (None, [VP]),
     "gpufhe_rescale_noalloc_max_words": (U64, []),
     "gpufhe_server_create": (I32, [VP, U32, U64, U32, U32, I32, C.POINTER(VP)]),
     "gpufhe_server_destroy": (None, [VP]),

@@ -266,6 +266,20 @@ int  gpufhe_run_ops(gpufhe_ctx* ctx, uint32_t nops, const gpufhe_op* ops, cudaSt
 int gpufhe_lintrans_bsgs(gpufhe_ctx* ctx, uint32_t level, const uint64_t* d_c0, const uint64_t* d_c1, uint32_t n1,
                          uint32_t n2, const uint64_t* const* diag, int hoisted, uint64_t* d_out0, uint64_t* d_out1,
                          cudaStream_t stream);
+/* Plan form of the same transform for repeated use: creation checks the
+ * rotation keys, allocates the scratch, uploads the pointer tables and builds
+ * the baby and giant rotation batches (which keep their keys resident while
+ * the plan lives); launching enqueues the four steps on `stream` with no
+ * allocation and no host transfer, so a launch can be captured in a CUDA graph
+ * and replayed. Input, diagonals and output buffers are fixed at creation.
+ * The reference runs the sequence as separate rotate / multiply / add calls
+ * per step (tests/test_c2s_bsgs.cpp:129-151). */
+typedef struct gpufhe_lintrans_plan gpufhe_lintrans_plan;
+int  gpufhe_lintrans_plan_create(gpufhe_ctx* ctx, uint32_t level, const uint64_t* d_c0, const uint64_t* d_c1,
+                                 uint32_t n1, uint32_t n2, const uint64_t* const* diag, int hoisted,
+                                 uint64_t* d_out0, uint64_t* d_out1, gpufhe_lintrans_plan** out);
+int  gpufhe_lintrans_plan_launch(gpufhe_lintrans_plan* plan, cudaStream_t stream);
+void gpufhe_lintrans_plan_destroy(gpufhe_lintrans_plan* plan);
 
 /* ---------------------------------------------------------------- no allocation
  * No counterpart in the reference. Rescale of one eval-form component
