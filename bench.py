@@ -533,6 +533,12 @@ def keys_and_encryption(G, torch, dev, ctx, galois, cts):
     t9 = clock()
     zd = enc.decode(em, 2.0 ** 40)
     t10 = clock()
+    enc.encode(z[:1], 2.0 ** 40, fast=True)
+    t11 = clock()
+    emf = enc.encode(z, 2.0 ** 40, fast=True)
+    t12 = clock()
+    enc.decode(em, 2.0 ** 40, fast=True)
+    t13 = clock()
     enc.close()
     return {"params": f"N=2^{N_LOG}, {L}+{ctx.K} towers, dnum={-(-ctx.fullQ // ctx.alpha)}, sigma=3.19, "
                       f"uniform ternary secret",
@@ -546,7 +552,13 @@ def keys_and_encryption(G, torch, dev, ctx, galois, cts):
                        "encodes_per_s": ENC_COUNT / (t9 - t8), "decodes_per_s": ENC_COUNT / (t10 - t9),
                        "round_trip_max_err": float(np.abs(zd - z).max()),
                        "form": "the reference's O(N^2) sums in its order, bit-identical, one thread per "
-                               "output index, 4 messages per thread"}}
+                               "output index, 4 messages per thread",
+                       "fast": {"encode_ms": (t12 - t11) * 1e3, "decode_ms": (t13 - t12) * 1e3,
+                                "encodes_per_s": ENC_COUNT / (t12 - t11), "decodes_per_s": ENC_COUNT / (t13 - t12),
+                                "max_coeff_diff_vs_exact": int(np.abs(emf - em).max()),
+                                "coeffs_differing": float((emf != em).mean()),
+                                "form": "O(N log N) transform over the rotation group, radix-2 stages over the "
+                                        "batch (coefficients within one of the reference's)"}}}
 
 
 def rotation_batch(G, torch, dev, local, gen, steps):

@@ -11,6 +11,7 @@
 // decodings equal the reference's bit for bit. A thread carries up to MB
 // messages of a batch, so each twiddle gather (from the 2N-entry table in L2)
 // serves MB sums.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <map>
@@ -30,6 +31,7 @@ struct gpufhe_encoder {
     double2* tw_enc = nullptr;   // [2n] polar(1, -pi t / n)
     double2* tw_dec = nullptr;   // [2n] polar(1, +pi t / n)
     uint32_t* r = nullptr;       // [n/2] 5^k mod 2n
+    double2* ksi = nullptr;      // [2n] exp(2 pi i t / 2n), the fast transform's roots
 };
 
 namespace {
@@ -98,6 +100,90 @@ __global__ void __launch_bounds__(ENT) k_decode(const double2* __restrict__ tw, 
         if (b < (int)nb) z[(size_t)(b0 + b) * S + k] = make_double2(__ddiv_rn(ar[b], delta), __ddiv_rn(ai[b], delta));
 }
 
+// ---------------------------------------------------------------- fast form
+// The same maps by an O(n log n) transform over the rotation group (the
+// "special" FFT of CKKS encoders): with S = n/2 and u_j = m_j + i m_{j+S},
+//   decode: z_k = (sum_{j<S} u_j zeta^{j r_k}) / Delta, zeta = exp(i pi / n),
+//   encode: u_j = (1/S) sum_k z_k zeta^{-j r_k}, m_j = Re u_j Delta,
+//           m_{j+S} = Im u_j Delta,
+// because zeta^{S r_k} = i for r_k = 1 mod 4. Radix-2 stages over the whole
+// batch, one launch each (the batch stays in L2 between stages). Rounding
+// differs from the reference's direct sums: coefficients may differ by one.
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+
+__global__ void k_bitrev(const double2* __restrict__ in, double2* __restrict__ out, uint32_t logS, size_t total) {
+    const uint32_t S = 1u << logS;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = i >> logS;
+        const uint32_t k = (uint32_t)(i & (S - 1));
+        out[i] = in[(b << logS) + (__brev(k) >> (32 - logS))];
+    }
+}
+
+// One stage of the forward (decode) transform, block length len:
+// (u, v) -> (u + v ksi[(r_j mod 4 len) 2n / (4 len)], u - v ksi[...]).
+__global__ void k_sfft_stage(double2* __restrict__ v, const uint32_t* __restrict__ r,
+                             const double2* __restrict__ ksi, uint32_t logS, uint32_t len, uint32_t M,
+                             size_t total) {
+    const uint32_t lenh = len >> 1, lenq = len << 2;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = t >> (logS - 1);
+        const uint32_t q = (uint32_t)(t & ((1u << (logS - 1)) - 1));
+        const uint32_t j = q % lenh, i = (q / lenh) * len;
+        double2* w = v + (b << logS) + i + j;
+        const double2 a = w[0], c = cmul(w[lenh], __ldg(ksi + (size_t)(r[j] % lenq) * (M / lenq)));
+        w[0] = make_double2(a.x + c.x, a.y + c.y);
+        w[lenh] = make_double2(a.x - c.x, a.y - c.y);
+    }
+}
+
+// One stage of the inverse (encode) transform:
+// (u, v) -> (u + v, (u - v) ksi[(4 len - r_j mod 4 len) 2n / (4 len)]).
+__global__ void k_sfft_inv_stage(double2* __restrict__ v, const uint32_t* __restrict__ r,
+                                 const double2* __restrict__ ksi, uint32_t logS, uint32_t len, uint32_t M,
+                                 size_t total) {
+    const uint32_t lenh = len >> 1, lenq = len << 2;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = t >> (logS - 1);
+        const uint32_t q = (uint32_t)(t & ((1u << (logS - 1)) - 1));
+        const uint32_t j = q % lenh, i = (q / lenh) * len;
+        double2* w = v + (b << logS) + i + j;
+        const double2 a = w[0], c = w[lenh];
+        w[0] = make_double2(a.x + c.x, a.y + c.y);
+        w[lenh] = cmul(make_double2(a.x - c.x, a.y - c.y),
+                       __ldg(ksi + (size_t)(lenq - r[j] % lenq) * (M / lenq)));
+    }
+}
+
+// m_j = llround(Re u_j * sc), m_{j+S} = llround(Im u_j * sc), sc = Delta / S.
+__global__ void k_fast_encode_out(const double2* __restrict__ u, int64_t* __restrict__ m, uint32_t logS, double sc,
+                                  size_t total) {
+    const uint32_t S = 1u << logS;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = i >> logS;
+        const uint32_t j = (uint32_t)(i & (S - 1));
+        const double2 x = u[i];
+        m[(b << (logS + 1)) + j] = llround(x.x * sc);
+        m[(b << (logS + 1)) + S + j] = llround(x.y * sc);
+    }
+}
+
+// u_j = (m_j + i m_{j+S}) / Delta
+__global__ void k_fast_decode_in(const int64_t* __restrict__ m, double2* __restrict__ u, uint32_t logS,
+                                 double inv_delta, size_t total) {
+    const uint32_t S = 1u << logS;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = i >> logS;
+        const uint32_t j = (uint32_t)(i & (S - 1));
+        u[i] = make_double2((double)m[(b << (logS + 1)) + j] * inv_delta,
+                            (double)m[(b << (logS + 1)) + S + j] * inv_delta);
+    }
+}
+
+unsigned grid_of(size_t work) { return (unsigned)std::min<size_t>((work + 255) / 256, 148u * 32u); }
+
 }  // namespace
 
 extern "C" {
@@ -127,6 +213,13 @@ int gpufhe_encoder_create(uint32_t n, int device, gpufhe_encoder** out) {
         std::vector<uint32_t> r(S);
         uint64_t rk = 1;
         for (uint32_t k = 0; k < S; ++k) { r[k] = (uint32_t)rk; rk = (rk * 5) % M; }
+        std::vector<double2> ks(M);
+        for (uint32_t t = 0; t < M; ++t) {
+            const std::complex<double> w = std::polar(1.0, M_PI * (double)t / (double)n);
+            ks[t] = make_double2(w.real(), w.imag());
+        }
+        ck(cudaMalloc(&E->ksi, M * sizeof(double2)), "cudaMalloc");
+        ck(cudaMemcpy(E->ksi, ks.data(), M * sizeof(double2), cudaMemcpyHostToDevice), "upload");
         ck(cudaMalloc(&E->tw_enc, M * sizeof(double2)), "cudaMalloc");
         ck(cudaMalloc(&E->tw_dec, M * sizeof(double2)), "cudaMalloc");
         ck(cudaMalloc(&E->r, S * sizeof(uint32_t)), "cudaMalloc");
@@ -149,7 +242,68 @@ void gpufhe_encoder_destroy(gpufhe_encoder* E) {
     cudaFree(E->tw_enc);
     cudaFree(E->tw_dec);
     cudaFree(E->r);
+    cudaFree(E->ksi);
     delete E;
+}
+
+int gpufhe_encode_batch_fast(gpufhe_encoder* E, uint32_t count, const double* z, double delta, int64_t* m,
+                             cudaStream_t s) {
+    if (!E || !z || !m) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    if (!count) return GPUFHE_OK;
+    const uint32_t n = E->n, S = n / 2, M = 2 * n;
+    uint32_t logS = 0;
+    while ((1u << logS) < S) ++logS;
+    if (logS < 1) { gfx::set_error("gpufhe_encode_batch_fast: n must be at least 4"); return GPUFHE_EINVAL; }
+    const size_t words = (size_t)count * S;
+    double2 *a = nullptr, *b = nullptr;
+    int64_t* dm = nullptr;
+    cudaError_t e = cudaMallocAsync(&a, words * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&b, words * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dm, (size_t)count * n * 8, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a, z, words * sizeof(double2), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        for (uint32_t len = S; len >= 2; len >>= 1)
+            k_sfft_inv_stage<<<grid_of(words / 2), 256, 0, s>>>(a, E->r, E->ksi, logS, len, M, words / 2);
+        k_bitrev<<<grid_of(words), 256, 0, s>>>(a, b, logS, words);
+        k_fast_encode_out<<<grid_of(words), 256, 0, s>>>(b, dm, logS, delta / (double)S, words);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m, dm, (size_t)count * n * 8, cudaMemcpyDeviceToHost, s);
+    for (void* p : {(void*)a, (void*)b, (void*)dm})
+        if (p) cudaFreeAsync(p, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
+}
+
+int gpufhe_decode_batch_fast(gpufhe_encoder* E, uint32_t count, const int64_t* m, double delta, double* z,
+                             cudaStream_t s) {
+    if (!E || !z || !m) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    if (!count) return GPUFHE_OK;
+    const uint32_t n = E->n, S = n / 2, M = 2 * n;
+    uint32_t logS = 0;
+    while ((1u << logS) < S) ++logS;
+    if (logS < 1) { gfx::set_error("gpufhe_decode_batch_fast: n must be at least 4"); return GPUFHE_EINVAL; }
+    const size_t words = (size_t)count * S;
+    double2 *a = nullptr, *b = nullptr;
+    int64_t* dm = nullptr;
+    cudaError_t e = cudaMallocAsync(&a, words * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&b, words * sizeof(double2), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&dm, (size_t)count * n * 8, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dm, m, (size_t)count * n * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        k_fast_decode_in<<<grid_of(words), 256, 0, s>>>(dm, a, logS, 1.0 / delta, words);
+        k_bitrev<<<grid_of(words), 256, 0, s>>>(a, b, logS, words);
+        for (uint32_t len = 2; len <= S; len <<= 1)
+            k_sfft_stage<<<grid_of(words / 2), 256, 0, s>>>(b, E->r, E->ksi, logS, len, M, words / 2);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(z, b, words * sizeof(double2), cudaMemcpyDeviceToHost, s);
+    for (void* p : {(void*)a, (void*)b, (void*)dm})
+        if (p) cudaFreeAsync(p, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+    return GPUFHE_OK;
 }
 
 int gpufhe_encode_batch(gpufhe_encoder* E, uint32_t count, const double* z, double delta, int64_t* m,

@@ -55,6 +55,8 @@ _API: dict = {
     "gpufhe_encoder_destroy": (None, [VP]),
     "gpufhe_encode_batch": (I32, [VP, U32, VP, C.c_double, VP, VP]),
     "gpufhe_decode_batch": (I32, [VP, U32, VP, C.c_double, VP, VP]),
+    "gpufhe_encode_batch_fast": (I32, [VP, U32, VP, C.c_double, VP, VP]),
+    "gpufhe_decode_batch_fast": (I32, [VP, U32, VP, C.c_double, VP, VP]),
     "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
     "gpufhe_ntt_job_bytes": (U64, []),
     "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),
@@ -166,23 +168,26 @@ class Encoder:
         except Exception:
             pass
 
-    def encode(self, z, delta):
-        """z: [count][n/2] or [n/2] complex -> int64 [count][n] (or [n])."""
+    def encode(self, z, delta, fast=False):
+        """z: [count][n/2] or [n/2] complex -> int64 [count][n] (or [n]).
+        fast: the O(n log n) form (coefficients within one of the reference's)."""
         import numpy as np
         z = np.asarray(z, dtype=np.complex128)
         one = z.ndim == 1
         z = np.ascontiguousarray(z.reshape(-1, self.n // 2))
         m = np.zeros((z.shape[0], self.n), np.int64)
-        check(lib().gpufhe_encode_batch(self.h, z.shape[0], z.ctypes.data, float(delta), m.ctypes.data, None))
+        f = lib().gpufhe_encode_batch_fast if fast else lib().gpufhe_encode_batch
+        check(f(self.h, z.shape[0], z.ctypes.data, float(delta), m.ctypes.data, None))
         return m[0] if one else m
 
-    def decode(self, m, delta):
+    def decode(self, m, delta, fast=False):
         import numpy as np
         m = np.asarray(m, dtype=np.int64)
         one = m.ndim == 1
         m = np.ascontiguousarray(m.reshape(-1, self.n))
         z = np.zeros((m.shape[0], self.n // 2), np.complex128)
-        check(lib().gpufhe_decode_batch(self.h, m.shape[0], m.ctypes.data, float(delta), z.ctypes.data, None))
+        f = lib().gpufhe_decode_batch_fast if fast else lib().gpufhe_decode_batch
+        check(f(self.h, m.shape[0], m.ctypes.data, float(delta), z.ctypes.data, None))
         return z[0] if one else z
 
 

@@ -129,6 +129,16 @@ int  gpufhe_encode_batch(gpufhe_encoder* enc, uint32_t count, const double* z, d
                          cudaStream_t stream);
 int  gpufhe_decode_batch(gpufhe_encoder* enc, uint32_t count, const int64_t* m, double delta, double* z,
                          cudaStream_t stream);
+/* The same maps by an O(n log n) transform over the rotation group instead
+ * of the reference's O(n^2) sums (no counterpart in the reference): encoded
+ * coefficients equal the reference's or differ by one where the exact value
+ * lies within rounding error of a half-integer; decoded slots agree to
+ * about n * 2^-52 relative. For serving paths where encoding would otherwise
+ * cost more than encryption. */
+int  gpufhe_encode_batch_fast(gpufhe_encoder* enc, uint32_t count, const double* z, double delta, int64_t* m,
+                              cudaStream_t stream);
+int  gpufhe_decode_batch_fast(gpufhe_encoder* enc, uint32_t count, const int64_t* m, double delta, double* z,
+                              cudaStream_t stream);
 
 /* ---------------------------------------------------------------- parameters
  * C forms of the reference's native parameter routines (include/params.h;

@@ -49,3 +49,25 @@ def test_encode_full_ring_round_trip():
     want = O.decode(m[2], n, d)
     assert np.array_equal(zd[2].real, want.real) and np.array_equal(zd[2].imag, want.imag)
     assert np.abs(zd - z).max() <= n / (2 * d)
+
+
+@pytest.mark.parametrize("n,count,dbits", [(4, 3, 10), (1024, 5, 40), (16384, 2, 40), (65536, 3, 40)])
+def test_fast_encode_decode(n, count, dbits):
+    """O(n log n) form: coefficients equal the reference's sums or differ by
+    one (rounding of a value within floating-point error of a half-integer);
+    decoded slots agree with the reference's decode to n * 2^-52 relative."""
+    import gpufhe_b200 as G
+    E = G.Encoder(n)
+    z = slots(np.random.default_rng(7 * n + count), n, count)
+    d = float(2.0 ** dbits)
+    mf = E.encode(z, d, fast=True)
+    me = E.encode(z, d)   # the exact form (bit-identical to the reference, checked above)
+    diff = np.abs(mf - me)
+    assert diff.max() <= 1, diff.max()
+    assert (diff != 0).mean() < 0.2
+    zf = E.decode(me, d, fast=True)
+    ze = E.decode(me, d)
+    scale = max(1.0, float(np.abs(ze).max()))
+    assert np.abs(zf - ze).max() <= n * 2.0 ** -52 * scale * 64
+    if n <= 1024:
+        assert np.array_equal(me[0], O.encode(z[0], n, d))
