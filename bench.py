@@ -865,15 +865,10 @@ def run_gpu(args):
         plain = plain_driver(levels, n, reps, local)
         plain["fused_single_pair"] = plain_fused
 
-    # kernel isolation: 64 polys x 12 towers x 2^16
-    ntt = None if args.no_ntt else ntt_isolation(G, torch, dev, local, cur, gen)
-
-    # rotation batch (plain and hoisted)
-    rotation = None
-    if not args.no_rot:
-        rotation = rotation_batch(G, torch, dev, local, gen, max(3, min(args.steps, 10)))
-
-    # serving trace (continuous batching vs one request at a time)
+    # serving trace (continuous batching vs one request at a time), right after
+    # the step it serves and before the isolation and rotation sections (run
+    # after the rotation section, with its key generation and encryptions, the
+    # trace measured 10-15% slower; the cause is not isolated)
     serving = None
     if not args.no_serve:
         del plan, ws, ins, outs, keep
@@ -881,6 +876,14 @@ def run_gpu(args):
         torch.cuda.empty_cache()
         free_b, _ = torch.cuda.mem_get_info(dev)
         serving = run_serving(G, local, args.serve_requests, free_b, dist, dev)
+
+    # kernel isolation: 64 polys x 12 towers x 2^16
+    ntt = None if args.no_ntt else ntt_isolation(G, torch, dev, local, cur, gen)
+
+    # rotation batch (plain and hoisted)
+    rotation = None
+    if not args.no_rot:
+        rotation = rotation_batch(G, torch, dev, local, gen, max(3, min(args.steps, 10)))
 
     # CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
     cpu = None
