@@ -177,6 +177,12 @@ SERVE_LOGNS = (14, 15, 16)
 SERVE_TOWERS, SERVE_K, SERVE_ALPHA = 24, 8, 8          # dnum = 3 at 24 towers
 SERVE_RATE = 2000.0                                     # Poisson arrivals, requests/s
 SERVE_ROT_STEPS = (1, 2, 4, 8, -1, -2, -4, -8)
+# Admission cap of the served form: at most this many requests active at once.
+# The trace offers more work than the GPU serves (about 18k operations in its
+# first second); with no cap some runs admitted over 500 requests and dropped
+# to 10.7-14.3k ops/s with p50 up to 690 ms, while at 384 repeated runs held
+# 15.7-15.8k ops/s and p50 160-180 ms.
+SERVE_MAX_ACTIVE = 384
 SERVE_WORKLOAD = ("serving trace: Poisson arrivals at 2000 req/s (seeded); per request N in {2^14,2^15,2^16}, "
                   "towers U[4,24], depth U[1,10] of EvalMult+Rescale (capped at towers-1) with U[0,8] rotations "
                   "by +-{1,2,4,8} interleaved; Q=1x60+23x50-bit, P=8x60-bit, alpha=8 (dnum=3)")
@@ -224,7 +230,7 @@ def serving_trace(count, seed):
 
 
 def serve(G, ctxs, reqs, budget, plain):
-    srv = G.Server(ctxs, budget, plain=plain)
+    srv = G.Server(ctxs, budget, max_active=0 if plain else SERVE_MAX_ACTIVE, plain=plain)
     tuned = srv.tune(512)                 # schedules per context and batch class, before the trace
     for i, (c, L, ops, t) in enumerate(reqs):
         srv.submit(c, L, ops, arrival_s=t, seed=SEED + i)
@@ -267,6 +273,8 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
         c.close()
     out = {"workload": SERVE_WORKLOAD, "requests": count, "requests_this_rank": len(reqs),
            "hbm_budget_bytes": budget, "inputs": "seeded residues generated on the device at admission",
+           "admission": f"served form: FIFO, at most {SERVE_MAX_ACTIVE} requests active at once; plain form: one "
+                        "request at a time",
            "served": served, "plain": plain, "served_vs_plain_ops": served["ops_per_s"] / plain["ops_per_s"]}
     if dist is not None:
         # whole-job rates: all ranks' operations over the slowest rank's busy time
@@ -866,9 +874,7 @@ def run_gpu(args):
         plain["fused_single_pair"] = plain_fused
 
     # serving trace (continuous batching vs one request at a time), right after
-    # the step it serves and before the isolation and rotation sections (run
-    # after the rotation section, with its key generation and encryptions, the
-    # trace measured 10-15% slower; the cause is not isolated)
+    # the step it serves
     serving = None
     if not args.no_serve:
         del plan, ws, ins, outs, keep
