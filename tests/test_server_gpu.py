@@ -56,9 +56,9 @@ def final_level(r):
     return r["level"] - sum(1 for m, _ in r["ops"] if m == EMR)
 
 
-def run(G, gctxs, setups, reqs, plain=False, budget=None, seeded=False, tune=0):
+def run(G, gctxs, setups, reqs, plain=False, budget=None, seeded=False, tune=0, max_active=0):
     resident = sum(g.resident_bytes() for g in gctxs)
-    srv = G.Server(gctxs, budget or resident + (1 << 30), plain=plain)
+    srv = G.Server(gctxs, budget or resident + (1 << 30), max_active=max_active, plain=plain)
     if tune:
         assert srv.tune(tune) > 0
     outs = []
@@ -122,6 +122,22 @@ def test_budget_admission(G, setups, gctxs):
     assert st["peak_active"] < len(reqs)         # admission waited for memory
     for i in range(len(reqs)):
         assert np.array_equal(small[i], big[i]), i
+
+
+def test_active_cap(G, setups, gctxs):
+    """max_active bounds the requests admitted at once (the bench's served
+    form runs with a cap); the results are the same bits as uncapped."""
+    reqs = make_trace(setups, 12, seed=21)
+    for r in reqs:
+        r["arrival"] = 0.0
+    capped, st, rec = run(G, gctxs, setups, reqs, max_active=3)
+    free, _, _ = run(G, gctxs, setups, reqs)
+    assert st["completed"] == len(reqs) and st["peak_active"] == 3 and st["max_batch"] > 1
+    for i in range(len(reqs)):
+        assert np.array_equal(capped[i], free[i]), i
+    admits = sorted(x["t_admit"] for x in rec)
+    finishes = sorted(x["t_finish"] for x in rec)
+    assert admits[3] >= finishes[0] - 1e-3     # the fourth admission waited for a finish
 
 
 def test_seeded_inputs_same_alone_and_mixed(G, setups, gctxs):
