@@ -2,12 +2,16 @@
 // DeviceCiphertext, DeviceTables / mul_resident / rescale_resident,
 // KeySwitchConstants / compute_keyswitch_constants / keyswitch_core_resident,
 // DeviceKSContext / DeviceKSWork / keyswitch_resident / rescale_resident_raw,
-// rotation, and the host keygen / evalkeygen / encrypt / decrypt harness.
+// rotation, the host keygen / evalkeygen / encrypt / decrypt harness, and the
+// headerless host-vector helpers (automorphism, plaintext embedding,
+// pointwise ciphertext ops).
 // Same names, arguments, results and error behaviour (std::runtime_error on
 // CUDA failures and unknown moduli) as the reference headers they replace.
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <random>
 #include <stdexcept>
@@ -18,6 +22,7 @@
 #include "ckks_ops.h"
 #include "context.hpp"
 #include "device_ciphertext.h"
+#include "host_ops.h"
 #include "hostmath.hpp"
 #include "keygen.h"
 #include "keyswitch.h"
@@ -68,13 +73,48 @@ __global__ void k_switch_copy(u64* __restrict__ dst, const u64* __restrict__ src
     }
 }
 
-// out[j] = in[sigma slot] for one eval-form tower
+// out[j] = in[sigma slot] for eval-form towers (blockIdx.y = tower)
 __global__ void k_galois_gather(u64* __restrict__ out, const u64* __restrict__ in, uint32_t logn, u64 k) {
     const uint32_t n = 1u << logn;
+    out += (size_t)blockIdx.y << logn;
+    in += (size_t)blockIdx.y << logn;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const uint32_t e = 2 * (__brev(j) >> (32 - logn)) + 1;
         const uint32_t t = (uint32_t)(((u64)e * k) & (2ull * n - 1));
         out[j] = in[__brev((t - 1) >> 1) >> (32 - logn)];
+    }
+}
+
+// c = c (+) d per tower (blockIdx.y = tower) for both components: the
+// reference's add, s = a + b then s - q when s >= q (ptops.cpp:11, 13-18), or
+// its exact product (a * b) mod q (ptops.cpp:10, 20-26); operands are reduced
+// first so the product is exact for any 64-bit words.
+__global__ void k_pointwise(u64* __restrict__ c0, u64* __restrict__ c1, const u64* __restrict__ d0,
+                            const u64* __restrict__ d1, const ModC* __restrict__ mods, uint32_t n, int mul) {
+    const ModC m = mods[blockIdx.y];
+    const size_t base = (size_t)blockIdx.y * n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const size_t x = base + k;
+        if (mul) {
+            c0[x] = mulmod(reduce64(c0[x], m), reduce64(d0[x], m), m);
+            c1[x] = mulmod(reduce64(c1[x], m), reduce64(d1[x], m), m);
+        } else {
+            const u64 s0 = c0[x] + d0[x], s1 = c1[x] + d1[x];
+            c0[x] = s0 >= m.q ? s0 - m.q : s0;
+            c1[x] = s1 >= m.q ? s1 - m.q : s1;
+        }
+    }
+}
+
+// out[t][k] = ((m[k] % q_t) + q_t) % q_t in signed 64-bit arithmetic, the
+// reference's embedding of an integer-coefficient plaintext (rotate.cpp:108-110).
+__global__ void k_embed_towers(u64* __restrict__ out, const int64_t* __restrict__ m, const ModC* __restrict__ mods,
+                               uint32_t n) {
+    const long long q = (long long)mods[blockIdx.y].q;
+    u64* o = out + (size_t)blockIdx.y * n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const long long v = (long long)m[k];
+        o[k] = (u64)((v % q + q) % q);
     }
 }
 
@@ -133,21 +173,92 @@ TabEntry tables_for(uint32_t n, u64 q, u64 root) {
     return e;
 }
 
-// Transforms every tower of a host [towers][n] array (tower t mod[t]).
-void host_xform(std::vector<u64>& h, uint32_t towers, uint32_t n, const std::vector<u64>& mod,
-                const std::vector<u64>& root, bool inverse) {
-    u64* d = dup_to_device(h);
+// Per-device staging for the host-vector helpers, grown on demand and kept
+// for the process: the reference calls them once per diagonal of a linear
+// transform, where a cudaMalloc / cudaFree pair per call would dominate.
+// A helper holds the device's lock from upload to download.
+struct Staging {
+    std::mutex mu;
+    char* p = nullptr;
+    size_t cap = 0;
+};
+std::mutex g_stage_map_mu;
+std::map<int, std::unique_ptr<Staging>> g_stage;
+
+struct StageLease {
+    std::unique_lock<std::mutex> lk;
+    char* base;
+    size_t off = 0;
+    // Next 256-byte aligned region of `bytes`.
+    template <class T>
+    T* take(size_t count) {
+        T* r = reinterpret_cast<T*>(base + off);
+        off += (count * sizeof(T) + 255) & ~(size_t)255;
+        return r;
+    }
+};
+
+// Total bytes of regions of the given sizes as StageLease::take lays them out.
+size_t stage_bytes(std::initializer_list<size_t> sizes) {
+    size_t t = 0;
+    for (size_t b : sizes) t += (b + 255) & ~(size_t)255;
+    return t;
+}
+
+StageLease stage(size_t bytes) {
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    Staging* st;
+    {
+        std::lock_guard<std::mutex> g(g_stage_map_mu);
+        auto& slot = g_stage[dev];
+        if (!slot) slot.reset(new Staging);
+        st = slot.get();
+    }
+    std::unique_lock<std::mutex> lk(st->mu);
+    if (bytes > st->cap) {
+        if (st->p) ck(cudaFree(st->p), "cudaFree");
+        st->p = nullptr;
+        st->cap = 0;
+        ck(cudaMalloc(&st->p, bytes), "cudaMalloc");
+        st->cap = bytes;
+    }
+    return StageLease{std::move(lk), st->p};
+}
+
+// Fills `jobs` with the transform of every tower of d ([towers][n], tower t
+// mod[t]) and launches it in one batched launch per pass on stream 0.
+void launch_xform(u64* d, xf::Job* d_jobs, uint32_t towers, uint32_t n, const std::vector<u64>& mod,
+                  const std::vector<u64>& root, bool inverse) {
     std::vector<xf::Job> jobs(towers);
     for (uint32_t t = 0; t < towers; ++t) {
         TabEntry e = tables_for(n, mod[t], root[t]);
         jobs[t] = xf::Job{d + (size_t)t * n, inverse ? e.i : e.f, nullptr, nullptr, mod[t], e.ninv, e.ninvp};
     }
-    xf::Job* dj = dup_to_device(jobs);
-    ck(xf_launch_ntt(dj, nullptr, (int)towers, hm::ilog2(n), inverse, 0), "transform");
-    ck(cudaDeviceSynchronize(), "sync");
-    ck(cudaMemcpy(h.data(), d, h.size() * 8, cudaMemcpyDeviceToHost), "download");
-    cudaFree(dj);
-    cudaFree(d);
+    ck(cudaMemcpy(d_jobs, jobs.data(), towers * sizeof(xf::Job), cudaMemcpyHostToDevice), "upload");
+    ck(xf_launch_ntt(d_jobs, nullptr, (int)towers, hm::ilog2(n), inverse, 0), "transform");
+}
+
+std::vector<ModC> modcs(const std::vector<u64>& mod, uint32_t towers) {
+    std::vector<ModC> m(towers);
+    for (uint32_t t = 0; t < towers; ++t) m[t] = hm::modc(mod[t]);
+    return m;
+}
+
+void need(bool ok, const char* what) {
+    if (!ok) throw std::invalid_argument(std::string("gpufhe: ") + what);
+}
+
+// Transforms every tower of a host [towers][n] array (tower t mod[t]).
+void host_xform(std::vector<u64>& h, uint32_t towers, uint32_t n, const std::vector<u64>& mod,
+                const std::vector<u64>& root, bool inverse) {
+    const size_t T = (size_t)towers * n;
+    StageLease L = stage(stage_bytes({towers * sizeof(xf::Job), T * 8}));
+    xf::Job* dj = L.take<xf::Job>(towers);
+    u64* d = L.take<u64>(T);
+    ck(cudaMemcpy(d, h.data(), T * 8, cudaMemcpyHostToDevice), "upload");
+    launch_xform(d, dj, towers, n, mod, root, inverse);
+    ck(cudaMemcpy(h.data(), d, T * 8, cudaMemcpyDeviceToHost), "download");
 }
 
 inline u64 emb(long v, u64 q) { return (u64)((v % (long)q + (long)q) % (long)q); }
@@ -475,9 +586,11 @@ void rotate_ct_device(uint64_t* d_c0, uint64_t* d_c1, uint32_t k, const DeviceKS
 void rotate_ct_resident(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, uint32_t k,
                         const KeySwitchConstants& Krot, uint32_t towers, uint32_t n, const std::vector<uint64_t>& mod,
                         const std::vector<uint64_t>& root) {
+    const size_t T = (size_t)towers * n;
+    need(c0.size() >= T && c1.size() >= T, "rotate_ct_resident: ciphertext shorter than towers*n");
+    c1.resize(T);
     DeviceKSContext C = ks_context_create(Krot);
     DeviceKSWork W = ks_work_create(C);
-    const size_t T = (size_t)towers * n;
     u64 *d0 = dup_to_device(c0), *d1 = dup_to_device(c1), *b0 = nullptr, *b1 = nullptr;
     ck(cudaMalloc(&b0, T * 8), "cudaMalloc");
     ck(cudaMalloc(&b1, T * 8), "cudaMalloc");
@@ -488,6 +601,99 @@ void rotate_ct_resident(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, ui
     cudaFree(d0); cudaFree(d1); cudaFree(b0); cudaFree(b1);
     ks_work_destroy(W);
     ks_context_destroy(C);
+}
+
+// ---------------------------------------------------------------- host-vector helpers
+// Functions the reference defines without a header (rotate.cpp:87-112,
+// 176-188, ptops.cpp:13-26) and its tests declare where they call them.
+// Each stages its operands through the device's staging buffer, runs one
+// batched launch per step over all towers, and copies the result back.
+
+void automorphism_eval_host(std::vector<uint64_t>& v, uint32_t towers, uint32_t n, uint32_t k,
+                            const std::vector<uint64_t>&, const std::vector<uint64_t>&) {
+    const size_t T = (size_t)towers * n;
+    need(hm::is_pow2(n) && n >= 2, "automorphism_eval_host: n must be a power of two");
+    need(k & 1, "automorphism_eval_host: Galois element must be odd");
+    need(v.size() >= T, "automorphism_eval_host: vector shorter than towers*n");
+    v.resize(T);
+    if (!T) return;
+    StageLease L = stage(stage_bytes({T * 8, T * 8}));
+    u64* din = L.take<u64>(T);
+    u64* dout = L.take<u64>(T);
+    ck(cudaMemcpy(din, v.data(), T * 8, cudaMemcpyHostToDevice), "upload");
+    k_galois_gather<<<dim3(grid_for(n), towers), 256>>>(dout, din, (uint32_t)hm::ilog2(n), k);
+    ck(cudaGetLastError(), "automorphism");
+    ck(cudaMemcpy(v.data(), dout, T * 8, cudaMemcpyDeviceToHost), "download");
+}
+
+void pt_to_eval_host(std::vector<uint64_t>& out, const std::vector<int64_t>& m, uint32_t towers, uint32_t n,
+                     const std::vector<uint64_t>& mod, const std::vector<uint64_t>& root) {
+    const size_t T = (size_t)towers * n;
+    need(xf_supported_logn(hm::ilog2(n)) && hm::is_pow2(n), "pt_to_eval_host: unsupported ring size");
+    need(m.size() >= n && mod.size() >= towers && root.size() >= towers, "pt_to_eval_host: short input");
+    out.resize(T);
+    if (!T) return;
+    const std::vector<ModC> mc = modcs(mod, towers);
+    StageLease L = stage(stage_bytes({towers * sizeof(xf::Job), towers * sizeof(ModC), (size_t)n * 8, T * 8}));
+    xf::Job* dj = L.take<xf::Job>(towers);
+    ModC* dm = L.take<ModC>(towers);
+    int64_t* dmsg = L.take<int64_t>(n);
+    u64* d = L.take<u64>(T);
+    ck(cudaMemcpy(dm, mc.data(), towers * sizeof(ModC), cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(dmsg, m.data(), (size_t)n * 8, cudaMemcpyHostToDevice), "upload");
+    k_embed_towers<<<dim3(grid_for(n), towers), 256>>>(d, dmsg, dm, n);
+    ck(cudaGetLastError(), "embed");
+    launch_xform(d, dj, towers, n, mod, root, false);
+    ck(cudaMemcpy(out.data(), d, T * 8, cudaMemcpyDeviceToHost), "download");
+}
+
+namespace {
+void pointwise_host(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, const std::vector<uint64_t>& d0,
+                    const std::vector<uint64_t>* d1, uint32_t towers, uint32_t n, const std::vector<uint64_t>& mod,
+                    int mul) {
+    const size_t T = (size_t)towers * n;
+    need(c0.size() >= T && c1.size() >= T && d0.size() >= T && (!d1 || d1->size() >= T) && mod.size() >= towers,
+         mul ? "ct_mul_pt_host: operand shorter than towers*n" : "ct_add_ct_host: operand shorter than towers*n");
+    if (!T) return;
+    const std::vector<ModC> mc = modcs(mod, towers);
+    StageLease L = stage(stage_bytes({towers * sizeof(ModC), T * 8, T * 8, T * 8, d1 ? T * 8 : 0}));
+    ModC* dm = L.take<ModC>(towers);
+    u64* a0 = L.take<u64>(T);
+    u64* a1 = L.take<u64>(T);
+    u64* b0 = L.take<u64>(T);
+    u64* b1 = d1 ? L.take<u64>(T) : b0;
+    ck(cudaMemcpy(dm, mc.data(), towers * sizeof(ModC), cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(a0, c0.data(), T * 8, cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(a1, c1.data(), T * 8, cudaMemcpyHostToDevice), "upload");
+    ck(cudaMemcpy(b0, d0.data(), T * 8, cudaMemcpyHostToDevice), "upload");
+    if (d1) ck(cudaMemcpy(b1, d1->data(), T * 8, cudaMemcpyHostToDevice), "upload");
+    k_pointwise<<<dim3(grid_for(n), towers), 256>>>(a0, a1, b0, b1, dm, n, mul);
+    ck(cudaGetLastError(), "pointwise");
+    ck(cudaMemcpy(c0.data(), a0, T * 8, cudaMemcpyDeviceToHost), "download");
+    ck(cudaMemcpy(c1.data(), a1, T * 8, cudaMemcpyDeviceToHost), "download");
+}
+}  // namespace
+
+void ct_add_ct_host(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, const std::vector<uint64_t>& d0,
+                    const std::vector<uint64_t>& d1, uint32_t towers, uint32_t n, const std::vector<uint64_t>& mod) {
+    pointwise_host(c0, c1, d0, &d1, towers, n, mod, 0);
+}
+
+void ct_mul_pt_host(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, const std::vector<uint64_t>& ptEval,
+                    uint32_t towers, uint32_t n, const std::vector<uint64_t>& mod) {
+    pointwise_host(c0, c1, ptEval, nullptr, towers, n, mod, 1);
+}
+
+void rotate_ct_host(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1, uint32_t k, const KeySwitchConstants& Krot,
+                    uint32_t towers, uint32_t n, const std::vector<uint64_t>& mod,
+                    const std::vector<uint64_t>& root) {
+    // Same result as the reference's host-orchestrated form (coefficient
+    // automorphism, keyswitch_core_resident, host add): the automorphism is
+    // a permutation of eval slots and the keyswitch is the resident one.
+    const size_t T = (size_t)towers * n;
+    need(c0.size() >= T && c1.size() >= T, "rotate_ct_host: ciphertext shorter than towers*n");
+    c0.resize(T);
+    rotate_ct_resident(c0, c1, k, Krot, towers, n, mod, root);
 }
 
 // ---------------------------------------------------------------- host harness

@@ -337,6 +337,9 @@ def load_ref_gpu():
         "refg_evalmult_rescale": (I32, [VP, U32, U32, u64p, u64p, u64p, u64p, u64p, u64p]),
         "refg_rotate_device": (I32, [VP, U32, U32, U32, U32, u64p, u64p]),
         "refg_ntt": (I32, [u64p, U32, U64, u64p, u64p, I32, U64, U64]),
+        "refg_pt_to_eval": (None, [U32, U32, u64p, u64p, i64p, u64p]),
+        "refg_ptops": (None, [U32, U32, u64p, I32, u64p, u64p, u64p, u64p]),
+        "refg_rotate_host": (I32, [VP, U32, U32, U32, U32, u64p, u64p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

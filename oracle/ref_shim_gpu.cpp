@@ -27,6 +27,15 @@ namespace gpufhe {
 void native_rescale_consts(std::vector<uint64_t>&, std::vector<uint64_t>&, const std::vector<uint64_t>&, uint32_t);
 void automorphism_eval_host(std::vector<uint64_t>&, uint32_t, uint32_t, uint32_t,
                             const std::vector<uint64_t>&, const std::vector<uint64_t>&);
+/* headerless in the reference; declared the way its tests declare them */
+void pt_to_eval_host(std::vector<uint64_t>&, const std::vector<int64_t>&, uint32_t, uint32_t,
+                     const std::vector<uint64_t>&, const std::vector<uint64_t>&);
+void ct_add_ct_host(std::vector<uint64_t>&, std::vector<uint64_t>&, const std::vector<uint64_t>&,
+                    const std::vector<uint64_t>&, uint32_t, uint32_t, const std::vector<uint64_t>&);
+void ct_mul_pt_host(std::vector<uint64_t>&, std::vector<uint64_t>&, const std::vector<uint64_t>&, uint32_t,
+                    uint32_t, const std::vector<uint64_t>&);
+void rotate_ct_host(std::vector<uint64_t>&, std::vector<uint64_t>&, uint32_t, const KeySwitchConstants&,
+                    uint32_t, uint32_t, const std::vector<uint64_t>&, const std::vector<uint64_t>&);
 }
 
 typedef uint64_t u64;
@@ -149,6 +158,40 @@ void refg_automorph_host(uint32_t n, uint32_t towers, uint32_t k, const u64* mod
     vec x(v, v + (size_t)towers * n);
     gpufhe::automorphism_eval_host(x, towers, n, k, vec(mods, mods + towers), vec(roots, roots + towers));
     std::memcpy(v, x.data(), x.size() * 8);
+}
+
+/* pt_to_eval_host (rotate.cpp:104-112) */
+void refg_pt_to_eval(uint32_t n, uint32_t towers, const u64* mods, const u64* roots, const int64_t* m, u64* out) {
+    vec o;
+    gpufhe::pt_to_eval_host(o, std::vector<int64_t>(m, m + n), towers, n, vec(mods, mods + towers),
+                            vec(roots, roots + towers));
+    std::memcpy(out, o.data(), o.size() * 8);
+}
+
+/* ct_add_ct_host (mul = 0, d1 used) or ct_mul_pt_host (mul = 1, d0 is the
+ * plaintext) (ptops.cpp:13-26) */
+void refg_ptops(uint32_t n, uint32_t towers, const u64* mods, int mul, u64* c0, u64* c1, const u64* d0,
+                const u64* d1) {
+    const size_t T = (size_t)towers * n;
+    vec a(c0, c0 + T), b(c1, c1 + T), md(mods, mods + towers);
+    if (mul) gpufhe::ct_mul_pt_host(a, b, vec(d0, d0 + T), towers, n, md);
+    else gpufhe::ct_add_ct_host(a, b, vec(d0, d0 + T), vec(d1, d1 + T), towers, n, md);
+    std::memcpy(c0, a.data(), T * 8);
+    std::memcpy(c1, b.data(), T * 8);
+}
+
+/* rotate_ct_host with rotation key `key` at level L (rotate.cpp:176-188) */
+int refg_rotate_host(void* hp, uint32_t key, uint32_t L, uint32_t numPart, uint32_t k, u64* c0, u64* c1) {
+    RefH* h = (RefH*)hp;
+    auto C = level_consts(h, L, numPart);
+    attach_key(h, C, key);
+    const size_t T = (size_t)L * h->n;
+    vec a(c0, c0 + T), b(c1, c1 + T);
+    gpufhe::rotate_ct_host(a, b, k, C, L, h->n, vec(h->Q.begin(), h->Q.begin() + L),
+                           vec(h->rQ.begin(), h->rQ.begin() + L));
+    std::memcpy(c0, a.data(), T * 8);
+    std::memcpy(c1, b.data(), T * 8);
+    return (int)cudaGetLastError();
 }
 
 /* keyswitch_resident at level L (device path) */

@@ -18,6 +18,7 @@
 #include "ckks_ops.h"
 #include "device_ciphertext.h"
 #include "encode.h"
+#include "host_ops.h"
 #include "keygen.h"
 #include "keyswitch.h"
 #include "keyswitch_resident.h"
@@ -142,6 +143,7 @@ int main(int argc, char** argv) {
         gate(R.ba0 == ks0 && R.ba1 == ks1, "keyswitch_core_resident bit-exact vs keyswitch_resident");
     }
 
+    std::vector<u64> sH, g0, g1;
     {   // rotation: device == resident (test_rot_resident.cpp:141-164), and decrypts rotated
         const u64 k = 5;
         std::vector<u64> sA = KPqp.s;
@@ -167,6 +169,17 @@ int main(int argc, char** argv) {
         cudaMemcpy(f0.data(), d0, T * 8, cudaMemcpyDeviceToHost);
         cudaMemcpy(f1.data(), d1, T * 8, cudaMemcpyDeviceToHost);
         gate(f0 == e0 && f1 == e1, "rotate_ct_device bit-exact vs rotate_ct_resident");
+        // the headerless host forms (test_rotate.cpp:42, test_c2s_engine.cpp:55, 101)
+        sH = KPqp.s;
+        gpufhe::automorphism_eval_host(sH, sizeQlP, n, (uint32_t)k, modQP, rootQP);
+        gate(sH == sA, "automorphism_eval_host bit-exact vs automorphism_eval_device");
+        g0 = c0a; g1 = c1a;
+        gpufhe::rotate_ct_host(g0, g1, (uint32_t)k, Kr, sizeQ, n, mod, root);
+        gate(g0 == e0 && g1 == e1, "rotate_ct_host bit-exact vs rotate_ct_resident");
+        bool thrown = false;
+        try { std::vector<u64> x = c0a; gpufhe::automorphism_eval_host(x, sizeQ, n, 4, mod, root); }
+        catch (const std::invalid_argument&) { thrown = true; }
+        gate(thrown, "automorphism_eval_host rejects an even Galois element");
         std::vector<int64_t> dec;
         gpufhe::decrypt_host(dec, f0, f1, KPq.s, n, mod, root);
         // sigma_5 maps X -> X^5: 3 - 2x -> 3 - 2x^5
@@ -196,6 +209,44 @@ int main(int argc, char** argv) {
         gate(thrown, "DeviceCiphertext::upload throws on size mismatch");
     }
 
+    // plaintext-ciphertext helpers as test_ptops.cpp:60-95 calls them:
+    // (3-2x)*D times the unscaled plaintext 4+5x^2, and the sum of the two
+    // ciphertexts, each checked by decryption and word for word
+    std::vector<u64> pe, pm0 = c0a, pm1 = c1a, pa0 = c0a, pa1 = c1a;
+    {
+        gpufhe::pt_to_eval_host(pe, a2, sizeQ, n, mod, root);
+        gpufhe::ct_mul_pt_host(pm0, pm1, pe, sizeQ, n, mod);
+        gpufhe::ct_add_ct_host(pa0, pa1, c0b, c1b, sizeQ, n, mod);
+        bool words = pe.size() == T;
+        for (uint32_t t = 0; t < sizeQ && words; ++t)
+            for (uint32_t j = 0; j < n; ++j) {
+                const size_t x = (size_t)t * n + j;
+                const u64 q = mod[t], s0 = c0a[x] + c0b[x], s1 = c1a[x] + c1b[x];
+                words &= pm0[x] == mm(c0a[x], pe[x], q) && pm1[x] == mm(c1a[x], pe[x], q) &&
+                         pa0[x] == (s0 >= q ? s0 - q : s0) && pa1[x] == (s1 >= q ? s1 - q : s1);
+            }
+        gate(words, "ct_mul_pt_host / ct_add_ct_host word for word");
+        std::vector<int64_t> dm, da;
+        gpufhe::decrypt_host(dm, pm0, pm1, KPq.s, n, mod, root);
+        gpufhe::decrypt_host(da, pa0, pa1, KPq.s, n, mod, root);
+        std::vector<int64_t> prod(n, 0);
+        for (uint32_t i = 0; i < n; ++i) if (a1[i]) for (uint32_t j = 0; j < n; ++j) if (a2[j]) {
+            uint32_t idx = (i + j) % n; int64_t sg = (i + j) >= n ? -1 : 1; prod[idx] += sg * a1[i] * a2[j]; }
+        int bad = 0;
+        for (uint32_t j = 0; j < n; ++j) {
+            bad += std::llround((double)dm[j] / (double)D) != prod[j];
+            bad += std::llround((double)da[j] / (double)D) != a1[j] + a2[j];
+        }
+        gate(bad == 0, "ct_mul_pt_host decrypts to (3-2x)(4+5x^2), ct_add_ct_host to the sum");
+        // fewer towers than the vectors hold: only the first towers*n words change
+        std::vector<u64> q0 = c0a, q1 = c1a;
+        gpufhe::ct_add_ct_host(q0, q1, c0b, c1b, sizeQ - 1, n, mod);
+        const size_t F = (size_t)(sizeQ - 1) * n;
+        gate(std::equal(q0.begin(), q0.begin() + F, pa0.begin()) && std::equal(q0.begin() + F, q0.end(), c0a.begin() + F) &&
+             std::equal(q1.begin(), q1.begin() + F, pa1.begin()) && q1.size() == T,
+             "ct_add_ct_host over fewer towers leaves the rest");
+    }
+
     // canonical encode / decode as the reference's tests call them
     // (test_alpha10.cpp:52-82): seeded slots at scale 2^40
     std::vector<int64_t> em;
@@ -223,6 +274,7 @@ int main(int argc, char** argv) {
         std::fwrite(ez.data(), 16, n / 2, f);
         std::fwrite(em.data(), 8, n, f);
         std::fwrite(dz.data(), 16, n / 2, f);
+        for (const auto* v : {&sH, &g0, &g1, &pe, &pm0, &pm1, &pa0, &pa1}) std::fwrite(v->data(), 8, v->size(), f);
         std::fclose(f);
     }
     gpufhe::ks_work_destroy(W);

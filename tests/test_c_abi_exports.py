@@ -54,6 +54,9 @@ def test_headers_declare_the_boundary():
     assert {"gpufhe_ctx_create", "gpufhe_plan_launch", "gpufhe_server_submit", "gpufhe_rescale_noalloc",
             "gpufhe_keygen", "gpufhe_encode_batch"} <= set(c_names)
     assert {"keyswitch_resident", "rescale_resident_raw", "ks_context_create", "keygen_host"} <= set(cpp_names)
+    # the reference's headerless helpers its tests declare in place
+    assert {"automorphism_eval_host", "rotate_ct_host", "pt_to_eval_host", "ct_add_ct_host",
+            "ct_mul_pt_host"} <= set(cpp_names)
 
 
 def test_every_c_function_resolves(lib):

@@ -63,3 +63,63 @@ def test_cpp_api(tmp_path):
     O.lib().orc_tensor(c0a, c1a, c0b, c1b, t0, t1, t2, Q, L, n)
     f0, f1 = octx.keyswitch(L, t2)
     assert np.array_equal(k0, f0) and np.array_equal(k1, f1)
+
+    # the headerless host helpers (automorphism_eval_host, rotate_ct_host,
+    # pt_to_eval_host, ct_mul_pt_host, ct_add_ct_host)
+    rest = rest[3 * n:]
+    TQP = (L + K) * n
+    sH, rest = rest[:TQP], rest[TQP:]
+    assert rest.size == 7 * T
+    g0, g1, pe, pm0, pm1, pa0, pa1 = (rest[i * T:(i + 1) * T] for i in range(7))
+    sA = octx.automorph_eval(L + K, 5, s)
+    assert np.array_equal(sH, sA)
+    ra, rb = octx.evalkeygen(s, sA, pkA, pkB, seed=404)
+    octx.set_key(1, ra, rb)
+    w0, w1 = octx.rotate(L, 5, c0a, c1a, 1)
+    assert np.array_equal(g0, w0) and np.array_equal(g1, w1)
+    a2 = np.zeros(n, np.int64)
+    a2[0], a2[2] = 4, 5
+    want_pe = []
+    for t in range(L):
+        q = int(Q[t])
+        fr, fp, _, _, _, _ = O.root_tables(n, q, int(octx.roots[t]))
+        want_pe.append(O.ntt(np.array([x % q for x in a2.tolist()], np.uint64), n, q, fr, fp))
+    want_pe = np.concatenate(want_pe)
+    assert np.array_equal(pe, want_pe)
+    m0, m1_, s0, s1 = (x.copy() for x in (c0a, c1a, c0a, c1a))
+    for t in range(L):
+        q, sl = int(Q[t]), slice(t * n, (t + 1) * n)
+        O.lib().orc_rns_mult(c0a[sl].copy(), want_pe[sl].copy(), m0[sl], q, n)
+        O.lib().orc_rns_mult(c1a[sl].copy(), want_pe[sl].copy(), m1_[sl], q, n)
+        x0, x1 = s0[sl].copy(), s1[sl].copy()
+        O.lib().orc_add_into(x0, c0b[sl].copy(), q, n)
+        O.lib().orc_add_into(x1, c1b[sl].copy(), q, n)
+        s0[sl], s1[sl] = x0, x1
+    assert np.array_equal(pm0, m0) and np.array_equal(pm1, m1_)
+    assert np.array_equal(pa0, s0) and np.array_equal(pa1, s1)
+
+    refg = O.load_ref_gpu()
+    if refg is None:
+        return
+    # the same calls into the reference library itself
+    x = s.copy()
+    refg.refg_automorph_host(n, L + K, 5, octx.QP, octx.roots, x)
+    assert np.array_equal(sH, x)
+    y = np.zeros(T, np.uint64)
+    refg.refg_pt_to_eval(n, L, Q, octx.roots, a2, y)
+    assert np.array_equal(pe, y)
+    u0, u1 = c0a.copy(), c1a.copy()
+    refg.refg_ptops(n, L, Q, 1, u0, u1, pe, pe)
+    assert np.array_equal(pm0, u0) and np.array_equal(pm1, u1)
+    u0, u1 = c0a.copy(), c1a.copy()
+    refg.refg_ptops(n, L, Q, 0, u0, u1, c0b, c1b)
+    assert np.array_equal(pa0, u0) and np.array_equal(pa1, u1)
+    h = refg.refg_create(n, Q, L, P, K, octx.roots)
+    try:
+        dnum = -(-L // alpha)
+        refg.refg_set_key(h, 1, dnum, ra, rb)
+        u0, u1 = c0a.copy(), c1a.copy()
+        assert refg.refg_rotate_host(h, 1, L, dnum, 5, u0, u1) == 0
+        assert np.array_equal(g0, u0) and np.array_equal(g1, u1)
+    finally:
+        refg.refg_destroy(h)
