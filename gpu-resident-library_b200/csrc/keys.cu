@@ -1,4 +1,5 @@
-// Key generation, encryption and decryption on the device (include/gpufhe_b200.h).
+// Key generation, encryption, decryption and ModRaise on the device
+// (include/gpufhe_b200.h).
 //
 // The reference builds every key and ciphertext with host loops: per tower it
 // embeds the sampled small polynomials, uploads them to a fresh cudaMalloc,
@@ -262,6 +263,32 @@ __global__ void k_garner(const u64* __restrict__ ph, u64* __restrict__ out, CrtC
 }
 
 // ---------------------------------------------------------------- host helpers
+// ModRaise, first step: x[p][k] = in[p][k] for the 2*count components
+// (p even: c0 of ciphertext p/2, odd: c1), tower 0 only.
+__global__ void k_gather_tower0(const u64* const* __restrict__ in, u64* __restrict__ x, uint32_t n) {
+    const u64* src = in[blockIdx.y];
+    u64* dst = x + (size_t)blockIdx.y * n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) dst[k] = src[k];
+}
+
+// ModRaise, third step: out[p][t][k] = centre(x[p][k]) mod q_t, where
+// centre(v) = v - q0 for v > q0 / 2 (the reference's decrypt_host centring,
+// src/encdec.cpp:79) and the embedding is ((v % q) + q) % q
+// (src/rotate.cpp:108-110). blockIdx.y = component, blockIdx.z = tower.
+__global__ void k_raise(const u64* __restrict__ x, u64* const* __restrict__ out, const ModC* __restrict__ mod,
+                        uint32_t n) {
+    const uint32_t p = blockIdx.y, t = blockIdx.z;
+    const u64 q0 = mod[0].q;
+    const ModC m = mod[t];
+    const u64* src = x + (size_t)p * n;
+    u64* dst = out[p] + (size_t)t * n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const u64 v = src[k];
+        const long long c = v > q0 / 2 ? (long long)v - (long long)q0 : (long long)v;
+        dst[k] = emb(c, m);
+    }
+}
+
 struct Scratch {
     cudaStream_t s;
     std::vector<void*> ptrs;
@@ -552,6 +579,47 @@ int gpufhe_decrypt_crt_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, con
         ck(cudaGetLastError(), "crt");
         ck(cudaMemcpyAsync(out128, dout, 2 * words * 8, cudaMemcpyDeviceToHost, stream), "download");
         ck(cudaStreamSynchronize(stream), "decrypt sync");
+        return GPUFHE_OK;
+    })
+}
+
+int gpufhe_modraise_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, const uint64_t* const* d_c0_in,
+                          const uint64_t* const* d_c1_in, uint64_t* const* d_c0_out, uint64_t* const* d_c1_out,
+                          cudaStream_t stream) {
+    Context* c = gpufhe_impl(h);
+    if (!c || !d_c0_in || !d_c1_in || !d_c0_out || !d_c1_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    if (!towers || towers > c->fullQ()) { gfx::set_error("modraise: towers out of range"); return GPUFHE_EINVAL; }
+    if (!count) return GPUFHE_OK;
+    if (2 * (size_t)count > 65535) { gfx::set_error("modraise: at most 32767 ciphertexts per call"); return GPUFHE_EINVAL; }
+    KEYS_TRY({
+        const uint32_t n = c->n(), comps = 2 * count;
+        const std::vector<u64> qp = qp_moduli(*c);
+        std::vector<const u64*> in(comps);
+        std::vector<u64*> out(comps);
+        for (uint32_t i = 0; i < count; ++i) {
+            if (!d_c0_in[i] || !d_c1_in[i] || !d_c0_out[i] || !d_c1_out[i])
+                throw std::invalid_argument("modraise: null ciphertext pointer");
+            in[2 * i] = d_c0_in[i];
+            in[2 * i + 1] = d_c1_in[i];
+            out[2 * i] = d_c0_out[i];
+            out[2 * i + 1] = d_c1_out[i];
+        }
+        Scratch S(stream);
+        u64* x = S.get<u64>((size_t)comps * n);
+        const u64* const* din = upload(S, in);
+        u64* const* dout = upload(S, out);
+        const unsigned gx = (n + KNT - 1) / KNT;
+        k_gather_tower0<<<dim3(gx, comps), KNT, 0, stream>>>(din, x, n);
+        ck(cudaGetLastError(), "modraise gather");
+        transform(*c, qp, S, x, comps, 1, true);                        // tower 0 -> coefficients
+        k_raise<<<dim3(gx, comps, towers), KNT, 0, stream>>>(x, dout, c->dev().mod, n);
+        ck(cudaGetLastError(), "modraise embed");
+        std::vector<xf::Job> jobs((size_t)comps * towers);           // every tower -> eval form
+        for (uint32_t p = 0; p < comps; ++p)
+            for (uint32_t t = 0; t < towers; ++t)
+                jobs[(size_t)p * towers + t] = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
+        xf::Job* dj = upload(S, jobs);
+        ck(xf_launch_ntt(dj, nullptr, (int)jobs.size(), (int)c->logn(), false, stream), "modraise transform");
         return GPUFHE_OK;
     })
 }

@@ -51,6 +51,7 @@ _API: dict = {
     "gpufhe_encrypt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, U64, C.c_double, VP, VP, VP]),
     "gpufhe_decrypt_batch": (I32, [VP, U32, VP, VP, VP, VP, VP]),
     "gpufhe_decrypt_crt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
+    "gpufhe_modraise_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
     "gpufhe_encoder_create": (I32, [U32, I32, C.POINTER(VP)]),
     "gpufhe_encoder_destroy": (None, [VP]),
     "gpufhe_encode_batch": (I32, [VP, U32, VP, C.c_double, VP, VP]),

@@ -111,6 +111,21 @@ int gpufhe_decrypt_batch(gpufhe_ctx* ctx, uint32_t count, const uint64_t* const*
 int gpufhe_decrypt_crt_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, const uint64_t* const* d_c0,
                              const uint64_t* const* d_c1, const uint64_t* d_s, uint64_t* out128,
                              cudaStream_t stream);
+/* ModRaise of `count` ciphertexts from tower q0 alone to the first `towers`
+ * towers of Q: each component's tower 0 goes to coefficients, is centred mod
+ * q0 (v > q0/2 -> v - q0) and embedded mod every q_t, and every tower goes
+ * back to eval form. The raised ciphertext decrypts to the original phase
+ * plus q0*I for a small integer polynomial I. Replaces the sequence the
+ * reference composes on the host in tests/test_modraise.cpp:50-58
+ * (decrypt_host with a zero partner, src/encdec.cpp:68-81, then
+ * pt_to_eval_host, src/rotate.cpp:104-112). d_c0_in / d_c1_in: host arrays
+ * of count device pointers, tower 0 = their first n words; d_c0_out /
+ * d_c1_out: host arrays of count device pointers to [towers][n], distinct
+ * from one another; an output may be its own input. At most 32767
+ * ciphertexts per call. Asynchronous on `stream`. */
+int gpufhe_modraise_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, const uint64_t* const* d_c0_in,
+                          const uint64_t* const* d_c1_in, uint64_t* const* d_c0_out, uint64_t* const* d_c1_out,
+                          cudaStream_t stream);
 
 /* ---------------------------------------------------------------- canonical encode / decode
  * The reference's encode_host / decode_host (src/encode.cpp:13-44): slots

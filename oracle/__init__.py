@@ -71,6 +71,7 @@ def lib():
             "orc_evalkeygen": (None, [VP, u64p, u64p, u64p, u64p, U64, DBL, U64, u64p, u64p]),
             "orc_encrypt": (None, [VP, U32, i64p, u64p, u64p, U64, DBL, U64, u64p, u64p]),
             "orc_decrypt": (None, [VP, U32, u64p, u64p, u64p, i64p]),
+            "orc_modraise": (None, [VP, U32, u64p, u64p, u64p, u64p]),
             "orc_phase_coeff": (None, [VP, U32, u64p, u64p, u64p, u64p]),
             "orc_keyswitch": (None, [VP, U32, U32, u64p, u64p, u64p]),
             "orc_rescale": (None, [VP, U32, u64p]),
@@ -194,6 +195,12 @@ class Ctx:
         ph = np.zeros(towers * self.n, np.uint64)
         lib().orc_phase_coeff(self.h, towers, _u64(c0), _u64(c1), _u64(s), ph)
         return ph
+
+    def modraise(self, towers, c0, c1):
+        """Tower-0 ciphertext raised to `towers` towers (test_modraise.cpp:50-58)."""
+        o0, o1 = np.zeros(towers * self.n, np.uint64), np.zeros(towers * self.n, np.uint64)
+        lib().orc_modraise(self.h, towers, _u64(c0[:self.n]), _u64(c1[:self.n]), o0, o1)
+        return o0, o1
 
     def decrypt_crt(self, towers, c0, c1, s):
         """Full-CRT decryption: centered integer coefficients over Q_towers."""

@@ -743,6 +743,31 @@ void orc_decrypt(const OrcCtx* c, uint32_t towers, const u64* c0, const u64* c1,
     for (uint32_t k = 0; k < n; ++k) { u64 v = ph[k]; mout[k] = v > q / 2 ? (int64_t)v - (int64_t)q : (int64_t)v; }
 }
 
+void orc_modraise(const OrcCtx* c, uint32_t towers, const u64* c0, const u64* c1, u64* out0, u64* out1) {
+    /* tests/test_modraise.cpp:50-58: per component, decrypt_host with a zero
+     * partner (encdec.cpp:68-81: tower-0 INTT, centre v > q0/2 -> v - q0),
+     * then pt_to_eval_host over `towers` towers (rotate.cpp:104-112:
+     * ((v % q) + q) % q, NTT per tower) */
+    const uint32_t n = c->n;
+    const u64 q0 = c->Q[0];
+    const u64* in[2] = {c0, c1};
+    u64* out[2] = {out0, out1};
+    vec x(n);
+    for (int p = 0; p < 2; ++p) {
+        std::memcpy(x.data(), in[p], (size_t)n * 8);
+        intt_one(c, x.data(), 0);
+        for (uint32_t t = 0; t < towers; ++t) {
+            const long long q = (long long)c->Q[t];
+            u64* o = out[p] + (size_t)t * n;
+            for (uint32_t k = 0; k < n; ++k) {
+                const long long v = x[k] > q0 / 2 ? (long long)x[k] - (long long)q0 : (long long)x[k];
+                o[k] = (u64)((v % q + q) % q);
+            }
+            ntt_one(c, o, t);
+        }
+    }
+}
+
 void orc_phase_coeff(const OrcCtx* c, uint32_t towers, const u64* c0, const u64* c1, const u64* s,
                      u64* phase) {
     const uint32_t n = c->n;

@@ -116,6 +116,8 @@ void orc_evalmult_rescale_batch(const OrcCtx* c, uint32_t npairs, const uint32_t
 /* sigma_k on every tower of an eval-form poly (rotate.cpp:87-101) */
 void orc_automorph_eval(const OrcCtx* c, uint32_t towers, uint32_t k, uint64_t* v, int qp_order);
 /* rotate_ct_host: automorph c0,c1; keyswitch c1 with key_id; c0 += ba0; c1 = ba1 */
+void orc_modraise(const OrcCtx* c, uint32_t towers, const uint64_t* c0, const uint64_t* c1, uint64_t* out0,
+                  uint64_t* out1);
 void orc_rotate(const OrcCtx* c, uint32_t key_id, uint32_t L, uint32_t k, uint64_t* c0, uint64_t* c1);
 /* hoisted: one ModUp of c1 shared by nrot rotations (automorph the digits). */
 void orc_lintrans_bsgs(const OrcCtx* c, uint32_t L, uint32_t n1, uint32_t n2, const uint64_t* c0, const uint64_t* c1,
