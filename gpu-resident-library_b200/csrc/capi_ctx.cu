@@ -119,6 +119,22 @@ int gpufhe_ctx_key_stats(const gpufhe_ctx* h, uint64_t* out) {
     return GPUFHE_OK;
 }
 
+int gpufhe_ctx_device_status(gpufhe_ctx* h, uint32_t* out) {
+    if (!h || !out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    GPUFHE_TRY({
+        u32* d = h->c->dev().err;
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(h->c->device());
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(out, d, 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemset(d, 0, 4);
+        cudaSetDevice(prev);
+        if (e != cudaSuccess) { gfx::set_error(cudaGetErrorString(e)); return GPUFHE_ECUDA; }
+        return GPUFHE_OK;
+    })
+}
+
 int gpufhe_ntt_batch(gpufhe_ctx* h, uint64_t* d_data, uint32_t npolys, uint32_t towers, uint32_t first_tower,
                      int inverse, uint64_t* d_jobs, cudaStream_t s) {
     if (!h || !d_data || !d_jobs) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }

@@ -82,13 +82,14 @@ uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan) {
 }
 
 int gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule) {
-    if (!plan || (schedule & 3) > 2 || ((schedule >> 3) & 3) > 2) {
+    if (!plan || ((schedule >> 3) & 3) > 2) {
         gfx::set_error("bad plan or schedule");
         return GPUFHE_EINVAL;
     }
     pl::Plan& p = *plan->p;
     p.p5_form = (int)(schedule & 3);
     if (p.p5_form == pl::P5_ASYNC && !pl::mac_async_ok(p.dc.dnum)) p.p5_form = pl::P5_REG128;
+    if (p.p5_form == pl::P5_TMA && !pl::mac_tma_ok(p.dc.dnum)) p.p5_form = pl::P5_REG128;
     p.mix = (schedule & 4) ? 0x1ffu : (schedule >> 8) & 0x1ffu;
     p.p3_form = (int)((schedule >> 3) & 3);
     if (p.p3_form > 2) { gfx::set_error("bad P3 form"); return GPUFHE_EINVAL; }

@@ -223,6 +223,7 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
     dc_.pdn = upload(pdn);
     dc_.pdnp = upload(pdnp);
     dc_.phatmodq = upload(phatmodq);
+    dc_.err = const_cast<u32*>(upload(std::vector<u32>(4, 0u)));
 }
 
 Context::~Context() {

@@ -55,6 +55,7 @@ struct DevCtx {
     const u64* pdn;           // [K] n^-1 * (P/p_j)^-1 mod p_j
     const u64* pdnp;
     const u64* phatmodq;      // [K][fullQ] (P/p_j) mod q_i
+    u32* err;                 // device status word: kernels with bounded waits OR in a code when one expires
 };
 
 // A resident eval key: av/bv over full QP for every digit, eval form, layout

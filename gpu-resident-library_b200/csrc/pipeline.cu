@@ -85,6 +85,9 @@ struct Launcher {
             if (mac_async_ok(dnum))
                 cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      maca_smem((int)dnum));
+            if (mac_tma_ok(dnum))
+                cudaFuncSetAttribute(p5_mac_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     p5t_smem((int)dnum));
             mac_dnum = dnum;
         }
     }
@@ -124,7 +127,10 @@ struct Launcher {
             if (k == 4) {
                 if (!p.job_cnt[4][0]) continue;
                 const unsigned grid = p.job_cnt[4][0] * MAC_TILES;
-                if (p.p5_form == P5_ASYNC && mac_async_ok(D.dnum))
+                if (p.p5_form == P5_TMA && mac_tma_ok(D.dnum))
+                    p5_mac_tma<LOGN><<<p.job_cnt[4][0] * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum), s>>>(
+                        D, p.d_pairs, p.d_mac_jobs, p.d_plist);
+                else if (p.p5_form == P5_ASYNC && mac_async_ok(D.dnum))
                     p5_mac_async<LOGN><<<grid, MACA_NT, maca_smem((int)D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
                                                                                      p.d_plist);
                 else if (p.p5_form == P5_REG256)
@@ -481,6 +487,7 @@ uint64_t tune_key(const Plan& p) {
 void apply_choice(Plan& p, int choice) {
     p.p5_form = choice & 3;
     if (p.p5_form == P5_ASYNC && !mac_async_ok(p.dc.dnum)) p.p5_form = P5_REG128;
+    if (p.p5_form == P5_TMA && !mac_tma_ok(p.dc.dnum)) p.p5_form = P5_REG128;
     p.mix = ((unsigned)choice >> 8) & 0x1ffu;
     p.p3_form = (choice >> 3) & 3;
     if (p.p3_form > 2) p.p3_form = 0;
@@ -545,6 +552,7 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
     cur = pick(1u << 2, 24, {0, 8, 16}, cur);                      // P3 form
     std::vector<int> p5v = {P5_REG128, P5_REG256};
     if (mac_async_ok(p.dc.dnum)) p5v.push_back(P5_ASYNC);
+    if (mac_tma_ok(p.dc.dnum)) p5v.push_back(P5_TMA);
     cur = pick(1u << 4, 3, p5v, cur);                              // P5 form
     cudaEventDestroy(a);
     cudaEventDestroy(b);

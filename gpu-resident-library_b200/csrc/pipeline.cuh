@@ -837,6 +837,259 @@ p5_mac_async(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __
     }
 }
 
+// P5, TMA form. One producer thread streams every pair's tiles (the four
+// tensor inputs or the keyswitch input, and each other digit of tower i: rows
+// of P5T_TILE contiguous words) into a ring of P5T_STAGES shared-memory stages
+// with cp.async.bulk; each stage completes on its own mbarrier by transaction
+// count. P5T_NC consumer threads own one 16-byte pair of the tile each,
+// release a stage by arriving on its empty mbarrier as soon as they hold its
+// words in registers, and then write the epilogue. The key tile of row r
+// arrives the same way, once per CTA. Hoisted-rotation digits (an eval-slot
+// gather) and the rotation source are read by the consumers directly.
+// Every wait is bounded in time (mbar_wait): when one expires the thread ORs
+// a code into D.err and leaves, and the producer waits (bounded again) for
+// its copies in flight to land before it leaves, so no copy outlives the CTA.
+// A CTA that starts with D.err set leaves before issuing anything.
+// Results equal p5_mac's word for word.
+constexpr int P5T_TILE = 256;
+constexpr int P5T_NC = P5T_TILE / 2;        // consumer threads
+constexpr int P5T_NT = P5T_NC + 32;         // + one producer warp
+constexpr int P5T_STAGES = 3;
+constexpr int P5T_BAR_WORDS = 16;           // mbarriers: key, full[S], empty[S] (padded)
+static_assert(1 + 2 * P5T_STAGES <= P5T_BAR_WORDS, "mbarrier area");
+__host__ __device__ constexpr int p5t_smem(int dnum) {
+    return (P5T_BAR_WORDS + (2 * dnum + P5T_STAGES * maca_slots(dnum)) * P5T_TILE) * 8;
+}
+
+__device__ __forceinline__ u32 smem_addr(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(u32 bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(u32 bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(u32 bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(u32 bar, u32 parity) {
+    u32 ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ u64 global_ns() {
+    u64 t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the phase of `bar` with parity `parity` to complete; false once
+// about two seconds have passed without it.
+__device__ __forceinline__ bool mbar_wait(u32 bar, u32 parity) {
+    if (mbar_test(bar, parity)) return true;
+    const u64 t0 = global_ns();
+    for (u32 k = 1;; ++k) {
+        if (mbar_test(bar, parity)) return true;
+        if ((k & 63) == 0 && global_ns() - t0 > 2000000000ull) return false;
+    }
+}
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global to this CTA's shared memory, completing on mbarrier `bar`.
+__device__ __forceinline__ void bulk_load(u32 dst, const void* src, u32 bytes, u32 bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(P5T_NT)
+p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
+           const u32* __restrict__ plist) {
+    constexpr int TILES = (1 << LOGN) / P5T_TILE;
+    constexpr u32 ROW = P5T_TILE * 8;           // bytes of one staged row
+    constexpr int S = P5T_STAGES;
+    extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
+    const uint4 jb = jobs[blockIdx.x / TILES];
+    const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
+    const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum);
+    u64* keys = sm + P5T_BAR_WORDS;
+    u64* stage = keys + 2 * dnum * P5T_TILE;
+    const u32 kbar = smem_addr(sm);
+    auto full = [&](u32 b) { return kbar + 8 * (1 + b); };
+    auto empty = [&](u32 b) { return kbar + 8 * (1 + S + b); };
+    __shared__ u32 failed;                      // a wait of an earlier CTA expired: skip the tile
+    if (threadIdx.x == 0) {
+        failed = *reinterpret_cast<volatile u32*>(D.err);
+        mbar_init(kbar, 1);
+        for (u32 b = 0; b < S; ++b) {
+            mbar_init(full(b), 1);
+            mbar_init(empty(b), P5T_NC);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();                            // the only CTA-wide barrier
+    if (failed) return;
+    const bool is_p = r >= D.fullQ;
+    const u32 K = D.K;
+    if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
+        if (threadIdx.x != P5T_NC) return;
+        const PairDesc& P0 = pairs[plist[jb.y]];
+        mbar_arrive_expect_tx(kbar, 2 * dnum * ROW);
+        for (u32 p = 0; p < dnum; ++p) {
+            const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0;
+            bulk_load(smem_addr(keys + (2 * p) * P5T_TILE), P0.kbv + off, ROW, kbar);
+            bulk_load(smem_addr(keys + (2 * p + 1) * P5T_TILE), P0.kav + off, ROW, kbar);
+        }
+        u32 issued = 0;
+        for (u32 g = 0; g < jb.z; ++g) {
+            const u32 b = g % S;
+            if (g >= S && !mbar_wait(empty(b), (g / S - 1) & 1)) {
+                atomicOr(D.err, 4u);
+                break;
+            }
+            const PairDesc& P = pairs[plist[jb.y + g]];
+            const u32 L = P.L, QlP = L + K;
+            const u32 i = is_p ? L + (r - D.fullQ) : r;
+            const u32 pin = is_p ? 0xffffffffu : i / D.alpha;
+            const WsLayout w = ws_layout(L, K, D.alpha);
+            const u32 nparts = D.lvl[L].nparts;
+            const u32 nin = is_p ? 0u : (P.mode == EMR ? 4u : (P.mode == KS ? 1u : 0u));
+            const u32 ndig = P.mode == HROT ? 0u : nparts - (pin < nparts ? 1u : 0u);
+            u64* sb = stage + (size_t)b * slots * P5T_TILE;
+            const size_t o = ((size_t)i << LOGN) + tile0;
+            mbar_arrive_expect_tx(full(b), (nin + ndig) * ROW);
+            if (nin == 4) {
+                for (u32 k = 0; k < 4; ++k) bulk_load(smem_addr(sb + k * P5T_TILE), P.in[k] + o, ROW, full(b));
+            } else if (nin == 1) {
+                bulk_load(smem_addr(sb + P5T_TILE), P.in[0] + o, ROW, full(b));
+            }
+            if (ndig)
+                for (u32 p = 0; p < nparts; ++p) {
+                    if (p == pin) continue;
+                    const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN) + tile0;
+                    bulk_load(smem_addr(sb + (MACA_IN + p) * P5T_TILE), Yt, ROW, full(b));
+                }
+            issued = g + 1;
+        }
+        // every issued stage's copies must land before this thread leaves
+        const u32 first = issued > (u32)S ? issued - S : 0u;
+        for (u32 g = first; g < issued; ++g)
+            if (!mbar_wait(full(g % S), (g / S) & 1)) atomicOr(D.err, 4u);
+        if (!mbar_wait(kbar, 0)) atomicOr(D.err, 1u);
+        return;
+    }
+    const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
+    const ModC m = D.mod[r];
+    if (!mbar_wait(kbar, 0)) {
+        atomicOr(D.err, 1u);
+        return;
+    }
+    for (u32 g = 0; g < jb.z; ++g) {
+        const u32 b = g % S;
+        if (!mbar_wait(full(b), (g / S) & 1)) {
+            atomicOr(D.err, 2u);
+            return;
+        }
+        const PairDesc& P = pairs[plist[jb.y + g]];
+        const u32 L = P.L, QlP = L + K;
+        const u32 i = is_p ? L + (r - D.fullQ) : r;
+        const Level& lv = D.lvl[L];
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        const u32 nparts = lv.nparts;
+        const u32 pin = is_p ? 0xffffffffu : i / D.alpha;
+        const bool emr = P.mode == EMR;
+        const u64* sb = stage + (size_t)b * slots * P5T_TILE + e;
+        ulonglong2 s{0, 0}, t0{0, 0}, t1{0, 0};
+        if (!is_p) {
+            if (emr) {
+                const ulonglong2 x0 = ld2(sb), x1 = ld2(sb + P5T_TILE);
+                const ulonglong2 y0 = ld2(sb + 2 * P5T_TILE), y1 = ld2(sb + 3 * P5T_TILE);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const u64 a0 = v2get(x0, j), a1 = v2get(x1, j), b0 = v2get(y0, j), b1 = v2get(y1, j);
+                    u64 lo, hi;
+                    mul_wide(a1, b1, lo, hi);
+                    v2set(s, j, acc_reduce(lo, hi, m, D.mont));
+                    mul_wide(a0, b0, lo, hi);
+                    v2set(t0, j, acc_reduce(lo, hi, m, D.mont));
+                    mul_wide(a0, b1, lo, hi);
+                    mac_wide(lo, hi, a1, b0);
+                    v2set(t1, j, acc_reduce(lo, hi, m, D.mont));
+                }
+            } else {
+                if (P.mode == ROT || P.mode == HROT) {
+                    const u64* src = P.in[1] + ((size_t)i << LOGN);
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) v2set(s, j, src[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
+                } else {
+                    s = ld2(sb + P5T_TILE);
+                }
+                if (D.mont) {
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) v2set(s, j, redc(v2get(s, j), 0, m));
+                }
+            }
+        }
+        u64 a0l[2] = {0, 0}, a0h[2] = {0, 0}, a1l[2] = {0, 0}, a1h[2] = {0, 0};
+        for (u32 p = 0; p < nparts; ++p) {
+            ulonglong2 dv;
+            if (p == pin) {
+                dv = s;
+            } else if (P.mode == HROT) {            // sigma_k of the shared digit: eval-slot gather
+                const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) v2set(dv, j, Yt[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
+            } else {
+                dv = ld2(sb + (MACA_IN + p) * P5T_TILE);
+            }
+            const ulonglong2 kbv = ld2(keys + (2 * p) * P5T_TILE + e);
+            const ulonglong2 kav = ld2(keys + (2 * p + 1) * P5T_TILE + e);
+            mac_wide(a0l[0], a0h[0], dv.x, kbv.x);
+            mac_wide(a0l[1], a0h[1], dv.y, kbv.y);
+            mac_wide(a1l[0], a1h[0], dv.x, kav.x);
+            mac_wide(a1l[1], a1h[1], dv.y, kav.y);
+        }
+        mbar_arrive(empty(b));                  // every word of stage b is in registers
+        const u32 use_redc = D.mont && (is_p || emr);
+        ulonglong2 r0, r1;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            v2set(r0, j, acc_reduce(a0l[j], a0h[j], m, use_redc));
+            v2set(r1, j, acc_reduce(a1l[j], a1h[j], m, use_redc));
+        }
+        const u64 q = m.q;
+        if (is_p) {
+            *reinterpret_cast<ulonglong2*>(slot_ptr(P, w.RP + (i - L), LOGN) + tile0 + e) = r0;
+            *reinterpret_cast<ulonglong2*>(slot_ptr(P, w.RP + K + (i - L), LOGN) + tile0 + e) = r1;
+            continue;
+        }
+        ulonglong2 o0, o1;
+        u64 *d0, *d1;
+        if (!emr) {   // keyswitch / rotation: W = res * P^-1 (the reduced accumulator)
+            d0 = slot_ptr(P, w.W + i, LOGN);
+            d1 = slot_ptr(P, w.W + L + i, LOGN);
+            o0 = r0;
+            o1 = r1;
+        } else {
+            const bool drop = i == L - 1;
+            const u64 s1 = lv.s1r[i], s1p = lv.s1rp[i];
+            d0 = drop ? slot_ptr(P, w.U, LOGN) : slot_ptr(P, w.W + i, LOGN);
+            d1 = drop ? slot_ptr(P, w.U + 1, LOGN) : slot_ptr(P, w.W + L + i, LOGN);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const u64 ua = csub(v2get(t0, j) + v2get(r0, j), q);
+                const u64 ub = csub(v2get(t1, j) + v2get(r1, j), q);
+                v2set(o0, j, drop ? ua : shoup(ua, s1, s1p, q));
+                v2set(o1, j, drop ? ub : shoup(ub, s1, s1p, q));
+            }
+        }
+        *reinterpret_cast<ulonglong2*>(d0 + tile0 + e) = o0;
+        *reinterpret_cast<ulonglong2*>(d1 + tile0 + e) = o1;
+    }
+}
+
 // ------------------------------------------------------------------ P6
 // INTT row stages of U[c] (t = 0, EvalMult+Rescale only) and RP[c][t-1].
 template <int LOGN, bool FP>

@@ -74,11 +74,14 @@ cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask = 0x1ff);
 void tune(Plan& p, cudaStream_t s, bool measure = true);
 constexpr int MAC_MAX_DNUM = 16;
 // P5 forms: register prefetch with 128 threads x 4 words, the cp.async
-// pipelined form, register prefetch with 256 threads x 2 words.
-constexpr int P5_REG128 = 0, P5_ASYNC = 1, P5_REG256 = 2;
+// pipelined form, register prefetch with 256 threads x 2 words, the TMA
+// (bulk copy + mbarrier) ring.
+constexpr int P5_REG128 = 0, P5_ASYNC = 1, P5_REG256 = 2, P5_TMA = 3;
 inline int mac_smem(uint32_t dnum) { return (int)(dnum * 2 * MAC_TILE * sizeof(u64)); }
 // The pipelined P5 runs when two CTAs' key tiles and staging buffers fit in one SM.
 inline bool mac_async_ok(uint32_t dnum) { return maca_smem((int)dnum) <= 113 * 1024; }
+// The TMA form needs its key tile and stage ring in one CTA's shared memory.
+inline bool mac_tma_ok(uint32_t dnum) { return p5t_smem((int)dnum) <= 200 * 1024; }
 int input_count(uint32_t mode);
 // Rebinds operation `idx` of a built plan to new buffers / mode (same level
 // and job shape) by a one-thread kernel on `s`: no allocation and no host

@@ -45,6 +45,7 @@ _API: dict = {
     "gpufhe_ctx_resident_bytes": (U64, [VP]),
     "gpufhe_ctx_set_key_budget": (I32, [VP, U64]),
     "gpufhe_ctx_key_stats": (I32, [VP, VP]),
+    "gpufhe_ctx_device_status": (I32, [VP, VP]),
     "gpufhe_keygen": (I32, [VP, U32, U32, U64, C.c_double, U64, VP, VP, VP, VP]),
     "gpufhe_evalkeygen": (I32, [VP, U32, VP, VP, VP, VP, VP, VP, U64, C.c_double, VP, VP, VP]),
     "gpufhe_ctx_set_key_device": (I32, [VP, U64, VP, VP]),
@@ -241,6 +242,13 @@ class Context:
         check(lib().gpufhe_ctx_key_stats(self.h, out))
         return dict(zip(("known", "resident", "resident_bytes", "uploads", "evictions", "budget"), map(int, out)))
 
+    def device_status(self):
+        """Synchronises and returns (then clears) the device status word:
+        0 unless a bounded wait inside a kernel expired."""
+        out = (C.c_uint32 * 1)()
+        check(lib().gpufhe_ctx_device_status(self.h, out))
+        return int(out[0])
+
     def key_bytes(self):
         """Device bytes of one key: 2 * dnum * (fullQ + K) * n words."""
         dnum = -(-self.fullQ // self.alpha)
@@ -287,7 +295,7 @@ class Plan:
     def schedule(self):
         """Autotuner choice: {'p5': form, 'mixed_paths': bool, 'tuned': bool}."""
         b = int(lib().gpufhe_plan_schedule(self.h))
-        form = {0: "register-128x4", 1: "cp.async", 2: "register-256x2"}.get(b & 3, "?")
+        form = {0: "register-128x4", 1: "cp.async", 2: "register-256x2", 3: "tma"}.get(b & 3, "?")
         p3 = {0: "plain", 1: "warp-specialised-128x2", 2: "warp-specialised-256x1"}.get((b >> 3) & 3, "?")
         mixed = [k + 1 for k in range(9) if b >> (8 + k) & 1]
         return {"p5": form, "mixed_paths": bool(b & 4), "mixed_phases": mixed, "p3": p3, "tuned": bool(b & 32)}

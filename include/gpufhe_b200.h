@@ -62,6 +62,13 @@ int  gpufhe_ctx_set_key_budget(gpufhe_ctx* ctx, uint64_t bytes);
 /* out[6] = {keys known, keys resident, resident key bytes, uploads from host
  * copies, evictions, budget}. */
 int  gpufhe_ctx_key_stats(const gpufhe_ctx* ctx, uint64_t* out);
+/* Synchronises the context's device and returns (then clears) its device
+ * status word: 0 when every bounded wait inside this library's kernels was
+ * met; otherwise bit 0 = a key-tile wait, bit 1 = a stage wait of a consumer,
+ * bit 2 = a stage-release wait of the producer in the TMA form of the key
+ * inner product expired (the kernel then left without writing that tile's
+ * results). No counterpart in the reference. */
+int  gpufhe_ctx_device_status(gpufhe_ctx* ctx, uint32_t* out);
 
 /* ---------------------------------------------------------------- keys and encryption
  * Seeded key generation, eval-key generation, encryption and decryption on
@@ -239,7 +246,8 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
 /* Launch schedule chosen by the autotuner (first gpufhe_plan_launch outside
  * graph capture, cached per context and batch shape): bits 0-1 = P5 form
  * (0 register prefetch, 128 threads x 4 words; 1 cp.async pipelined;
- * 2 register prefetch, 256 threads x 2 words), bit 2 = every phase launches
+ * 2 register prefetch, 256 threads x 2 words; 3 bulk-copy (TMA) stage ring
+ * with mbarriers, one producer warp and 128 consumer threads), bit 2 = every phase launches
  * its integer and FP64 transform jobs interleaved in one launch, bits 3-4 =
  * P3 form (0 plain; 1 warp-specialised, 128 conversion threads, two CTAs per
  * SM; 2 warp-specialised, 256 conversion threads, one CTA per SM: conversion

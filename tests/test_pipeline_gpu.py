@@ -133,9 +133,19 @@ def test_rotate_hoisted_groups(G, S, gctx):
         sync()
         for j, (o0, o1, e0, e1) in enumerate(want):
             assert np.array_equal(host(o0), e0) and np.array_equal(host(o1), e1), (rep, j)
+    for form in (1, 3):                       # the staged P5 forms gather hoisted digits themselves
+        for o0, o1, _, _ in want:
+            o0.zero_()
+            o1.zero_()
+        plan.set_schedule(form | 4)
+        plan.launch()
+        sync()
+        assert gctx.device_status() == 0
+        for j, (o0, o1, e0, e1) in enumerate(want):
+            assert np.array_equal(host(o0), e0) and np.array_equal(host(o1), e1), (form, j)
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2, 4, 5, 6, 8, 12, 13, 16, 20])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5, 6, 7, 8, 11, 12, 13, 16, 19, 20])
 def test_every_schedule_same_bits(G, S, gctx, schedule):
     """Each launch schedule the autotuner can pick (P5 form x interleaved or
     separate integer / FP64 transform launches) gives the oracle's bits on a
@@ -163,6 +173,8 @@ def test_every_schedule_same_bits(G, S, gctx, schedule):
     plan.launch()
     sync()
     got = plan.schedule()
+    assert gctx.device_status() == 0          # no bounded wait expired (TMA form)
+    assert got["p5"] == ("register-128x4", "cp.async", "register-256x2", "tma")[schedule & 3]
     assert got["tuned"] and got["mixed_paths"] == bool(schedule & 4)
     assert got["p3"] == ("plain", "warp-specialised-128x2", "warp-specialised-256x1")[schedule >> 3]
     for outs, (e0, e1) in want:
