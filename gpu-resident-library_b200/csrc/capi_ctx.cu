@@ -78,7 +78,7 @@ int gpufhe_ctx_create(uint32_t n, const uint64_t* Q, uint32_t fullQ, const uint6
 
 void gpufhe_ctx_destroy(gpufhe_ctx* h) {
     if (!h) return;
-    delete h->c;
+    Context::retire(h->c);   // deleted now, or when its last plan or server goes
     delete h;
 }
 

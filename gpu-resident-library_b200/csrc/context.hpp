@@ -4,6 +4,7 @@
 // Everything a kernel needs is reachable from the POD `DevCtx`, passed by
 // value to each launch.
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -120,7 +121,21 @@ public:
     bool tuned_choice(uint64_t key, int& choice) const;
     void set_tuned_choice(uint64_t key, int choice) const;
 
+    // Lifetime. Plans (and through them linear-transform plans) and servers
+    // hold the context they use; retire() deletes it at once when nothing
+    // holds it, else the last holder's drop() does, so a context destroyed
+    // before its plans stays valid until they are gone. Owners end a context
+    // with retire(), never with delete.
+    void hold() const { life_.fetch_add(2); }
+    static void drop(const Context* c) {
+        if (c->life_.fetch_sub(2) - 2 == 1) delete const_cast<Context*>(c);
+    }
+    static void retire(Context* c) {
+        if (c && c->life_.fetch_or(1) == 0) delete c;
+    }
+
 private:
+    mutable std::atomic<uint32_t> life_{0};   // 2 * holders + retired bit
     uint32_t n_, logn_, alpha_, dnum_;
     int device_;
     std::vector<u64> Q_, P_, roots_;

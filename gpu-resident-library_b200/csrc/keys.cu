@@ -289,6 +289,18 @@ __global__ void k_raise(const u64* __restrict__ x, u64* const* __restrict__ out,
     }
 }
 
+// out[p][t][k] = m[p][k] mod q_t (blockIdx.y = message, blockIdx.z = tower),
+// the reference's plaintext embedding ((v % q) + q) % q (src/rotate.cpp:108-110).
+__global__ void k_embed_ptrs(const int64_t* __restrict__ m, u64* const* __restrict__ out,
+                             const ModC* __restrict__ mod, uint32_t n) {
+    const uint32_t p = blockIdx.y, t = blockIdx.z;
+    const ModC md = mod[t];
+    const int64_t* src = m + (size_t)p * n;
+    u64* dst = out[p] + (size_t)t * n;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        dst[k] = emb(src[k], md);
+}
+
 struct Scratch {
     cudaStream_t s;
     std::vector<void*> ptrs;
@@ -579,6 +591,33 @@ int gpufhe_decrypt_crt_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, con
         ck(cudaGetLastError(), "crt");
         ck(cudaMemcpyAsync(out128, dout, 2 * words * 8, cudaMemcpyDeviceToHost, stream), "download");
         ck(cudaStreamSynchronize(stream), "decrypt sync");
+        return GPUFHE_OK;
+    })
+}
+
+int gpufhe_pt_to_eval_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, const int64_t* d_m,
+                            uint64_t* const* d_out, cudaStream_t stream) {
+    Context* c = gpufhe_impl(h);
+    if (!c || !d_m || !d_out) { gfx::set_error("null argument"); return GPUFHE_EINVAL; }
+    if (!towers || towers > c->fullQ()) { gfx::set_error("pt_to_eval: towers out of range"); return GPUFHE_EINVAL; }
+    if (count > 65535) { gfx::set_error("pt_to_eval: at most 65535 plaintexts per call"); return GPUFHE_EINVAL; }
+    if (!count) return GPUFHE_OK;
+    KEYS_TRY({
+        const uint32_t n = c->n();
+        const std::vector<u64> qp = qp_moduli(*c);
+        std::vector<u64*> out(d_out, d_out + count);
+        for (u64* o : out)
+            if (!o) throw std::invalid_argument("pt_to_eval: null output pointer");
+        Scratch S(stream);
+        u64* const* dout = upload(S, out);
+        k_embed_ptrs<<<dim3((n + KNT - 1) / KNT, count, towers), KNT, 0, stream>>>(d_m, dout, c->dev().mod, n);
+        ck(cudaGetLastError(), "pt_to_eval embed");
+        std::vector<xf::Job> jobs((size_t)count * towers);
+        for (uint32_t p = 0; p < count; ++p)
+            for (uint32_t t = 0; t < towers; ++t)
+                jobs[(size_t)p * towers + t] = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
+        xf::Job* dj = upload(S, jobs);
+        ck(xf_launch_ntt(dj, nullptr, (int)jobs.size(), (int)c->logn(), false, stream), "pt_to_eval transform");
         return GPUFHE_OK;
     })
 }

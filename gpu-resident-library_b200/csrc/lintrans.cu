@@ -85,7 +85,14 @@ struct DevBuf {
 // rotation keys while the plan lives). Launching enqueues four steps and
 // nothing else, so a launch can be captured in a CUDA graph.
 struct gpufhe_lintrans_plan {
-    gfx::Context* ctx = nullptr;
+    gfx::Context* ctx = nullptr;     // held for the plan's lifetime
+    ~gpufhe_lintrans_plan() {
+        baby.reset();
+        giant.reset();
+        tables.reset();
+        scratch.reset();
+        if (ctx) gfx::Context::drop(ctx);
+    }
     uint32_t L = 0, n = 0, n1 = 0, n2 = 0;
     std::unique_ptr<DevBuf> scratch, tables;
     std::unique_ptr<pl::Plan> baby, giant;
@@ -107,6 +114,7 @@ gpufhe_lintrans_plan* build_lintrans(gfx::Context* c, uint32_t level, const uint
         if (!c->key(galois_of(g * n1, n))) throw std::invalid_argument("missing rotation key for a giant step");
     auto pl_ = std::make_unique<gpufhe_lintrans_plan>();
     gpufhe_lintrans_plan& P = *pl_;
+    c->hold();
     P.ctx = c;
     P.L = L;
     P.n = n;

@@ -162,7 +162,7 @@ struct Launcher {
 
 }  // namespace
 
-bool supported_logn(int logn) { return logn >= 11 && logn <= 16; }
+bool supported_logn(int logn) { return logn >= 10 && logn <= 16; }
 
 int input_count(uint32_t mode) { return mode == EMR ? 4 : (mode == ROT || mode == HROT) ? 2 : 1; }
 uint32_t output_towers(const Op& op) { return (op.mode == EMR || op.mode == RESCALE) ? op.L - 1 : op.L; }  // ROT, HROT, KS: L
@@ -321,8 +321,10 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
 Plan::Plan() : staging(std::make_unique<HostTables>()) {}
 
 Plan::~Plan() {
-    if (ctx)
+    if (ctx) {
         for (uint64_t id : key_pins) ctx->release(id);
+        gfx::Context::drop(ctx);                 // may delete a retired context: touch it no more
+    }
     if (d_blob) cudaFree(d_blob);
     if (h_blob) cudaFreeHost(h_blob);
     if (own_ws && ws) cudaFree(ws);
@@ -378,10 +380,15 @@ static void pin_keys(Plan& p, const gfx::Context& c, const std::vector<Op>& ops)
     std::set<uint64_t> ids;
     for (const Op& op : ops)
         if (op.mode != RESCALE) ids.insert(op.key_id);
-    if (p.ctx)
-        for (uint64_t id : p.key_pins) p.ctx->release(id);
+    const gfx::Context* old = p.ctx;
+    if (old)
+        for (uint64_t id : p.key_pins) old->release(id);
     p.key_pins.clear();
-    p.ctx = &c;
+    if (old != &c) {
+        c.hold();
+        p.ctx = &c;
+        if (old) gfx::Context::drop(old);
+    }
     try {
         for (uint64_t id : ids) {
             if (!c.acquire(id)) throw std::invalid_argument("missing eval key");
@@ -395,10 +402,9 @@ static void pin_keys(Plan& p, const gfx::Context& c, const std::vector<Op>& ops)
 }
 
 std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& ops, u64* ws, size_t ws_words) {
-    if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
+    if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^10 .. 2^16");
     auto plan = std::make_unique<Plan>();
-    plan->ctx = &c;
-    plan->dc = c.dev();
+    plan->dc = c.dev();                          // plan->ctx (and its hold) is set by pin_keys
     plan->logn = c.logn();
     size_t need = 0;
     for (const Op& op : ops) { validate(c, op); need += op_workspace_words(c, op.L); }
@@ -425,7 +431,7 @@ std::unique_ptr<Plan> build_plan(const gfx::Context& c, const std::vector<Op>& o
 
 void build_plan_into(Plan& p, const gfx::Context& c, const std::vector<Op>& ops, const std::vector<u64*>& ws_ptrs,
                      cudaStream_t s) {
-    if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^11 .. 2^16");
+    if (!supported_logn((int)c.logn())) throw std::invalid_argument("pipeline supports n = 2^10 .. 2^16");
     if (ws_ptrs.size() != ops.size()) throw std::invalid_argument("one workspace per operation");
     for (u64* w : ws_ptrs)
         if (!w || (reinterpret_cast<uintptr_t>(w) & 15)) throw std::invalid_argument("workspace must be 16-byte aligned");
@@ -563,6 +569,7 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
 
 cudaError_t launch(const Plan& p, cudaStream_t s, unsigned mask) {
     switch (p.logn) {
+        case 10: Launcher<10>::launch(p, s, mask); break;
         case 11: Launcher<11>::launch(p, s, mask); break;
         case 12: Launcher<12>::launch(p, s, mask); break;
         case 13: Launcher<13>::launch(p, s, mask); break;

@@ -48,6 +48,8 @@ struct Plan {
     size_t blob_cap = 0;
     std::unique_ptr<HostTables> staging;
     ~Plan();
+    Plan(const Plan&) = delete;                  // owns device memory and a hold on ctx
+    Plan& operator=(const Plan&) = delete;
 };
 
 bool supported_logn(int logn);

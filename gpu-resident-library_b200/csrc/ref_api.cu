@@ -463,7 +463,7 @@ DeviceKSContext ks_context_create(const KeySwitchConstants& K) {
 }
 
 void ks_context_destroy(DeviceKSContext& C) {
-    delete static_cast<gfx::Context*>(C.impl);
+    gfx::Context::retire(static_cast<gfx::Context*>(C.impl));
     C.impl = nullptr;
 }
 

@@ -109,7 +109,7 @@ Server::Server(const std::vector<gfx::Context*>& ctxs, size_t budget_bytes, uint
     for (auto* c : ctxs_) {
         if (!c) throw std::invalid_argument("server: null context");
         if (c->device() != device_) throw std::invalid_argument("server: contexts on different devices");
-        if (!pl::supported_logn((int)c->logn())) throw std::invalid_argument("server: ring size outside 2^11..2^16");
+        if (!pl::supported_logn((int)c->logn())) throw std::invalid_argument("server: ring size outside 2^10..2^16");
         resident += c->resident_bytes();
     }
     ck(cudaSetDevice(device_), "cudaSetDevice");
@@ -122,6 +122,7 @@ Server::Server(const std::vector<gfx::Context*>& ctxs, size_t budget_bytes, uint
     for (size_t i = 0; i < 2 * ctxs_.size(); ++i) plans_.push_back(std::make_unique<pl::Plan>());
     ck(cudaEventCreate(&epoch_ev_), "cudaEventCreate");
     epoch_ = std::chrono::steady_clock::now();
+    for (auto* c : ctxs_) c->hold();       // the contexts outlive the server
 }
 
 Server::~Server() {
@@ -133,6 +134,7 @@ Server::~Server() {
     if (epoch_ev_) cudaEventDestroy(epoch_ev_);
     plans_.clear();
     for (auto s : streams_) cudaStreamDestroy(s);
+    for (auto* c : ctxs_) gfx::Context::drop(c);
 }
 
 uint32_t Server::final_level(uint32_t level, const std::vector<ReqOp>& ops) {

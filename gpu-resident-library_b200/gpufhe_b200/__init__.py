@@ -53,6 +53,7 @@ _API: dict = {
     "gpufhe_decrypt_batch": (I32, [VP, U32, VP, VP, VP, VP, VP]),
     "gpufhe_decrypt_crt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
     "gpufhe_modraise_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
+    "gpufhe_pt_to_eval_batch": (I32, [VP, U32, U32, VP, VP, VP]),
     "gpufhe_encoder_create": (I32, [U32, I32, C.POINTER(VP)]),
     "gpufhe_encoder_destroy": (None, [VP]),
     "gpufhe_encode_batch": (I32, [VP, U32, VP, C.c_double, VP, VP]),
@@ -278,6 +279,7 @@ class Plan:
         h = VP()
         check(lib().gpufhe_plan_create(ctx.h, self.nops, C.cast(self.ops, VP), d_ws, ws_bytes, C.byref(h)))
         self.h = h
+        self._ctx = ctx                  # the context object outlives the plan
 
     def launch(self, stream=None):
         check(lib().gpufhe_plan_launch(self.h, stream))

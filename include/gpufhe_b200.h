@@ -42,6 +42,9 @@ const char* gpufhe_last_error(void);
  * setup of ks_context_create (reference keyswitch_resident.cpp:32-101). */
 int  gpufhe_ctx_create(uint32_t n, const uint64_t* Q, uint32_t fullQ, const uint64_t* P, uint32_t K,
                        uint32_t alpha, const uint64_t* roots_qp, int device, gpufhe_ctx** out);
+/* Ends the handle. The context's device state is freed at once, or, while
+ * plans, linear-transform plans or servers built on it still exist, when the
+ * last of them is destroyed (they stay valid until then). */
 void gpufhe_ctx_destroy(gpufhe_ctx* ctx);
 int  gpufhe_ctx_roots(const gpufhe_ctx* ctx, uint64_t* roots_qp);
 /* Key over full QP, host [dnum][fullQ+K][n] (dnum = ceil(fullQ/alpha)),
@@ -118,6 +121,15 @@ int gpufhe_decrypt_batch(gpufhe_ctx* ctx, uint32_t count, const uint64_t* const*
 int gpufhe_decrypt_crt_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, const uint64_t* const* d_c0,
                              const uint64_t* const* d_c1, const uint64_t* d_s, uint64_t* out128,
                              cudaStream_t stream);
+/* Integer plaintexts to eval form: message i (device int64, d_m + i*n)
+ * embedded mod each of the first `towers` Q towers (((v % q) + q) % q) and
+ * transformed into d_out[i] (host array of count device pointers to
+ * [towers][n]), with one embedding launch and one batched NTT launch pair
+ * for the whole batch. Replaces the reference's pt_to_eval_host
+ * (src/rotate.cpp:104-112), which its linear transforms call once per
+ * diagonal. At most 65535 plaintexts per call. Asynchronous on `stream`. */
+int gpufhe_pt_to_eval_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, const int64_t* d_m,
+                            uint64_t* const* d_out, cudaStream_t stream);
 /* ModRaise of `count` ciphertexts from tower q0 alone to the first `towers`
  * towers of Q: each component's tower 0 goes to coefficients, is centred mod
  * q0 (v > q0/2 -> v - q0) and embedded mod every q_t, and every tower goes
@@ -209,7 +221,7 @@ int gpufhe_rns_mult_batch(gpufhe_ctx* ctx, const uint64_t* d_a, const uint64_t* 
  *       the reference (its rotate_ct_device, rotate.cpp:118-132, does one ModUp
  *       per rotation); the result differs from GPUFHE_ROTATE by the
  *       approximate-basis-conversion term, as hoisting always does.
- * Device pointers, 16-byte aligned; ring sizes 2^11..2^16. */
+ * Device pointers, 16-byte aligned; ring sizes 2^10..2^16. */
 #define GPUFHE_EVALMULT_RESCALE 0u
 #define GPUFHE_KEYSWITCH 1u
 #define GPUFHE_ROTATE 2u
