@@ -66,30 +66,24 @@ struct Variant {
 
 template <int LOGN>
 struct Launcher {
-    static void attrs(uint32_t dnum) {
-        using G = ntt::Geo<LOGN>;
+    // Kernel attributes, once per ring size. The P5 forms' dynamic shared
+    // memory grows with dnum, so their limits are set to the largest size any
+    // context can ask for (a limit set for the first context's dnum would be
+    // too low for a later context with a different one).
+    static void attrs(uint32_t) {
         static bool done = false;
-        static uint32_t mac_dnum = 0;
-        if (!done) {
-            Variant<LOGN, 0>::attrs();
-            Variant<LOGN, 1>::attrs();
-            Variant<LOGN, 2>::attrs();
-            p3ws_attrs<0>();
-            p3ws_attrs<1>();
-            p3ws_attrs<2>();
-            done = true;
-        }
-        if (dnum > mac_dnum) {
-            cudaFuncSetAttribute(p5_mac<LOGN, MAC_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(dnum));
-            cudaFuncSetAttribute(p5_mac<LOGN, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(dnum));
-            if (mac_async_ok(dnum))
-                cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     maca_smem((int)dnum));
-            if (mac_tma_ok(dnum))
-                cudaFuncSetAttribute(p5_mac_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     p5t_smem((int)dnum));
-            mac_dnum = dnum;
-        }
+        if (done) return;
+        Variant<LOGN, 0>::attrs();
+        Variant<LOGN, 1>::attrs();
+        Variant<LOGN, 2>::attrs();
+        p3ws_attrs<0>();
+        p3ws_attrs<1>();
+        p3ws_attrs<2>();
+        cudaFuncSetAttribute(p5_mac<LOGN, MAC_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
+        cudaFuncSetAttribute(p5_mac<LOGN, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
+        cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_ASYNC_SMEM_MAX);
+        cudaFuncSetAttribute(p5_mac_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
+        done = true;
     }
     // persistent warp-specialised P3 over job segment PATH: form 1 = 128
     // conversion threads, two CTAs per SM; form 2 = 256, one CTA per SM

@@ -81,9 +81,12 @@ constexpr int MAC_MAX_DNUM = 16;
 constexpr int P5_REG128 = 0, P5_ASYNC = 1, P5_REG256 = 2, P5_TMA = 3;
 inline int mac_smem(uint32_t dnum) { return (int)(dnum * 2 * MAC_TILE * sizeof(u64)); }
 // The pipelined P5 runs when two CTAs' key tiles and staging buffers fit in one SM.
-inline bool mac_async_ok(uint32_t dnum) { return maca_smem((int)dnum) <= 113 * 1024; }
+constexpr int MAC_ASYNC_SMEM_MAX = 113 * 1024;
+inline bool mac_async_ok(uint32_t dnum) { return maca_smem((int)dnum) <= MAC_ASYNC_SMEM_MAX; }
 // The TMA form needs its key tile and stage ring in one CTA's shared memory.
-inline bool mac_tma_ok(uint32_t dnum) { return p5t_smem((int)dnum) <= 200 * 1024; }
+constexpr int MAC_TMA_SMEM_MAX = 200 * 1024;
+inline bool mac_tma_ok(uint32_t dnum) { return p5t_smem((int)dnum) <= MAC_TMA_SMEM_MAX; }
+static_assert(MAC_MAX_DNUM * 2 * MAC_TILE * 8 <= 227 * 1024, "register P5 forms at the largest dnum");
 int input_count(uint32_t mode);
 // Rebinds operation `idx` of a built plan to new buffers / mode (same level
 // and job shape) by a one-thread kernel on `s`: no allocation and no host

@@ -54,6 +54,7 @@ _API: dict = {
     "gpufhe_decrypt_crt_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
     "gpufhe_modraise_batch": (I32, [VP, U32, U32, VP, VP, VP, VP, VP]),
     "gpufhe_pt_to_eval_batch": (I32, [VP, U32, U32, VP, VP, VP]),
+    "gpufhe_pointwise_batch": (I32, [VP, U32, VP, VP]),
     "gpufhe_encoder_create": (I32, [U32, I32, C.POINTER(VP)]),
     "gpufhe_encoder_destroy": (None, [VP]),
     "gpufhe_encode_batch": (I32, [VP, U32, VP, C.c_double, VP, VP]),
@@ -421,6 +422,26 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+PW_ADD, PW_SUB, PW_MUL_PT, PW_ADD_PT, PW_SUB_PT, PW_MUL_INT = range(6)
+
+
+class PwOp(C.Structure):
+    """struct gpufhe_pw_op."""
+    _fields_ = [("kind", U32), ("towers", U32), ("a0", VP), ("a1", VP), ("b0", VP), ("b1", VP),
+                ("o0", VP), ("o1", VP), ("scalar", U64)]
+
+
+def pointwise(ctx, ops, stream=None):
+    """ops: dicts {kind, towers, a: (a0, a1), b: (b0, b1) or (pt,), o: (o0, o1), scalar}
+    of device pointers; one launch for the whole list."""
+    arr = (PwOp * len(ops))()
+    for i, o in enumerate(ops):
+        b = tuple(o.get("b", ())) + (None, None)
+        arr[i] = PwOp(o["kind"], o["towers"], o["a"][0], o["a"][1], b[0], b[1], o["o"][0], o["o"][1],
+                      int(o.get("scalar", 0)))
+    check(lib().gpufhe_pointwise_batch(ctx.h, len(ops), C.cast(arr, VP), stream))
 
 
 def lintrans_bsgs(ctx, level, c0, c1, n1, n2, diags, out0, out1, hoisted=False, stream=None):

@@ -121,6 +121,40 @@ int gpufhe_decrypt_batch(gpufhe_ctx* ctx, uint32_t count, const uint64_t* const*
 int gpufhe_decrypt_crt_batch(gpufhe_ctx* ctx, uint32_t count, uint32_t towers, const uint64_t* const* d_c0,
                              const uint64_t* const* d_c1, const uint64_t* d_s, uint64_t* out128,
                              cudaStream_t stream);
+/* ---------------------------------------------------------------- ciphertext arithmetic
+ * Batched arithmetic without a keyswitch on eval-form ciphertexts at any
+ * level (towers = the operation's level, the first `towers` Q moduli), with
+ * the reference's formulas and so its bits: the host loops of
+ * src/ptops.cpp:13-26 (ct_add_ct_host, ct_mul_pt_host) and the subtract,
+ * plaintext subtract and scale-by-integer loops its tests write around them
+ * (tests/test_evalmod.cpp:100-113). All operations run in one launch; an
+ * output may be its own input. Device buffers are [towers][n]:
+ *   ADD      o = a + b          (both components; b0, b1)
+ *   SUB      o = a - b          (both components; b0, b1)
+ *   MUL_PT   o = a (.) b0       (both components times the plaintext b0)
+ *   ADD_PT   o0 = a0 + b0, o1 = a1
+ *   SUB_PT   o0 = a0 - b0, o1 = a1
+ *   MUL_INT  o = a * scalar mod q (both components) */
+#define GPUFHE_PW_ADD 0u
+#define GPUFHE_PW_SUB 1u
+#define GPUFHE_PW_MUL_PT 2u
+#define GPUFHE_PW_ADD_PT 3u
+#define GPUFHE_PW_SUB_PT 4u
+#define GPUFHE_PW_MUL_INT 5u
+typedef struct gpufhe_pw_op {
+    uint32_t kind;
+    uint32_t towers;
+    const uint64_t* a0;
+    const uint64_t* a1;
+    const uint64_t* b0;
+    const uint64_t* b1;
+    uint64_t* o0;
+    uint64_t* o1;
+    uint64_t scalar;
+} gpufhe_pw_op;
+/* Asynchronous on `stream`; at most 65535 operations per call. */
+int gpufhe_pointwise_batch(gpufhe_ctx* ctx, uint32_t count, const gpufhe_pw_op* ops, cudaStream_t stream);
+
 /* Integer plaintexts to eval form: message i (device int64, d_m + i*n)
  * embedded mod each of the first `towers` Q towers (((v % q) + q) % q) and
  * transformed into d_out[i] (host array of count device pointers to

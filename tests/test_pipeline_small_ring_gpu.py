@@ -76,3 +76,32 @@ def test_context_destroyed_before_plan(S):
     e0, e1 = S.octx.evalmult_rescale(4, c0a, c1a, c0b, c1b)
     assert np.array_equal(host(outs[0]), e0) and np.array_equal(host(outs[1]), e1)
     plan.close()                              # frees the context too
+
+
+def test_forms_after_a_larger_dnum():
+    """Every P5 form still launches on a context with fewer digits than one
+    used before it in the same process (kernel shared-memory limits are set
+    for the largest digit count, not the first one seen), with equal bits."""
+    import gpufhe_b200 as G
+    rng = np.random.default_rng(8)
+    q0 = O.native_primes(1, 60, N)
+    Q = np.concatenate([q0, O.native_primes(13, 50, N, avoid=list(q0))])
+    P = O.native_primes(2, 60, N, avoid=list(Q))
+    for tw, alpha in ((14, 2), (5, 2), (3, 2)):            # dnum 7, then 3 and 2
+        g = G.Context(N, Q[:tw], P, alpha)
+        QP = np.concatenate([Q[:tw], P])
+        rows = -(-tw // alpha) * len(QP)
+        key = [np.concatenate([rng.integers(0, int(QP[r % len(QP)]), N, dtype=np.uint64) for r in range(rows)])
+               for _ in range(2)]
+        g.set_key(0, key[0], key[1])
+        x = [dev(np.concatenate([rng.integers(0, int(q), N, dtype=np.uint64) for q in Q[:tw]])) for _ in range(4)]
+        got = []
+        for sched in (0, 1, 2, 3):
+            o0, o1 = empty((tw - 1) * N), empty((tw - 1) * N)
+            plan = G.Plan(g, [dict(level=tw, inp=[ptr(t) for t in x], out=[ptr(o0), ptr(o1)])])
+            plan.set_schedule(sched)
+            plan.launch()
+            sync()
+            got.append((host(o0), host(o1)))
+        for sched in (1, 2, 3):
+            assert np.array_equal(got[sched][0], got[0][0]) and np.array_equal(got[sched][1], got[0][1]), (tw, sched)
