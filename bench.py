@@ -628,6 +628,7 @@ def rotation_batch(G, torch, dev, local, gen, steps):
             hspecs.append(dict(level=L, mode=G.ROTATE_HOISTED, key_id=gal[k], galois=gal[k],
                                inp=[c[0].data_ptr(), c[1].data_ptr()], out=[o[0].data_ptr(), o[1].data_ptr()]))
     ms_hoist, sched_hoist = timed(hspecs)
+    boot = bootstrap_steps(G, torch, dev, ctx, cts, outs, L, n)
     del hcts, outs, cts
     ctx.close()
     return {"workload": "256 ciphertexts, N=2^16, 10 towers (1x60+9x50), P=3x60, alpha=3, index from "
@@ -636,9 +637,55 @@ def rotation_batch(G, torch, dev, local, gen, steps):
             "keys_and_encryption": keys,
             "rotations_per_s": ROT_COUNT / (ms_plain * 1e-3), "ms_per_batch": ms_plain, "schedule": sched_plain,
             "hoisted_rotations_per_s": ROT_COUNT / (ms_hoist * 1e-3), "hoisted_ms_per_batch": ms_hoist,
-            "hoisted_schedule": sched_hoist, "resident_bytes": evk_bytes,
+            "hoisted_schedule": sched_hoist, "resident_bytes": evk_bytes, "bootstrap_steps": boot,
             "distinct_keys": len(set(gal)), "evk_bytes": len(set(gal)) * 2 * rows * n * 8,
             "note": "rotations by +2^14 and -2^14 share one Galois element at N=2^16 (2^15 slots)"}
+
+
+def bootstrap_steps(G, torch, dev, ctx, cts, outs, L, n, reps=5):
+    """Batched bootstrapping steps on the rotation batch's 256 ciphertexts:
+    ModRaise of every ciphertext from its first tower to all L towers
+    (gpufhe_modraise_batch), eval forms of 256 integer plaintexts
+    (gpufhe_pt_to_eval_batch), and one pointwise batch of 256 ciphertext x
+    plaintext products (gpufhe_pointwise_batch). Milliseconds per batch by
+    CUDA events, mean of `reps` launches after one untimed launch; bytes are
+    the words each step must read and write once."""
+    import ctypes as C
+    cnt = len(cts)
+    arr = lambda ts: (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+    c0s, c1s = arr([c[0] for c in cts]), arr([c[1] for c in cts])
+    o0s, o1s = arr([o[0] for o in outs]), arr([o[1] for o in outs])
+    msgs = torch.randint(-(1 << 40), 1 << 40, (cnt, n), dtype=torch.int64, device=dev)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    lib = G.lib()
+    ms_mr = timed(lambda: G.check(lib.gpufhe_modraise_batch(ctx.h, cnt, L, c0s, c1s, o0s, o1s, None)))
+    ms_pt = timed(lambda: G.check(lib.gpufhe_pt_to_eval_batch(ctx.h, cnt, L, msgs.data_ptr(), o0s, None)))
+    ops = [dict(kind=G.PW_MUL_PT, towers=L, a=(c[0].data_ptr(), c[1].data_ptr()), b=(o[0].data_ptr(),),
+                o=(o[0].data_ptr(), o[1].data_ptr())) for c, o in zip(cts, outs)]
+    ms_pw = timed(lambda: G.pointwise(ctx, ops))
+    pk = peaks()["hbm_gbs"]
+
+    def entry(ms, nbytes, unit_count, unit):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        return {"ms_per_batch": ms, unit: unit_count / (ms * 1e-3), "gbs": gbs, "hbm_frac": gbs / pk}
+
+    return {"workload": f"{cnt} ciphertexts / plaintexts, N=2^16, {L} towers",
+            "modraise": entry(ms_mr, cnt * 8 * n * (2 + 2 * L), cnt, "ciphertexts_per_s"),
+            "pt_to_eval": entry(ms_pt, cnt * 8 * n * (1 + L), cnt, "plaintexts_per_s"),
+            "mul_pt": entry(ms_pw, cnt * 8 * n * 5 * L, cnt, "ciphertexts_per_s"),
+            "note": "ModRaise and the embedding are bound by their batched NTTs (L + 1 tower transforms per "
+                    "component), not by HBM; the pointwise product is HBM-bound"}
 
 
 def plain_driver(levels, n, reps, local):
@@ -941,6 +988,7 @@ def run_gpu(args):
                        else {"p50": ms_step, "p99": ms_step, "source": "whole batch per step"}),
         "ntt_kernel_isolation": ntt,
         "rotation_batch": rotation,
+        "bootstrap_steps": rotation.pop("bootstrap_steps") if rotation else None,
         "serving": serving,
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk.summary(),
