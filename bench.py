@@ -183,6 +183,7 @@ SERVE_ROT_STEPS = (1, 2, 4, 8, -1, -2, -4, -8)
 # to 10.7-14.3k ops/s with p50 up to 690 ms, while at 384 repeated runs held
 # 15.7-15.8k ops/s and p50 160-180 ms.
 SERVE_MAX_ACTIVE = 384
+SERVE_WARMUP = 400                  # requests in the untimed warm-up trace of the served form
 SERVE_WORKLOAD = ("serving trace: Poisson arrivals at 2000 req/s (seeded); per request N in {2^14,2^15,2^16}, "
                   "towers U[4,24], depth U[1,10] of EvalMult+Rescale (capped at towers-1) with U[0,8] rotations "
                   "by +-{1,2,4,8} interleaved; Q=1x60+23x50-bit, P=8x60-bit, alpha=8 (dnum=3)")
@@ -241,6 +242,9 @@ def serve(G, ctxs, reqs, budget, plain):
     lat = np.array([r["t_finish"] - r["t_arrival"] for r in rec]) * 1e3
     lat_admit = np.array([r["t_finish"] - r["t_admit"] for r in rec]) * 1e3
     span = max(r["t_finish"] for r in rec) - min(r["t_arrival"] for r in rec)
+    fin = np.sort(np.array([r["t_finish"] for r in rec]))
+    gaps = np.diff(fin) if len(fin) > 1 else np.zeros(1)
+    g = int(np.argmax(gaps))
     return {
         "ops_per_s": st["ops"] / st["busy_s"], "evalmult_rescale_ops_per_s": st["emr_ops"] / st["busy_s"],
         "requests_per_s": st["completed"] / st["busy_s"], "busy_s": st["busy_s"], "trace_span_s": span,
@@ -252,6 +256,8 @@ def serve(G, ctxs, reqs, budget, plain):
         "completed": st["completed"], "peak_active": st["peak_active"], "max_batch": st["max_batch"],
         "peak_arena_bytes": st["peak_bytes"], "arena_bytes": st["arena_bytes"],
         "resident_bytes": st["resident_bytes"], "tuned_batch_shapes": tuned,
+        "largest_completion_gap_ms": {"ms": float(gaps[g] * 1e3), "after_s": float(fin[g] - fin[0])
+                                      if len(fin) > 1 else 0.0, "completed_before": g + 1},
     }
 
 
@@ -267,6 +273,11 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
         owner = shard_requests(len(reqs), budgets)
         reqs = [r for r, o in zip(reqs, owner) if o == dist.get_rank()]
     budget = resident + arena
+    # untimed warm-up traces (the head of the same trace): the first trace a
+    # process serves ran at 15.0-15.4k ops/s with p50 over 200 ms where later
+    # ones held 15.8k and 165 ms
+    serve(G, ctxs, reqs[:SERVE_WARMUP], budget, plain=False)
+    serve(G, ctxs, reqs[:SERVE_WARMUP // 4], budget, plain=True)
     served = serve(G, ctxs, reqs, budget, plain=False)
     plain = serve(G, ctxs, reqs, budget, plain=True)
     for c in ctxs:
@@ -275,6 +286,8 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
            "hbm_budget_bytes": budget, "inputs": "seeded residues generated on the device at admission",
            "admission": f"served form: FIFO, at most {SERVE_MAX_ACTIVE} requests active at once; plain form: one "
                         "request at a time",
+           "warmup": f"untimed: the trace's first {SERVE_WARMUP} requests (served) and {SERVE_WARMUP // 4} (plain) "
+                     "on fresh servers before the timed traces",
            "served": served, "plain": plain, "served_vs_plain_ops": served["ops_per_s"] / plain["ops_per_s"]}
     if dist is not None:
         # whole-job rates: all ranks' operations over the slowest rank's busy time

@@ -4,6 +4,9 @@
 # reference tree; its sources are compiled in place, read-only.
 #   libref_host.so : params.cpp + ks_constants.cpp + encode.cpp (CPU only)
 #   libref_gpu.so  : every src/*.cpp and kernels/*.cu for sm_100a
+#   ref_test_boot  : the reference's composed-bootstrap test program
+#                    (tests/test_boot.cpp) with the same sources, for timing
+#                    the reference's own bootstrap beside this library's
 # Usage: sh oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -e
 REF=${1:-${REF:-/root/reference}}
@@ -22,4 +25,7 @@ NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
     -gencode arch=compute_100a,code=sm_100a \
     -I"$REF/include" "$REF"/src/*.cpp "$REF"/kernels/*.cu \
     "$HERE/ref_shim_gpu.cpp" -Xlinker -Bsymbolic -o "$OUT/libref_gpu.so"
-echo "built $OUT/libref_host.so $OUT/libref_gpu.so"
+"$NVCC" -std=c++17 -O2 -ccbin /usr/bin/g++ -gencode arch=compute_100a,code=sm_100a \
+    -I"$REF/include" "$REF"/src/*.cpp "$REF"/kernels/*.cu "$REF/tests/test_boot.cpp" \
+    -o "$OUT/ref_test_boot"
+echo "built $OUT/libref_host.so $OUT/libref_gpu.so $OUT/ref_test_boot"

@@ -298,7 +298,6 @@ def negacyclic_int(a, s):
 
 
 def test_bootstrap():
-    t_start = time.time()
     B = Boot()
     G, Q = B.G, B.Q
     q0 = int(Q[0])
@@ -314,10 +313,22 @@ def test_bootstrap():
     G.check(G.lib().gpufhe_encrypt_batch(B.full.h, 1, 1, np.ascontiguousarray(mz).ctypes.data,
                                          (C.c_uint64 * 1)(303), ptr(a1), ptr(b1), 1, 3.19, parr([c0]), parr([c1]),
                                          None))
+    # stage clock as the reference's (test_boot.cpp:112, 536-543), checks excluded
+    laps, mark = {}, [0.0]
+
+    def lap(name=None):
+        sync()
+        now = time.time()
+        if name:
+            laps[name] = laps.get(name, 0.0) + now - mark[0]
+        mark[0] = now
+
+    lap()
 
     # 1. ModRaise and the reference's congruence gate
     R0, R1 = empty(SQ * N), empty(SQ * N)
     G.check(G.lib().gpufhe_modraise_batch(B.full.h, 1, SQ, parr([c0]), parr([c1]), parr([R0]), parr([R1]), None))
+    lap("modraise")
     zero = empty(N)
     a0c = B.decrypt((c0, zero))                      # centred c0, c1 at q0 (decrypt_host with a zero partner)
     a1c = B.decrypt((c1, zero))
@@ -332,12 +343,16 @@ def test_bootstrap():
     aq = np.array([float(v) / q0 for v in aref])     # slots after C2S: y_k = (a_k + i a_{k+S}) / q0
 
     # rotation keys: every stage offset, seed 4000 + offset; conjugation, seed 7400
+    lap()
     c2s = [stage_diagonals(g, False) for g in range(LST)]
+    lap("c2s")
     s2c = {g: stage_diagonals(g, True) for g in range(LST)}
+    lap("s2c")
     offsets = sorted(({d for o, _ in c2s for d in o} | {d for g in s2c for d in s2c[g][0]}) - {0})
     assert len(offsets) == 75
     keys0 = B.rotation_keys([(pow(5, d, M), 4000 + d) for d in offsets] + [(M - 1, 7400)],
                             copy=[pow(5, d, M) for d in c2s[0][0] if d])
+    lap("rotation_keys")
 
     # 2. CoeffsToSlots: declared input scale q0, the scale held flat through
     #    the first two stages (diagonals encoded at the modulus being dropped)
@@ -351,27 +366,31 @@ def test_bootstrap():
         sc = sc * dpt / B.qd[tw - 1]
         tw -= 1
     nt, s_out = tw, sc
-    sync()
+    lap("c2s")
     v = B.enc.decode(B.decrypt(ct), s_out)
     ref = aq[:S] + 1j * aq[S:]
     perm = np.array([brev(k) for k in range(S)])
     err_c2s = np.max(np.abs(v[perm] - ref))
 
     # 3. real / imaginary split by conjugation
+    lap()
     (k0, k1), = B.rotate_many(ct, [M - 1], nt)
     ctR = Ct(*B.op(G.PW_ADD, ct, (k0, k1), nt), nt, s_out)
     ctI = Ct(*B.op(G.PW_SUB, ct, (k0, k1), nt), nt, s_out)
+    lap("split")
 
     # 4. EvalMod on both branches
     aaff, baff = 2 * math.pi / 2.0 ** RDBL, -(math.pi / 2) / 2.0 ** RDBL
     cc = chebyshev_cos(DEG)
     oR = B.evalmod(ctR, complex(aaff / 2.0, 0), cc, baff)
     oI = B.evalmod(ctI, complex(0, -aaff / 2.0), cc, baff)
+    lap("evalmod")
     assert oR.tw == oI.tw == nt - (1 + (DEG - 1) + 1 + RDBL)
     vR = B.enc.decode(B.decrypt((oR.c0, oR.c1)), oR.scale)
     err_mod = np.max(np.abs(vR.real - np.sin(2 * math.pi * aq[perm])))
 
     # 5. SlotsToCoeffs: the imaginary branch folded into the first stage
+    lap()
     ct, tw, sc = None, oR.tw, oR.scale
     for g in range(LST - 1, -1, -1):
         offs, dg = s2c[g]
@@ -380,16 +399,19 @@ def test_bootstrap():
         ct = B.fft_stage(srcs, offs, dg, tw, dpt)
         sc = sc * dpt / B.qd[tw - 1]
         tw -= 1
+    lap("s2c")
 
     # 6. decrypt, decode at the final scale, compare with z
     d_final = sc * 2 * math.pi * DELTA_IN / q0
     zf = B.enc.decode(B.decrypt(ct), d_final)
-    sync()
+    lap("decrypt_decode")
     err = np.max(np.abs(zf - z))
-    secs = time.time() - t_start
     print(f"\nbootstrap n={N}: ModRaise congruence mismatches {bad}; C2S slot err {err_c2s:.3e}; "
           f"EvalMod(R) err {err_mod:.3e}; output towers {tw}; {len(offsets) + 1} rotation keys; "
-          f"max |boot(z) - z| = {err:.3e}; {secs:.1f} s including keys and host diagonals")
+          f"max |boot(z) - z| = {err:.3e}")
+    print("bootstrap seconds (checks excluded; c2s and s2c include their host diagonals, evalmod its "
+          "per-level relinearisation keys): " + ", ".join(f"{k} {v:.3f}" for k, v in laps.items())
+          + f"; total {sum(laps.values()):.3f}")
     assert tw == SQ - 2 * LST - (1 + (DEG - 1) + 1 + RDBL)
     assert err < 2e-2, err
 
