@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the resident leveled-CKKS hot path.
  *
- * TEST INFRASTRUCTURE ONLY: the checker for tests/, __graft_entry__.smoke()
+ * TEST INFRASTRUCTURE ONLY: the reference result for tests/, __graft_entry__.smoke()
  * and the CPU-baseline leg of bench.py. It is a scalar restatement of the
  * reference's formulas (samfrazerdutton/GPU-Resident-Library); each function
  * names the reference file:line it follows. No CUDA, no product code.

@@ -160,8 +160,8 @@ def main():
         json.dump(config1(R), f, indent=1)
     with open(os.path.join(HERE, "rotation_golden.json"), "w") as f:
         json.dump(rotation(R), f, indent=1)
-    out = os.path.join(ROOT, "gpurun_out")
-    if os.path.isdir(out):
+    out = os.environ.get("GOLDEN_COPY_DIR")      # optional second copy of the GPU-made vectors
+    if out and os.path.isdir(out):
         import shutil
         for name in ("config1_golden.json", "rotation_golden.json"):
             shutil.copy(os.path.join(HERE, name), os.path.join(out, name))
