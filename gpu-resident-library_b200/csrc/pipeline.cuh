@@ -237,7 +237,7 @@ __device__ __forceinline__ void p1_inv_row_body(const DevCtx& D, const PairDesc*
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 4)
 p1_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
@@ -265,7 +265,7 @@ __device__ __forceinline__ void p2_inv_col_body(const DevCtx& D, const PairDesc*
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 4)
 p2_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -321,7 +321,7 @@ __device__ __forceinline__ void p3_modup_fwd_col_body(const DevCtx& D, const Pai
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 4)
 p3_modup_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -460,7 +460,7 @@ __device__ __forceinline__ void p4_modup_fwd_row_body(const DevCtx& D, const Pai
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 4)
 p4_modup_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
@@ -1116,7 +1116,7 @@ __device__ __forceinline__ void p6_moddown_inv_row_body(const DevCtx& D, const P
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 4)
 p6_moddown_inv_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
@@ -1150,7 +1150,7 @@ __device__ __forceinline__ void p7a_moddown_inv_col_body(const DevCtx& D, const 
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 4)
 p7a_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -1190,7 +1190,7 @@ __device__ __forceinline__ void p7b_moddown_inv_col_body(const DevCtx& D, const 
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 4)
 p7b_moddown_inv_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -1291,7 +1291,7 @@ __device__ __forceinline__ void p8_moddown_fwd_col_body(const DevCtx& D, const P
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::COL_THREADS, 4)
 p8_moddown_fwd_col(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::COL_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::COL_TILES;
@@ -1340,7 +1340,7 @@ __device__ __forceinline__ void p9_final_fwd_row_body(const DevCtx& D, const Pai
 }
 
 template <int LOGN, int PATH>
-__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, PATH == 1 ? 4 : 3)
+__global__ void __launch_bounds__(ntt::Geo<LOGN>::ROW_THREADS, 4)
 p9_final_fwd_row(const DevCtx D, const PairDesc* __restrict__ pairs, const uint2* __restrict__ jobs) {
     uint2 jb = jobs[blockIdx.x / ntt::Geo<LOGN>::ROW_TILES];
     const u32 tile = blockIdx.x % ntt::Geo<LOGN>::ROW_TILES;
