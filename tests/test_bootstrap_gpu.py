@@ -58,6 +58,12 @@ def parr(ts):
     return (C.c_void_p * len(ts))(*[ptr(t) for t in ts])
 
 
+def to_int128(lo, hi):
+    """Two's-complement 128-bit integer from its low and high 64-bit words."""
+    v = int(lo) | (int(hi) << 64)
+    return v - (1 << 128) if v >> 127 else v
+
+
 def brev(i):
     return int(format(i, f"0{LGS}b")[::-1], 2)
 
@@ -190,8 +196,7 @@ class Boot:
         out = np.zeros((1, N, 2), np.uint64)
         self.G.check(self.G.lib().gpufhe_decrypt_crt_batch(self.full.h, 1, towers, parr([a[0]]), parr([a[1]]),
                                                            ptr(self.s), out.ctypes.data, None))
-        return [int(lo) | (int(hi) << 64) if hi < (1 << 63) else (int(lo) | (int(hi) << 64)) - (1 << 128)
-                for lo, hi in out[0]]
+        return [to_int128(lo, hi) for lo, hi in out[0]]
 
     # ---------------------------------------------------------------- the reference's lambdas
     def lvl(self, A, tw):
