@@ -273,6 +273,12 @@ struct WorkImpl {
 
 namespace gpufhe {
 
+// The reference's A/B switch between its batched and per-digit inner-product
+// launches. Here every keyswitch is one fused plan whatever the value; both of
+// the reference's settings give the same bits, so the flag is accepted and
+// read by nothing.
+bool g_ks_batched = true;
+
 // ---------------------------------------------------------------- DeviceCiphertext
 DeviceCiphertext::DeviceCiphertext(Scheme scheme, uint32_t n, uint32_t num_towers)
     : scheme_(scheme), n_(n), towers_(num_towers) {

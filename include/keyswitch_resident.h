@@ -7,6 +7,14 @@
 
 namespace gpufhe {
 
+/* A/B switch the reference defines beside its keyswitch (reference
+ * src/keyswitch_resident.cpp:16) and its rotation test writes
+ * (tests/test_rot_resident.cpp:17,188-200) to time its batched inner product
+ * against one launch per digit. This library runs every keyswitch as one fused
+ * plan; the variable exists so such callers link, and its value changes
+ * neither the launches nor the result. */
+extern bool g_ks_batched;
+
 /* Shared read-only device state for one level: constants, eval key, root
  * tables (reference include/keyswitch_resident.h:11-29). Built once by
  * ks_context_create; any number of streams may use it concurrently, each

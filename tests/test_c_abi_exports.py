@@ -81,3 +81,11 @@ def test_no_link_time_driver_dependency():
     points, so it loads (and the CPU tests run) where no driver is installed."""
     out = subprocess.run(["readelf", "-d", LIB], capture_output=True, text=True, check=True).stdout
     assert "libcuda.so" not in out
+
+
+def test_reference_globals_exported():
+    """Variables the reference's test programs declare and write
+    (gpufhe::g_ks_batched in tests/test_rot_resident.cpp:17) are data symbols
+    of the library, so those programs link unchanged."""
+    out = subprocess.run(["nm", "-DC", "--defined-only", LIB], capture_output=True, text=True, check=True).stdout
+    assert re.search(r"\s[BD]\s+gpufhe::g_ks_batched$", out, re.M), "gpufhe::g_ks_batched not exported"
