@@ -4,36 +4,15 @@
 #include <stdexcept>
 
 #include "hostmath.hpp"
+#include "params.h"
 
 namespace gfx {
 
 namespace {
 thread_local std::string g_err;
 
-using hm::u128;
-
-// a*b mod m for m < 2^127 (shift-and-add; setup only).
-u128 mulmod128(u128 a, u128 b, u128 m) {
-    a %= m;
-    u128 r = 0;
-    while (b) {
-        if (b & 1) { r += a; if (r >= m) r -= m; }
-        a <<= 1; if (a >= m) a -= m;
-        b >>= 1;
-    }
-    return r;
-}
-
-// smallest generator-derived primitive 2n-th root (same search as the
-// reference's native_root, params.cpp:42-48)
-u64 native_root(uint32_t n, u64 q) {
-    const u64 M = 2ull * n;
-    for (u64 g = 2; g < q; ++g) {
-        u64 c = hm::powmod(g, (q - 1) / M, q);
-        if (hm::powmod(c, n, q) == q - 1) return c;
-    }
-    throw std::runtime_error("no primitive 2n-th root of unity");
-}
+// the reference's root choice (params.cpp:42-48), from this library's params.cu
+u64 native_root(uint32_t n, u64 q) { return gpufhe::native_root(n, q); }
 }  // namespace
 
 std::string last_error() { return g_err; }
@@ -149,20 +128,15 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
             }
         }
         if (L >= 2) {
-            // params.cpp:54-75: s1 = ql^-1 mod q_i, s2 = floor(Ql*u/ql) mod q_i
+            // s1 = ql^-1 mod q_i and s2 = floor(Ql*u/ql) mod q_i (params.cpp:54-75),
+            // which equals q_i - s1 (the derivation is at native_rescale_consts)
             const uint32_t last = L - 1;
-            const u64 ql = Q[last];
-            u64 QlModql = 1 % ql;
-            for (uint32_t t = 0; t < last; ++t) QlModql = hm::mulmod(QlModql, Q[t] % ql, ql);
-            const u64 u = hm::invmod(QlModql, ql);
+            std::vector<u64> s1, s2;
+            gpufhe::native_rescale_consts(s1, s2, Q, last);
             for (uint32_t i = 0; i < last; ++i) {
                 const u64 qi = Q[i];
-                lv.s1[i] = hm::invmod(ql % qi, qi);
-                u128 m2 = (u128)ql * qi, Ql2 = 1 % m2;
-                for (uint32_t t = 0; t < last; ++t) Ql2 = mulmod128(Ql2, Q[t], m2);
-                u128 prod = mulmod128(Ql2, u, m2);
-                u128 pm1 = prod == 0 ? m2 - 1 : prod - 1;
-                lv.s2[i] = (u64)((pm1 / ql) % qi);
+                lv.s1[i] = s1[i];
+                lv.s2[i] = s2[i];
                 lv.s1p[i] = hm::precon(lv.s1[i], qi);
                 lv.s1r[i] = hm::mulmod(lv.s1[i], rmod(qi), qi);
                 lv.s1rp[i] = hm::precon(lv.s1r[i], qi);

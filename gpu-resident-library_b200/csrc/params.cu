@@ -4,6 +4,7 @@
 // Exposed as the reference's C++ functions (namespace gpufhe, include/params.h)
 // and as C entry points for non-C++ callers (include/gpufhe_b200.h).
 #include <cstring>
+#include <string>
 #include <stdexcept>
 #include <vector>
 
@@ -13,7 +14,6 @@
 #include "params.h"
 
 namespace {
-using hm::u128;
 
 bool is_prime(uint64_t x) {
     if (x < 2) return false;
@@ -35,16 +35,6 @@ bool is_prime(uint64_t x) {
     return true;
 }
 
-u128 mulmod128(u128 a, u128 b, u128 m) {
-    a %= m;
-    u128 r = 0;
-    while (b) {
-        if (b & 1) { r += a; if (r >= m) r -= m; }
-        a <<= 1; if (a >= m) a -= m;
-        b >>= 1;
-    }
-    return r;
-}
 }  // namespace
 
 namespace gpufhe {
@@ -55,7 +45,9 @@ void native_primes(std::vector<uint64_t>& out, uint32_t count, uint32_t bits, ui
     const uint64_t M = 2ull * n;
     uint64_t q = ((1ull << bits) / M) * M + 1;
     while (out.size() < count) {
-        if (q < (1ull << (bits - 1))) throw std::runtime_error("prime search exhausted");
+        if (q < (1ull << (bits - 1)))
+            throw std::runtime_error("native_primes: fewer than the requested count of " + std::to_string(bits) +
+                                     "-bit primes q = 1 mod 2n outside the avoid list");
         bool skip = false;
         for (uint64_t a : avoid) if (a == q) skip = true;
         if (!skip && is_prime(q)) out.push_back(q);
@@ -65,29 +57,34 @@ void native_primes(std::vector<uint64_t>& out, uint32_t count, uint32_t bits, ui
 
 uint64_t native_root(uint32_t n, uint64_t q) {
     const uint64_t M = 2ull * n;
+    if (n == 0 || q < 3 || (q - 1) % M != 0)
+        throw std::runtime_error("native_root: q - 1 is not a multiple of 2n, so q has no primitive 2n-th root");
     for (uint64_t g = 2; g < q; ++g) {
         uint64_t c = hm::powmod(g, (q - 1) / M, q);
         if (hm::powmod(c, n, q) == q - 1) return c;
     }
-    throw std::runtime_error("no 2n-th root");
+    throw std::runtime_error("native_root: no element of order 2n below q (q is not prime)");
 }
 
+// Rescale constants for dropping tower `last` of mod[0..last]. With
+// Q_l = mod[0] * ... * mod[last-1], q_l = mod[last] and u = Q_l^-1 mod q_l,
+// the reference defines s1[i] = q_l^-1 mod q_i and
+// s2[i] = floor(Q_l * u / q_l) mod q_i. Because Q_l * u = 1 (mod q_l), the
+// division is exact after subtracting one: floor(Q_l * u / q_l) =
+// (Q_l * u - 1) / q_l. Every q_i with i < last divides Q_l, so modulo q_i the
+// numerator is -1 and s2[i] = -q_l^-1 = q_i - s1[i]. The rescale
+// a * s1 + b * s2 is then (a - b) * q_l^-1, as it must be.
 void native_rescale_consts(std::vector<uint64_t>& s1, std::vector<uint64_t>& s2, const std::vector<uint64_t>& mod,
                            uint32_t last) {
+    if (last >= mod.size()) throw std::invalid_argument("native_rescale_consts: tower index beyond the modulus list");
     const uint64_t ql = mod[last];
     s1.resize(last);
     s2.resize(last);
-    uint64_t QlModql = 1 % ql;
-    for (uint32_t t = 0; t < last; ++t) QlModql = hm::mulmod(QlModql, mod[t] % ql, ql);
-    const uint64_t u = hm::invmod(QlModql, ql);
     for (uint32_t i = 0; i < last; ++i) {
         const uint64_t qi = mod[i];
+        if (ql % qi == 0) throw std::invalid_argument("native_rescale_consts: moduli are not coprime");
         s1[i] = hm::invmod(ql % qi, qi);
-        u128 m2 = (u128)ql * qi, Ql2 = 1 % m2;
-        for (uint32_t t = 0; t < last; ++t) Ql2 = mulmod128(Ql2, mod[t], m2);
-        u128 prod = mulmod128(Ql2, u, m2);
-        u128 pm1 = prod == 0 ? m2 - 1 : prod - 1;
-        s2[i] = (uint64_t)((pm1 / ql) % qi);
+        s2[i] = qi - s1[i];
     }
 }
 
@@ -116,7 +113,12 @@ uint64_t gpufhe_native_root(uint32_t n, uint64_t q) {
 int gpufhe_rescale_consts(uint64_t* s1, uint64_t* s2, const uint64_t* mod, uint32_t last) {
     if (!s1 || !s2 || !mod) return GPUFHE_EINVAL;
     std::vector<uint64_t> a, b, m(mod, mod + last + 1);
-    gpufhe::native_rescale_consts(a, b, m, last);
+    try {
+        gpufhe::native_rescale_consts(a, b, m, last);
+    } catch (const std::exception& e) {
+        gfx::set_error(e.what());
+        return GPUFHE_EINVAL;
+    }
     std::memcpy(s1, a.data(), last * 8);
     std::memcpy(s2, b.data(), last * 8);
     return GPUFHE_OK;

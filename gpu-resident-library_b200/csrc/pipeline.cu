@@ -4,6 +4,8 @@
 // captured in a CUDA graph and replayed.
 #include "pipeline.hpp"
 
+#include "devonce.hpp"
+
 #include <algorithm>
 #include <cstring>
 #include <map>
@@ -14,15 +16,7 @@ namespace pl {
 
 namespace {
 
-int sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-    }
-    return n;
-}
+int sm_count() { return gfx::current_sm_count(); }
 
 // PATH 0 / 1: the integer / FP64 job segment of a phase; PATH 2: the mixed
 // segment (both kinds interleaved, one launch).
@@ -66,13 +60,16 @@ struct Variant {
 
 template <int LOGN>
 struct Launcher {
-    // Kernel attributes, once per ring size. The P5 forms' dynamic shared
-    // memory grows with dnum, so their limits are set to the largest size any
-    // context can ask for (a limit set for the first context's dnum would be
-    // too low for a later context with a different one).
+    // Kernel attributes, once per ring size and device (and thread-safe). The
+    // P5 forms' dynamic shared memory grows with dnum, so their limits are set
+    // to the largest size any context can ask for (a limit set for the first
+    // context's dnum would be too low for a later context with a different
+    // one).
     static void attrs(uint32_t) {
-        static bool done = false;
-        if (done) return;
+        static gfx::DeviceOnce once;
+        once(set_attrs);
+    }
+    static void set_attrs() {
         Variant<LOGN, 0>::attrs();
         Variant<LOGN, 1>::attrs();
         Variant<LOGN, 2>::attrs();
@@ -83,7 +80,6 @@ struct Launcher {
         cudaFuncSetAttribute(p5_mac<LOGN, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
         cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_ASYNC_SMEM_MAX);
         cudaFuncSetAttribute(p5_mac_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
-        done = true;
     }
     // persistent warp-specialised P3 over job segment PATH: form 1 = 128
     // conversion threads, two CTAs per SM; form 2 = 256, one CTA per SM

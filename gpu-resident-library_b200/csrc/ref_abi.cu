@@ -11,6 +11,7 @@
 #include "gf.cuh"
 #include "hostmath.hpp"
 #include "xform.cuh"
+#include "devonce.hpp"
 
 namespace {
 
@@ -271,9 +272,16 @@ void LaunchApproxSwitchCRTBasis(const uint64_t* d_src, uint64_t* d_dst, const ui
                                 cudaStream_t s) {
     int threads = 128;
     size_t smem = (size_t)sizeQ * threads * 8;
-    if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_approx_switch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    }
+    // the limit only caps what a launch may ask for: raise it once per device
+    // to the opt-in maximum, so concurrent callers with different sizeQ never
+    // lower it under one another
+    static gfx::DeviceOnce attrs;
+    attrs([] {
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
+            cudaFuncSetAttribute(k_approx_switch, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    });
     unsigned blocks = (unsigned)(((uint64_t)n + threads - 1) / threads);
     k_approx_switch<<<blocks, threads, smem, s>>>(d_src, d_dst, d_QHatInvModq, d_QHatInvModqPrecon, d_q,
                                                   d_QHatModp, d_p, d_mu_lo, d_mu_hi, sizeQ, sizeP, n);

@@ -1,18 +1,19 @@
 #include "xform.cuh"
 
+#include "devonce.hpp"
+
 namespace {
 
 template <int LOGN, bool SINGLE>
 cudaError_t launch_t(const xf::Job* jobs, const xf::Job* one, int njobs, bool inverse, cudaStream_t s) {
     using G = ntt::Geo<LOGN>;
-    static bool attr_done = false;
-    if (!attr_done) {
+    static gfx::DeviceOnce attrs;   // shared-memory limits, once per device
+    attrs([] {
         cudaFuncSetAttribute(xf::k_fwd_col<LOGN, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
         cudaFuncSetAttribute(xf::k_inv_col<LOGN, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::COL_SMEM);
         cudaFuncSetAttribute(xf::k_fwd_row<LOGN, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
         cudaFuncSetAttribute(xf::k_inv_row<LOGN, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::ROW_SMEM);
-        attr_done = true;
-    }
+    });
     const xf::Job o = one ? *one : xf::Job{};
     if (!inverse) {
         xf::k_fwd_col<LOGN, SINGLE><<<njobs * G::COL_TILES, G::COL_THREADS, G::COL_SMEM, s>>>(jobs, o);

@@ -178,3 +178,34 @@ def test_keyswitch_reuse_across_levels():
         ql = int(ctx.Q[L - 1])
         got = [round(v * ql / (D * D)) for v in dec[:11]]
         assert got == [4, 0, 0, 0, 0, -12, 0, 0, 0, 0, 9], L
+
+
+@needs_ref
+@pytest.mark.parametrize("L", [2, 4, 7, 12, 24])
+def test_library_rescale_consts_match_reference(L):
+    """The library's own rescale constants (host code, no GPU call): s1 from
+    the inverse of the dropped prime, s2 = q_i - s1 by the exact-division
+    identity. Same values as the reference's params.cpp and as the big-integer
+    definition floor(Ql * (Ql^-1 mod ql) / ql) mod q_i."""
+    import gpufhe_b200 as G
+    n = 1 << 14
+    mods = np.concatenate([O.native_primes(1, 60, n), O.native_primes(L - 1, 50, n)])
+    s1, s2 = np.zeros(L - 1, np.uint64), np.zeros(L - 1, np.uint64)
+    assert G.lib().gpufhe_rescale_consts(s1.ctypes.data, s2.ctypes.data, mods.ctypes.data, L - 1) == 0
+    r1, r2 = np.zeros(L - 1, np.uint64), np.zeros(L - 1, np.uint64)
+    REF.ref_rescale_consts(r1, r2, mods, L, L - 1)
+    assert np.array_equal(s1, r1) and np.array_equal(s2, r2)
+    Ql = 1
+    for q in mods[: L - 1]:
+        Ql *= int(q)
+    ql = int(mods[L - 1])
+    D = Ql * pow(Ql % ql, -1, ql) // ql
+    assert [D % int(q) for q in mods[: L - 1]] == [int(x) for x in s2]
+
+
+def test_library_rescale_consts_reject_non_coprime():
+    import gpufhe_b200 as G
+    mods = np.array([97, 193, 97], np.uint64)
+    s1, s2 = np.zeros(2, np.uint64), np.zeros(2, np.uint64)
+    assert G.lib().gpufhe_rescale_consts(s1.ctypes.data, s2.ctypes.data, mods.ctypes.data, 2) == -1
+    assert b"coprime" in G.lib().gpufhe_last_error()
