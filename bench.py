@@ -183,6 +183,10 @@ SERVE_ROT_STEPS = (1, 2, 4, 8, -1, -2, -4, -8)
 # to 10.7-14.3k ops/s with p50 up to 690 ms, while at 384 repeated runs held
 # 15.7-15.8k ops/s and p50 160-180 ms.
 SERVE_MAX_ACTIVE = 384
+# A second served trace at an arrival rate below the served throughput (about
+# 16k operations/s against about 9 operations per request), so that p50/p99
+# measure service in a steady state rather than the growth of the queue.
+SERVE_SUSTAINED_RATE = 1500.0
 SERVE_WARMUP = 400                  # requests in the untimed warm-up trace of the served form
 SERVE_WORKLOAD = ("serving trace: Poisson arrivals at 2000 req/s (seeded); per request N in {2^14,2^15,2^16}, "
                   "towers U[4,24], depth U[1,10] of EvalMult+Rescale (capped at towers-1) with U[0,8] rotations "
@@ -194,29 +198,44 @@ def galois_element(r, n):
     return pow(5, r, M) if r >= 0 else pow(pow(5, -r, M), -1, M)
 
 
+def serving_chain(primes_fn, lg):
+    """Ring size and chain of one serving context: Q = 1x60 + 23x50, P = 8x60."""
+    n = 1 << lg
+    q0 = primes_fn(1, 60, n)
+    qs = primes_fn(SERVE_TOWERS - 1, 50, n, avoid=list(q0))
+    Q = np.concatenate([q0, qs])
+    P = primes_fn(SERVE_K, 60, n, avoid=list(Q))
+    return n, Q, P
+
+
+def serving_keys(lg):
+    """(key id, av, bv) of every serving key at ring size 2^lg: the
+    relinearisation key (id 0) and one key per rotation step (id = Galois
+    element), seeded material below every prime of the chain."""
+    n = 1 << lg
+    rows = -(-SERVE_TOWERS // SERVE_ALPHA) * (SERVE_TOWERS + SERVE_K)
+    rng = np.random.default_rng(SEED + lg)
+    pool = rng.integers(0, 1 << 49, 2 * rows * n, dtype=np.uint64)
+    for j, k in enumerate([0] + [galois_element(r, n) for r in SERVE_ROT_STEPS]):
+        key = np.roll(pool, 7919 * j)                                  # distinct material per key
+        yield k, key[: rows * n], key[rows * n:]
+
+
 def serving_contexts(G, device):
     """One context per ring size with a relinearisation key and one key per rotation step."""
     ctxs = []
     for lg in SERVE_LOGNS:
-        n = 1 << lg
-        q0 = G.native_primes(1, 60, n)
-        qs = G.native_primes(SERVE_TOWERS - 1, 50, n, avoid=list(q0))
-        Q = np.concatenate([q0, qs])
-        P = G.native_primes(SERVE_K, 60, n, avoid=list(Q))
+        n, Q, P = serving_chain(G.native_primes, lg)
         c = G.Context(n, Q, P, SERVE_ALPHA, device=device)
-        rows = -(-SERVE_TOWERS // SERVE_ALPHA) * (SERVE_TOWERS + SERVE_K)
-        rng = np.random.default_rng(SEED + lg)
-        pool = rng.integers(0, 1 << 49, 2 * rows * n, dtype=np.uint64)   # below every prime of the chain
-        for j, k in enumerate([0] + [galois_element(r, n) for r in SERVE_ROT_STEPS]):
-            key = np.roll(pool, 7919 * j)                                  # distinct material per key
-            c.set_key(k, key[: rows * n], key[rows * n:])
+        for k, av, bv in serving_keys(lg):
+            c.set_key(k, av, bv)
         ctxs.append(c)
     return ctxs
 
 
-def serving_trace(count, seed):
+def serving_trace(count, seed, rate=SERVE_RATE):
     rng = np.random.default_rng(seed)
-    arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, count))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
     reqs = []
     for i in range(count):
         c = int(rng.integers(0, len(SERVE_LOGNS)))
@@ -265,6 +284,7 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
     """The trace on this rank's share of requests (all of it at N=1)."""
     ctxs = serving_contexts(G, device)
     reqs = serving_trace(count, SEED + 5)
+    reqs_s = serving_trace(count, SEED + 5, rate=SERVE_SUSTAINED_RATE)
     resident = sum(c.resident_bytes() for c in ctxs)
     arena = min(int(free_bytes * 0.6), 80 << 30)
     if dist is not None:
@@ -272,6 +292,7 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
         dist.all_gather_object(budgets, arena)
         owner = shard_requests(len(reqs), budgets)
         reqs = [r for r, o in zip(reqs, owner) if o == dist.get_rank()]
+        reqs_s = [r for r, o in zip(reqs_s, owner) if o == dist.get_rank()]
     budget = resident + arena
     # untimed warm-up traces (the head of the same trace): the first trace a
     # process serves ran at 15.0-15.4k ops/s with p50 over 200 ms where later
@@ -280,6 +301,8 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
     serve(G, ctxs, reqs[:SERVE_WARMUP // 4], budget, plain=True)
     served = serve(G, ctxs, reqs, budget, plain=False)
     plain = serve(G, ctxs, reqs, budget, plain=True)
+    sustained = serve(G, ctxs, reqs_s, budget, plain=False)
+    check = serving_check_run(G, ctxs, reqs, budget)
     for c in ctxs:
         c.close()
     out = {"workload": SERVE_WORKLOAD, "requests": count, "requests_this_rank": len(reqs),
@@ -288,7 +311,13 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
                         "request at a time",
            "warmup": f"untimed: the trace's first {SERVE_WARMUP} requests (served) and {SERVE_WARMUP // 4} (plain) "
                      "on fresh servers before the timed traces",
-           "served": served, "plain": plain, "served_vs_plain_ops": served["ops_per_s"] / plain["ops_per_s"]}
+           "served": served, "plain": plain, "served_vs_plain_ops": served["ops_per_s"] / plain["ops_per_s"],
+           "served_at_sustained_rate": {"arrival_rate_per_s": SERVE_SUSTAINED_RATE,
+                                        "latency_ms": sustained["latency_ms"],
+                                        "service_latency_ms": sustained["service_latency_ms"],
+                                        "ops_per_s": sustained["ops_per_s"], "peak_active": sustained["peak_active"],
+                                        "trace_span_s": sustained["trace_span_s"]},
+           "_check": check}
     if dist is not None:
         # whole-job rates: all ranks' operations over the slowest rank's busy time
         for form in ("served", "plain"):
@@ -297,6 +326,30 @@ def run_serving(G, device, count, free_bytes, dist=None, dev=None):
             emr = sum_over_ranks(out[form]["evalmult_rescale_ops"], dist, dev)
             out[form]["job_ops_per_s"] = ops / busy
             out[form]["job_evalmult_rescale_ops_per_s"] = emr / busy
+    return out
+
+
+def serving_check_run(G, ctxs, reqs, budget, per_ring=2):
+    """Untimed: the first `per_ring` requests of each ring size of the trace,
+    with seeded host inputs, served together in the served form; returns the
+    requests and their results for the oracle check in the CPU leg."""
+    picked = []
+    for c in range(len(SERVE_LOGNS)):
+        picked += [r for r in reqs if r[0] == c][:per_ring]
+    srv = G.Server(ctxs, budget, max_active=SERVE_MAX_ACTIVE)
+    rng = np.random.default_rng(SEED + 77)
+    out = []
+    for i, (c, L, ops, _) in enumerate(picked):
+        n = 1 << SERVE_LOGNS[c]
+        _, Q, _ = serving_chain(G.native_primes, SERVE_LOGNS[c])
+        h_in = np.concatenate([rng.integers(0, int(q), n, dtype=np.uint64) for q in Q[:L]] * 2)
+        fin = L - sum(1 for m, _ in ops if m == 0)
+        h_out = np.zeros(2 * fin * n, np.uint64)
+        srv.submit(c, L, ops, arrival_s=0.0, seed=SEED + i, h_in=h_in, h_out=h_out)
+        out.append((c, L, ops, h_in, h_out))
+    srv.start()
+    srv.drain(300.0)
+    srv.close()
     return out
 
 
@@ -333,33 +386,125 @@ def sum_over_ranks(x, dist, dev):
 
 
 # ---------------------------------------------------------------- CPU oracle
-def cpu_port_rate(levels, n, nthreads, budget_s=20.0):
-    """Oracle (CPU restatement of the reference path) on a bounded sample."""
+def split_pairs(flat, levels, n, per_pair):
+    """Per-pair arrays of a batch laid out contiguously in op order:
+    per_pair arrays of L*n (inputs) or (L-1)*n (outputs) words each."""
+    out, off = [], 0
+    for L in levels:
+        words = (L if per_pair == 4 else L - 1) * n
+        out.append([flat[off + i * words: off + (i + 1) * words] for i in range(per_pair)])
+        off += per_pair * words
+    return out
+
+
+def cpu_port_rate(levels, n, nthreads, check=None, budget_s=20.0):
+    """Oracle (CPU restatement of the reference path) on the whole workload:
+    all pairs at their levels, OpenMP over pairs, repeated while the time
+    budget lasts. With `check` = (av, bv, inputs, outputs) of the GPU's timed
+    step it uses the same key and inputs, and its first repetition is also the
+    bit-for-bit check of every output of that step."""
     sys.path.insert(0, ROOT)
     import oracle as O
     Q, P = chain(O.native_primes, n)
     ctx = O.Ctx(n, Q, P, ALPHA)
     rng = np.random.default_rng(SEED + 7)
-    rows = ctx.dnum * (FULLQ + K_SPECIAL)
-    QP = ctx.QP
-    av = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
-    bv = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+    if check is not None:
+        av, bv, h_in, h_out = check
+        ins_pp = split_pairs(h_in, levels, n, 4)
+        ins = [[x[i] for x in ins_pp] for i in range(4)]
+    else:
+        rows = ctx.dnum * (FULLQ + K_SPECIAL)
+        QP = ctx.QP
+        av = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+        bv = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
+        ins = [[np.concatenate([rng.integers(0, int(q), n, dtype=np.uint64) for q in Q[:L]]) for L in levels]
+               for _ in range(4)]
     ctx.set_key(0, av, bv)
     threads = nthreads or O.num_threads()
-    sample = levels[:max(1, min(len(levels), threads))]
-    ins = [[np.concatenate([rng.integers(0, int(q), n, dtype=np.uint64) for q in Q[:L]]) for L in sample]
-           for _ in range(4)]
-    reps, t_total = 0, 0.0
+    reps, t_total, parity = 0, 0.0, None
     while True:
         t0 = time.perf_counter()
-        ctx.evalmult_rescale_batch(sample, *ins, nthreads=threads)
+        o0, o1 = ctx.evalmult_rescale_batch(levels, *ins, nthreads=threads)
         t_total += time.perf_counter() - t0
+        if check is not None and parity is None:
+            got = split_pairs(h_out, levels, n, 2)
+            bad = [j for j in range(len(levels))
+                   if not (np.array_equal(got[j][0], o0[j]) and np.array_equal(got[j][1], o1[j]))]
+            parity = {"pairs_checked": len(levels), "mismatched_pairs": bad,
+                      "result": "bit-exact" if not bad else f"{len(bad)} pairs differ",
+                      "what": "every output of the timed, graph-replayed step (tuned schedule) against the "
+                              "oracle on the same key and inputs"}
         reps += 1
-        if t_total > budget_s / 4 or reps >= 3:
+        if reps >= 2 and (t_total > budget_s / 2 or reps >= 3):
             break
-    return {"value": reps * len(sample) / t_total, "unit": "ops/s", "cores": threads, "kind": "port",
-            "sample": f"{len(sample)} pairs (levels {sample}) x {reps} reps of the same N=2^16 workload, "
-                      f"OpenMP over pairs"}
+    return {"value": reps * len(levels) / t_total, "unit": "ops/s", "cores": threads, "kind": "port",
+            "sample": f"the whole workload ({len(levels)} pairs, levels U{{4..12}}, mean "
+                      f"{float(np.mean(levels)):.2f}) x {reps} reps, N=2^16, OpenMP over pairs on {threads} host "
+                      f"threads", "parity": parity}
+
+
+def cpu_rotation_check(chk, n):
+    """Oracle check of the rotation batch's timed outputs: the keys are
+    regenerated from the seeds the GPU used (the GPU key generation is
+    bit-exact with the oracle's), then two plain rotations and three hoisted
+    rotations of one group are recomputed and compared bit for bit."""
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    q0 = O.native_primes(1, 60, n)
+    Q = np.concatenate([q0, O.native_primes(ROT_TOWERS - 1, 50, n, avoid=list(q0))])
+    P = O.native_primes(K_SPECIAL, 60, n, avoid=list(Q))
+    ctx = O.Ctx(n, Q, P, ALPHA)
+    T, L = ROT_TOWERS + K_SPECIAL, ROT_TOWERS
+    s, a, b = ctx.keygen(T, seed=SEED)
+    need = {p[0] for p in chk["plain"]} | {g for g, _, _ in chk["hoisted"][2]}
+    for j, g in enumerate(chk["galois"]):
+        if g in need:
+            av, bv = ctx.evalkeygen(s, ctx.automorph_eval(T, g, s), a, b, seed=SEED + 100 + j)
+            ctx.set_key(g, av, bv)
+    bad = []
+    for g, c0, c1, o0, o1 in chk["plain"]:
+        e0, e1 = ctx.rotate(L, g, c0, c1, g)
+        if not (np.array_equal(e0, o0) and np.array_equal(e1, o1)):
+            bad.append(f"plain {g}")
+    c0, c1, hs = chk["hoisted"]
+    ks = [g for g, _, _ in hs]
+    e0s, e1s = ctx.rotate_hoisted(L, ks, ks, c0, c1)
+    for r, (g, o0, o1) in enumerate(hs):
+        if not (np.array_equal(e0s[r], o0) and np.array_equal(e1s[r], o1)):
+            bad.append(f"hoisted {g}")
+    return {"checked": f"{len(chk['plain'])} plain rotations and {len(hs)} hoisted rotations of one group, from "
+                       "the timed replays", "mismatches": bad, "result": "bit-exact" if not bad else "differ"}
+
+
+def cpu_serving_check(chk):
+    """Oracle check of requests served together in the served form (one per
+    entry of chk: ring, level, operations, host input, served result)."""
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    ctxs = {}
+    bad = []
+    for c, L, ops, h_in, h_out in chk:
+        lg = SERVE_LOGNS[c]
+        if c not in ctxs:
+            n, Q, P = serving_chain(O.native_primes, lg)
+            o = O.Ctx(n, Q, P, SERVE_ALPHA)
+            used = {0} | {k for cc, _, oo, _, _ in chk if cc == c for m, k in oo if m == 2}
+            for k, av, bv in serving_keys(lg):
+                if k in used:
+                    o.set_key(k, av, bv)
+            ctxs[c] = (o, n)
+        o, n = ctxs[c]
+        c0, c1 = h_in[: L * n].copy(), h_in[L * n:].copy()
+        for m, k in ops:
+            if m == 0:
+                c0, c1 = o.evalmult_rescale(L, c0, c1, c0, c1)
+                L -= 1
+            else:
+                c0, c1 = o.rotate(L, k, c0, c1, k)
+        if not np.array_equal(np.concatenate([c0[: L * n], c1[: L * n]]), h_out):
+            bad.append(c)
+    return {"checked": f"{len(chk)} requests ({len(chk) // len(SERVE_LOGNS)} per ring size) served together",
+            "mismatches": bad, "result": "bit-exact" if not bad else "differ"}
 
 
 def cpu_keys_rate(n):
@@ -418,7 +563,7 @@ def run_reference(args):
     bv = np.concatenate([rng.integers(0, int(QP[r % len(QP)]), n, dtype=np.uint64) for r in range(rows)])
     ctx.set_key(0, av, bv)
     threads = O.num_threads()
-    sample = levels[:max(1, min(len(levels), threads))]
+    sample = levels   # the whole workload: same pairs, levels and key shape as the GPU arm
     ins = [[np.concatenate([rng.integers(0, int(q), n, dtype=np.uint64) for q in Q[:L]]) for L in sample]
            for _ in range(4)]
     for _ in range(args.warmup):
@@ -428,8 +573,9 @@ def run_reference(args):
         ctx.evalmult_rescale_batch(sample, *ins, nthreads=threads)
     dt = time.perf_counter() - t0
     value = args.steps * len(sample) / dt
-    desc = (f"{len(sample)} pairs (levels {sample}) of the N=2^16 workload per step, OpenMP over pairs "
-            f"on {threads} host threads; the reference's CPU path restated (oracle/)")
+    desc = (f"all {len(sample)} pairs of the N=2^16 workload per step (levels U{{4..12}}, mean "
+            f"{float(np.mean(sample)):.2f}), OpenMP over pairs on {threads} host threads; the reference's CPU "
+            f"path restated (oracle/)")
     line = {"metric": METRIC, "value": value, "unit": "ops/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
@@ -632,6 +778,13 @@ def rotation_batch(G, torch, dev, local, gen, steps):
                   inp=[c[0].data_ptr(), c[1].data_ptr()], out=[o[0].data_ptr(), o[1].data_ptr()])
              for c, o, k in zip(cts, outs, idx)]
     ms_plain, sched_plain = timed(specs)
+    hostw = lambda t: t.reshape(-1).cpu().numpy().view(np.uint64).copy()
+    # outputs of the timed replays for the oracle check in the CPU leg (kept
+    # before the hoisted run reuses the output buffers)
+    check = {"galois": sorted(set(gal)), "plain": [], "hoisted": []}
+    for i in range(2):
+        check["plain"].append((gal[idx[i]], hostw(cts[i][0]), hostw(cts[i][1]), hostw(outs[i][0]),
+                               hostw(outs[i][1])))
     hrng = np.random.default_rng(SEED + 46)
     hcts = cts[:ROT_COUNT // ROT_HOIST]
     hspecs = []
@@ -641,6 +794,8 @@ def rotation_batch(G, torch, dev, local, gen, steps):
             hspecs.append(dict(level=L, mode=G.ROTATE_HOISTED, key_id=gal[k], galois=gal[k],
                                inp=[c[0].data_ptr(), c[1].data_ptr()], out=[o[0].data_ptr(), o[1].data_ptr()]))
     ms_hoist, sched_hoist = timed(hspecs)
+    check["hoisted"] = (hostw(hcts[0][0]), hostw(hcts[0][1]),
+                        [(hspecs[r]["galois"], hostw(outs[r][0]), hostw(outs[r][1])) for r in range(3)])
     boot = bootstrap_steps(G, torch, dev, ctx, cts, outs, L, n)
     del hcts, outs, cts
     ctx.close()
@@ -651,7 +806,7 @@ def rotation_batch(G, torch, dev, local, gen, steps):
             "rotations_per_s": ROT_COUNT / (ms_plain * 1e-3), "ms_per_batch": ms_plain, "schedule": sched_plain,
             "hoisted_rotations_per_s": ROT_COUNT / (ms_hoist * 1e-3), "hoisted_ms_per_batch": ms_hoist,
             "hoisted_schedule": sched_hoist, "resident_bytes": evk_bytes, "bootstrap_steps": boot,
-            "distinct_keys": len(set(gal)), "evk_bytes": len(set(gal)) * 2 * rows * n * 8,
+            "distinct_keys": len(set(gal)), "evk_bytes": len(set(gal)) * 2 * rows * n * 8, "_check": check,
             "note": "rotations by +2^14 and -2^14 share one Galois element at N=2^16 (2^15 slots)"}
 
 
@@ -816,6 +971,9 @@ def run_gpu(args):
     ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     ms_step = ms / args.steps
     value = world * pairs * args.steps / (ms * 1e-3)
+    # the timed step's outputs (outside the timed region), checked against the
+    # oracle in the CPU leg
+    h_out_main = torch.cat([o.reshape(-1) for os_ in outs for o in os_]).cpu().numpy().view(np.uint64)
 
     # per-phase device times (outside the timed region)
     cur = torch.cuda.current_stream().cuda_stream
@@ -841,6 +999,7 @@ def run_gpu(args):
     bi, bo = 8 * sum(in_words), 8 * sum(out_words)
     h_in_buf = torch.cat([x.reshape(-1) for xs in ins for x in xs]).cpu().pin_memory()
     keep = [h_in_buf]
+    h_in_main = h_in_buf.numpy().view(np.uint64)
 
     def e2e_arm():
         d_in = torch.empty(sum(in_words), dtype=torch.int64, device=dev)
@@ -951,10 +1110,18 @@ def run_gpu(args):
     if not args.no_rot:
         rotation = rotation_batch(G, torch, dev, local, gen, max(3, min(args.steps, 10)))
 
-    # CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
-    cpu = None
+    # CPU baseline (rank 0, N=1 only): the oracle on the workload, and as the
+    # checker of the timed outputs
+    rot_check = rotation.pop("_check") if rotation else None
+    serve_check = serving.pop("_check") if serving else None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_port_rate(levels, n, 0)
+        cpu = cpu_port_rate(levels, n, 0, check=(av, bv, h_in_main, h_out_main))
+        parity = {"evalmult_rescale_step": cpu.pop("parity")}
+        if rot_check is not None:
+            parity["rotation_batch"] = cpu_rotation_check(rot_check, n)
+        if serve_check is not None:
+            parity["serving"] = cpu_serving_check(serve_check)
         if not args.no_rot:
             cpu["keys_and_encryption"] = cpu_keys_rate(n)
 
@@ -994,8 +1161,11 @@ def run_gpu(args):
                                               "streams (one pinned host buffer per direction, the batch laid out "
                                               "contiguously; every step copies all inputs in and outputs out)"},
         "plain": plain,
-        "served_vs_plain": (value / world / plain["value"]) if plain else None,
-        "served_vs_plain_16streams": (value / world / plain["streams16"]["value"]) if plain else None,
+        # primary: against the reference's own run shape (its per-chain graphs on 16 streams at once,
+        # bench/bench_evalmult_resident.cpp:36,104-108); then one chain at a time, and this library's
+        # fused one-pair plan
+        "served_vs_plain": (value / world / plain["streams16"]["value"]) if plain else None,
+        "served_vs_plain_one_stream": (value / world / plain["value"]) if plain else None,
         "served_vs_plain_fused": (value / world / plain["fused_single_pair"]["value"]) if plain else None,
         "latency_ms": (dict(serving["served"]["latency_ms"], source="serving trace, served form") if serving
                        else {"p50": ms_step, "p99": ms_step, "source": "whole batch per step"}),
@@ -1006,6 +1176,7 @@ def run_gpu(args):
         "gpu_launches": kernels_per_step * args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "parity": parity,
     }
     print(json.dumps(line), flush=True)
     return 0
