@@ -50,6 +50,30 @@ struct TwD {
     const double* t;
     __device__ __forceinline__ double operator()(u32 i) const { return __ldg(t + i); }
 };
+
+// The 2^L twiddles tw(base + g), g < 2^L, of one butterfly group at local
+// stage L (base = B << L, so the run is aligned to 2^L entries). The
+// library's double tables (TwD, 16-byte aligned per modulus) load them as
+// 16-byte vectors; other tables load word by word.
+template <int L, class TW>
+__device__ __forceinline__ void tw_run(const TW& tw, u32 base, double (&w)[1 << L]) {
+#pragma unroll
+    for (int g = 0; g < (1 << L); ++g) w[g] = tw(base + (u32)g);
+}
+template <int L>
+__device__ __forceinline__ void tw_run(const TwD& tw, u32 base, double (&w)[1 << L]) {
+    if constexpr (L == 0) {
+        w[0] = __ldg(tw.t + base);
+    } else {
+        const double2* p = reinterpret_cast<const double2*>(tw.t + base);
+#pragma unroll
+        for (int h = 0; h < (1 << (L - 1)); ++h) {
+            const double2 v = __ldg(p + h);
+            w[2 * h] = v.x;
+            w[2 * h + 1] = v.y;
+        }
+    }
+}
 struct TwDConv {
     const u64* w;
     __device__ __forceinline__ double operator()(u32 i) const { return u2d(__ldg(w + i)); }
@@ -161,9 +185,11 @@ struct FpArT {
     __device__ __forceinline__ void ct_stage(double (&v)[1 << K], const TW& tw, u32 B) const {
         static_assert(K <= 4, "bounds are proven for rounds of at most four stages");
         constexpr int half = 1 << (K - 1 - L);
+        double wr[1 << L];
+        tw_run<L>(tw, B << L, wr);
 #pragma unroll
         for (int g = 0; g < (1 << L); ++g) {
-            const double w = tw((B << L) + g);
+            const double w = wr[g];
 #pragma unroll
             for (int o = 0; o < half; ++o) {
                 double& x = v[g * 2 * half + o];
@@ -184,9 +210,11 @@ struct FpArT {
         static_assert(K <= 4, "bounds are proven for rounds of at most four stages");
         constexpr int half = 1 << (K - 1 - L);
         constexpr bool EVEN = !SIGNED_TW || (K - 1 - L) >= 3;
+        double wr[1 << L];
+        tw_run<L>(tw, B << L, wr);
 #pragma unroll
         for (int g = 0; g < (1 << L); ++g) {
-            const double w = tw((B << L) + g);
+            const double w = wr[g];
 #pragma unroll
             for (int o = 0; o < half; ++o) {
                 double& x = v[g * 2 * half + o];

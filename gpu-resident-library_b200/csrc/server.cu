@@ -287,8 +287,10 @@ void Server::retire_oldest() {
     InFlight f = std::move(inflight_.front());
     inflight_.pop_front();
     std::vector<double> t(f.ev.size());
+    const auto w0 = std::chrono::steady_clock::now();
+    for (size_t k = 0; k < f.ev.size(); ++k) ck(cudaEventSynchronize(f.ev[k]), "step wait");
+    st_.host_wait_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
     for (size_t k = 0; k < f.ev.size(); ++k) {
-        ck(cudaEventSynchronize(f.ev[k]), "step wait");
         float ms = 0;
         ck(cudaEventElapsedTime(&ms, epoch_ev_, f.ev[k]), "cudaEventElapsedTime");
         t[k] = ms * 1e-3;
@@ -378,6 +380,7 @@ int Server::step() {
     InFlight f;
     int queued = 0;
     const int slot = (int)(step_no_ & 1);
+    const auto b0 = std::chrono::steady_clock::now();
     for (size_t c = 0; c < nctx; ++c) {
         if (ops[c].empty()) continue;
         cudaStream_t s = streams_[c];
@@ -408,6 +411,7 @@ int Server::step() {
         queued += (int)ops[c].size();
         st_.max_batch = std::max<uint64_t>(st_.max_batch, ops[c].size());
     }
+    st_.host_build_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - b0).count();
     if (queued) {
         inflight_.push_back(std::move(f));
         ++step_no_;
@@ -538,6 +542,8 @@ int gpufhe_server_get_stats(gpufhe_server* h, gpufhe_server_stats* out) {
     out->arena_bytes = s.arena_bytes;
     out->resident_bytes = s.resident_bytes;
     out->busy_s = s.busy_s;
+    out->host_build_s = s.host_build_s;
+    out->host_wait_s = s.host_wait_s;
     return GPUFHE_OK;
 }
 

@@ -82,6 +82,8 @@ struct Stats {
     size_t arena_bytes = 0;      // arena capacity
     size_t resident_bytes = 0;   // tables + keys of every context
     double busy_s = 0;           // first admission to last completion
+    double host_build_s = 0;     // host time building and launching steps
+    double host_wait_s = 0;      // host time blocked on a step still running on the GPU
 };
 
 class Server {

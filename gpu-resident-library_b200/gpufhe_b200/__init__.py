@@ -64,6 +64,8 @@ _API: dict = {
     "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
     "gpufhe_ntt_job_bytes": (U64, []),
     "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),
+    "gpufhe_approx_switch_tensor": (I32, [VP, VP, VP, VP, VP, VP, VP, VP, VP, U32, U32, U32, I32, VP]),
+    "gpufhe_approx_switch_status": (I32, [VP]),
     "gpufhe_rns_mult_batch": (I32, [VP, VP, VP, VP, U32, U32, U32, VP]),
     "gpufhe_op_workspace_bytes": (U64, [VP, U32]),
     "gpufhe_plan_create": (I32, [VP, U32, VP, VP, U64, C.POINTER(VP)]),
@@ -340,7 +342,7 @@ class ServerStats(C.Structure):
     """struct gpufhe_server_stats."""
     _fields_ = [("steps", U64), ("ops", U64), ("emr_ops", U64), ("completed", U64), ("peak_active", U64),
                 ("max_batch", U64), ("peak_bytes", U64), ("arena_bytes", U64), ("resident_bytes", U64),
-                ("busy_s", DBL)]
+                ("busy_s", DBL), ("host_build_s", DBL), ("host_wait_s", DBL)]
 
 
 class RequestRecord(C.Structure):
