@@ -317,6 +317,7 @@ Plan::~Plan() {
     }
     if (d_blob) cudaFree(d_blob);
     if (h_blob) cudaFreeHost(h_blob);
+    for (void* h : old_h_blobs) cudaFreeHost(h);
     if (own_ws && ws) cudaFree(ws);
 }
 
@@ -331,14 +332,29 @@ static void commit(Plan& p, const HostTables& T, const std::vector<Op>& ops, cud
     const size_t b_plist = al(T.plist.size() * sizeof(uint32_t));
     const size_t total = std::max<size_t>(b_pairs + b_jobs + b_mac + b_plist, 256);
     if (total > p.blob_cap) {
-        if (p.d_blob) cudaFree(p.d_blob);
-        if (p.h_blob) cudaFreeHost(p.h_blob);
-        p.d_blob = nullptr;
-        p.h_blob = nullptr;
-        p.blob_cap = 0;
-        const size_t cap = total + total / 2;
-        if (cudaMalloc(&p.d_blob, cap) != cudaSuccess) throw std::runtime_error("plan allocation failed");
-        if (cudaMallocHost(&p.h_blob, cap) != cudaSuccess) throw std::runtime_error("plan host allocation failed");
+        // Grow by doubling without stalling the device: an asynchronous rebuild
+        // frees the old device blob in stream order (its last reader is earlier
+        // work on s) and keeps the old pinned mirror until the plan is
+        // destroyed; cudaFree / cudaFreeHost here would wait for every running
+        // kernel, which stalled the serving loop's host whenever its batches
+        // reached a new size.
+        const size_t cap = std::max<size_t>(2 * total, (size_t)1 << 16);
+        void* nd = nullptr;
+        void* nh = nullptr;
+        const cudaError_t ed = async ? cudaMallocAsync(&nd, cap, s) : cudaMalloc(&nd, cap);
+        if (ed != cudaSuccess) throw std::runtime_error("plan allocation failed");
+        if (cudaMallocHost(&nh, cap) != cudaSuccess) {
+            if (async) cudaFreeAsync(nd, s); else cudaFree(nd);
+            throw std::runtime_error("plan host allocation failed");
+        }
+        if (p.d_blob) {
+            if (async) cudaFreeAsync(p.d_blob, s); else cudaFree(p.d_blob);
+        }
+        if (p.h_blob) {
+            if (async) p.old_h_blobs.push_back(p.h_blob); else cudaFreeHost(p.h_blob);
+        }
+        p.d_blob = nd;
+        p.h_blob = nh;
         p.blob_cap = cap;
     }
     char* h = static_cast<char*>(p.h_blob);

@@ -46,6 +46,10 @@ struct Plan {
     void* d_blob = nullptr;            // device tables (pairs, jobs, P5 groups, pair lists)
     void* h_blob = nullptr;            // pinned host mirror of d_blob
     size_t blob_cap = 0;
+    // pinned mirrors outgrown by a rebuild: freeing one (cudaFreeHost) would
+    // synchronize the device under a running step, so they are kept until the
+    // plan is destroyed (at most the sum of a doubling series: < 2x h_blob)
+    std::vector<void*> old_h_blobs;
     std::unique_ptr<HostTables> staging;
     ~Plan();
     Plan(const Plan&) = delete;                  // owns device memory and a hold on ctx
