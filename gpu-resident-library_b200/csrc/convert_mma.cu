@@ -24,6 +24,7 @@
 #include <cstdint>
 #include <string>
 
+#include "convert.hpp"
 #include "devonce.hpp"
 #include "gf.cuh"
 #include "gpufhe_b200.h"
@@ -188,16 +189,20 @@ cudaError_t cv_launch(const u64* src, u64* dst, const u64* qhi, const u64* qhip,
 // swizzle: byte b of row r at (r % 8) * 16 + (r / 8) * 256 + (b / 16) * 128.
 // The 32-bit partial sums land in tensor memory (row r = lane r, column
 // 16 * target + s); every thread then reads its row's sixteen columns per
-// target (tcgen05.ld 32x32b), folds them into four 64-bit words, combines
-// them into 128 bits and reduces, writing 32 consecutive coefficients per warp.
-// Targets go in chunks of at most 16 (256 columns: the CTA's tensor memory),
-// two CTAs per SM. The wait on each MMA batch is bounded (about two seconds of
-// %globaltimer); on expiry the CTA records an error in g_cv_err, waits
-// (bounded) once more, frees its tensor memory and returns.
+// target (tcgen05.ld 32x32b, two targets per wait), folds them into four
+// 64-bit words, combines them into 128 bits and reduces, writing 32
+// consecutive coefficients per warp. Targets go in chunks of at most 8 (128
+// tensor-memory columns per CTA), up to four CTAs per SM, so one CTA's MMA
+// and tile loads overlap the others' reductions; the next tile's inputs are
+// loaded into registers before the current tile's MMA is awaited. The wait on
+// each MMA batch is bounded (about two seconds of %globaltimer); on expiry the
+// CTA records an error in g_cv_err, waits (bounded) once more, frees its
+// tensor memory and returns.
 constexpr int TC_THREADS = 256;
 constexpr int TC_M = 128;
-constexpr int TC_COLS = 256;        // tensor-memory columns per CTA
-constexpr int TC_MIN_SMEM = 80 * 1024;   // keeps at most two CTAs (2 x 256 columns) on an SM
+constexpr int TC_CHUNK = 8;          // targets per MMA batch
+constexpr int TC_COLS = 128;         // tensor-memory columns per CTA (16 per target)
+constexpr int TC_MIN_SMEM = 46 * 1024;   // at most four CTAs (4 x 128 columns) on an SM
 
 __device__ u32 g_cv_err;
 
@@ -238,21 +243,31 @@ __device__ __forceinline__ void tc_ld16(u32 taddr, uint32_t (&r)[16]) {
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tc_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // One 16-byte unit of A or B for the canonical layout: row r, K-half h, at
 // base + (r % 8) * 16 + (r / 8) * 256 + h * 128.
 __device__ __forceinline__ u32 canon_off(int r, int h) { return (u32)((r & 7) * 16 + (r >> 3) * 256 + h * 128); }
 
+// The sixteen partial sums of one output (fifteen shifts) -> the exact sum -> mod p_j.
+__device__ __forceinline__ u64 tc_reduce(const uint32_t (&cs)[16], const ModC& m) {
+    u64 acc4[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int sft = 0; sft < 15; ++sft) acc4[sft >> 2] += (u64)cs[sft] << (8 * (sft & 3));
+    u64 lo = acc4[0], hi = acc4[2] + (acc4[3] << 32);
+    add_wide(lo, hi, acc4[1] << 32, acc4[1] >> 32);
+    return barrett(lo, hi, m);
+}
+
 template <int KS>
-__global__ void __launch_bounds__(TC_THREADS, 2)
+__global__ void __launch_bounds__(TC_THREADS, 4)
 k_approx_switch_tc(const u64* __restrict__ src, u64* __restrict__ dst, const u64* __restrict__ qhi,
                    const u64* __restrict__ qhip, const u64* __restrict__ qm, const u64* __restrict__ qmp,
                    const u64* __restrict__ p, const u64* __restrict__ mulo, const u64* __restrict__ muhi,
                    uint32_t sizeQ, uint32_t sizeP, uint32_t n) {
     extern __shared__ __align__(1024) unsigned char tc_sm[];
-    const int chunks = (int)(sizeP + 15) / 16;
+    const int chunks = (int)(sizeP + TC_CHUNK - 1) / TC_CHUNK;
     unsigned char* A = tc_sm;                                   // [KS][4096]
     unsigned char* B = tc_sm + KS * 4096;                       // [chunk][KS][Nc * 32]
     const u32 b_bytes = (u32)KS * 32u * 16u * sizeP;            // sum over chunks of KS * Nc * 32
@@ -265,11 +280,11 @@ k_approx_switch_tc(const u64* __restrict__ src, u64* __restrict__ dst, const u64
     {
         u32 off = 0;
         for (int c = 0; c < chunks; ++c) {
-            const int tc = min(16, (int)sizeP - 16 * c);
+            const int tc = min(TC_CHUNK, (int)sizeP - TC_CHUNK * c);
             const int nc = 16 * tc;
             for (int e = tid; e < KS * nc * 2; e += TC_THREADS) {
                 const int h = e & 1, nr = (e >> 1) % nc, ks = (e >> 1) / nc;
-                const int jl = nr >> 4, s = nr & 15, j = 16 * c + jl;
+                const int jl = nr >> 4, s = nr & 15, j = TC_CHUNK * c + jl;
                 u64 w[2] = {0, 0};
 #pragma unroll
                 for (int d = 0; d < 2; ++d) {
@@ -305,26 +320,42 @@ k_approx_switch_tc(const u64* __restrict__ src, u64* __restrict__ dst, const u64
     u32 phase = 0;
     bool ok = true;
 
-    const int row = tid & (TC_M - 1);          // A staging: row, and pairs of towers from tid / 128
+    // A staging: thread -> row (tid % 128) and tower pairs pr = tid / 128, +2, ...; the raw
+    // residues of the next tile are loaded one tile ahead
+    const int row = tid & (TC_M - 1);
+    const int pr0 = tid >> 7;
     const uint32_t tiles = n / TC_M;
+    u64 raw[KS][2];
+    auto load_raw = [&](uint32_t tile) {
+#pragma unroll
+        for (int q = 0; q < KS; ++q)
+#pragma unroll
+            for (int d = 0; d < 2; ++d) {
+                const int i = 2 * (pr0 + 2 * q) + d;
+                raw[q][d] = (i < (int)sizeQ && tile < tiles) ? src[(size_t)i * n + (size_t)tile * TC_M + row] : 0;
+            }
+    };
+    load_raw(blockIdx.x);
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t n0 = tile * TC_M;
         // A: x_i = shoup(a_i, QHatInv_i) as bytes; pair pr = towers (2 pr, 2 pr + 1)
 #pragma unroll
-        for (int pr = tid >> 7; pr < 2 * KS; pr += 2) {
+        for (int q = 0; q < KS; ++q) {
+            const int pr = pr0 + 2 * q;
             u64 x[2];
 #pragma unroll
             for (int d = 0; d < 2; ++d) {
                 const int i = 2 * pr + d;
-                x[d] = i < (int)sizeQ ? shoup(src[(size_t)i * n + n0 + row], qhi[i], qhip[i], qm[i]) : 0;
+                x[d] = i < (int)sizeQ ? shoup(raw[q][d], qhi[i], qhip[i], qm[i]) : 0;
             }
             *reinterpret_cast<uint4*>(A + (pr >> 1) * 4096 + canon_off(row, pr & 1)) =
                 make_uint4((u32)x[0], (u32)(x[0] >> 32), (u32)x[1], (u32)(x[1] >> 32));
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        load_raw(tile + gridDim.x);
         u32 boff = 0;
         for (int c = 0; c < chunks && ok; ++c) {
-            const int tc = min(16, (int)sizeP - 16 * c);
+            const int tc = min(TC_CHUNK, (int)sizeP - TC_CHUNK * c);
             const int nc = 16 * tc;
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();   // A written (first chunk), previous chunk's tensor-memory reads done
@@ -353,21 +384,25 @@ k_approx_switch_tc(const u64* __restrict__ src, u64* __restrict__ dst, const u64
             }
             phase ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // epilogue: warp quadrant q reads rows 32q..32q+31; warps q and q+4 split the targets
+            // epilogue: warp quadrant q reads rows 32q..32q+31; warps q and q+4 split the
+            // chunk's targets (jl = half, half + 2, ...), two per tensor-memory wait
             const int q = warp & 3;
             const u32 r_out = (u32)(32 * q + lane);
-            for (int jl = warp >> 2; jl < tc; jl += 2) {
-                uint32_t cs[16];
-                tc_ld16(tmem + ((u32)(32 * q) << 16) + (u32)(16 * jl), cs);
-                u64 acc4[4] = {0, 0, 0, 0};
-#pragma unroll
-                for (int sft = 0; sft < 15; ++sft) acc4[sft >> 2] += (u64)cs[sft] << (8 * (sft & 3));
-                u64 lo = acc4[0], hi = acc4[2] + (acc4[3] << 32);
-                add_wide(lo, hi, acc4[1] << 32, acc4[1] >> 32);
-                const int j = 16 * c + jl;
+            const u32 tq = tmem + ((u32)(32 * q) << 16);
+            for (int jl = warp >> 2; jl < tc; jl += 4) {
+                uint32_t c0[16], c1[16];
+                const bool two = jl + 2 < tc;
+                tc_ld16(tq + (u32)(16 * jl), c0);
+                if (two) tc_ld16(tq + (u32)(16 * (jl + 2)), c1);
+                tc_ld_wait();
+                const int j = TC_CHUNK * c + jl;
                 ModC m;
                 m.q = p[j]; m.two_q = 2 * m.q; m.mu_lo = mulo[j]; m.mu_hi = muhi[j];
-                dst[(size_t)j * n + n0 + r_out] = barrett(lo, hi, m);
+                dst[(size_t)j * n + n0 + r_out] = tc_reduce(c0, m);
+                if (two) {
+                    m.q = p[j + 2]; m.two_q = 2 * m.q; m.mu_lo = mulo[j + 2]; m.mu_hi = muhi[j + 2];
+                    dst[(size_t)(j + 2) * n + n0 + r_out] = tc_reduce(c1, m);
+                }
             }
             boff += (u32)KS * nc * 32;
         }
@@ -401,7 +436,8 @@ cudaError_t tc_launch(const u64* src, u64* dst, const u64* qhi, const u64* qhip,
                              (int)tc_smem<KS>(CV_MAX_P));
     });
     const uint32_t tiles = n / TC_M;
-    const unsigned grid = (unsigned)std::min<uint32_t>(tiles, 2u * (uint32_t)gfx::current_sm_count());
+    const uint32_t per_sm = (uint32_t)std::max<size_t>(1, std::min<size_t>(4, (227u * 1024u) / tc_smem<KS>(sizeP)));
+    const unsigned grid = (unsigned)std::min<uint32_t>(tiles, per_sm * (uint32_t)gfx::current_sm_count());
     k_approx_switch_tc<KS><<<grid, TC_THREADS, tc_smem<KS>(sizeP), s>>>(src, dst, qhi, qhip, qm, qmp, p, mulo, muhi,
                                                                         sizeQ, sizeP, n);
     return cudaGetLastError();
@@ -409,32 +445,51 @@ cudaError_t tc_launch(const u64* src, u64* dst, const u64* qhi, const u64* qhip,
 
 }  // namespace
 
-extern "C" int gpufhe_approx_switch_tensor(const uint64_t* d_src, uint64_t* d_dst, const uint64_t* d_QHatInvModq,
-                                           const uint64_t* d_QHatInvModqPrecon, const uint64_t* d_q,
-                                           const uint64_t* d_QHatModp, const uint64_t* d_p, const uint64_t* d_mu_lo,
-                                           const uint64_t* d_mu_hi, uint32_t sizeQ, uint32_t sizeP, uint32_t n, int form,
-                                           cudaStream_t s) {
+namespace cv {
+
+bool tcgen05_shape(uint32_t sizeQ, uint32_t sizeP, uint32_t n) {
+    return sizeQ >= 1 && sizeQ <= CV_MAX_Q && sizeP >= 1 && sizeP <= CV_MAX_P && n && n % TC_M == 0;
+}
+
+cudaError_t approx_switch_tcgen05(const uint64_t* d_src, uint64_t* d_dst, const uint64_t* qhi, const uint64_t* qhip,
+                                  const uint64_t* q, const uint64_t* qmp, const uint64_t* p, const uint64_t* mulo,
+                                  const uint64_t* muhi, uint32_t sizeQ, uint32_t sizeP, uint32_t n, cudaStream_t s) {
+    const int ks = (int)(sizeQ + 3) / 4;
+    return ks == 1 ? tc_launch<1>(d_src, d_dst, qhi, qhip, q, qmp, p, mulo, muhi, sizeQ, sizeP, n, s)
+         : ks == 2 ? tc_launch<2>(d_src, d_dst, qhi, qhip, q, qmp, p, mulo, muhi, sizeQ, sizeP, n, s)
+                   : tc_launch<3>(d_src, d_dst, qhi, qhip, q, qmp, p, mulo, muhi, sizeQ, sizeP, n, s);
+}
+
+}  // namespace cv
+
+extern "C" int gpufhe_approx_switch(const uint64_t* d_src, uint64_t* d_dst, const uint64_t* d_QHatInvModq,
+                                    const uint64_t* d_QHatInvModqPrecon, const uint64_t* d_q, const uint64_t* d_QHatModp,
+                                    const uint64_t* d_p, const uint64_t* d_mu_lo, const uint64_t* d_mu_hi,
+                                    uint32_t sizeQ, uint32_t sizeP, uint32_t n, int form, cudaStream_t s) {
     if (!d_src || !d_dst || !d_QHatInvModq || !d_QHatInvModqPrecon || !d_q || !d_QHatModp || !d_p || !d_mu_lo ||
         !d_mu_hi) {
-        gfx::set_error("gpufhe_approx_switch_tensor: null argument");
+        gfx::set_error("gpufhe_approx_switch: null argument");
         return GPUFHE_EINVAL;
     }
-    const uint32_t align = form == GPUFHE_CONVERT_TCGEN05 ? (uint32_t)TC_M : 16u;
-    if (sizeQ == 0 || sizeQ > CV_MAX_Q || sizeP == 0 || sizeP > CV_MAX_P || n == 0 || n % align ||
-        (form != GPUFHE_CONVERT_TCGEN05 && form != GPUFHE_CONVERT_MMA_SYNC)) {
-        gfx::set_error("gpufhe_approx_switch_tensor: needs 1 <= sizeQ <= 12, 1 <= sizeP <= 64, n a multiple of "
-                       "128 (tcgen05 form) or 16 (mma.sync form), and a known form");
+    const bool shape_ok = form == GPUFHE_CONVERT_TCGEN05   ? cv::tcgen05_shape(sizeQ, sizeP, n)
+                        : form == GPUFHE_CONVERT_MMA_SYNC ? (sizeQ >= 1 && sizeQ <= CV_MAX_Q && sizeP >= 1 &&
+                                                             sizeP <= CV_MAX_P && n && n % 16 == 0)
+                        : form == GPUFHE_CONVERT_INTEGER  ? (sizeQ >= 1 && sizeP >= 1 && n)
+                                                          : false;
+    if (!shape_ok) {
+        gfx::set_error("gpufhe_approx_switch: unknown form, or a shape it does not take (tcgen05: sizeQ <= 12, "
+                       "sizeP <= 64, n a multiple of 128; mma.sync: the same with n a multiple of 16)");
         return GPUFHE_EINVAL;
     }
-    const int ks = (int)(sizeQ + 3) / 4;
     cudaError_t e;
     if (form == GPUFHE_CONVERT_TCGEN05) {
-        auto go = [&](auto launch) {
-            return launch(d_src, d_dst, d_QHatInvModq, d_QHatInvModqPrecon, d_q, d_QHatModp, d_p, d_mu_lo, d_mu_hi,
-                          sizeQ, sizeP, n, s);
-        };
-        e = ks == 1 ? go(tc_launch<1>) : ks == 2 ? go(tc_launch<2>) : go(tc_launch<3>);
+        e = cv::approx_switch_tcgen05(d_src, d_dst, d_QHatInvModq, d_QHatInvModqPrecon, d_q, d_QHatModp, d_p, d_mu_lo,
+                                      d_mu_hi, sizeQ, sizeP, n, s);
+    } else if (form == GPUFHE_CONVERT_INTEGER) {
+        e = cv::approx_switch_integer(d_src, d_dst, d_QHatInvModq, d_QHatInvModqPrecon, d_q, d_QHatModp, d_p, d_mu_lo,
+                                      d_mu_hi, sizeQ, sizeP, n, s);
     } else {
+        const int ks = (int)(sizeQ + 3) / 4;
         auto go = [&](auto launch) {
             return launch(d_src, d_dst, d_QHatInvModq, d_QHatInvModqPrecon, d_q, d_QHatModp, d_p, d_mu_lo, d_mu_hi,
                           sizeQ, sizeP, n, s);
@@ -442,7 +497,7 @@ extern "C" int gpufhe_approx_switch_tensor(const uint64_t* d_src, uint64_t* d_ds
         e = ks == 1 ? go(cv_launch<1>) : ks == 2 ? go(cv_launch<2>) : go(cv_launch<3>);
     }
     if (e != cudaSuccess) {
-        gfx::set_error(std::string("gpufhe_approx_switch_tensor: ") + cudaGetErrorString(e));
+        gfx::set_error(std::string("gpufhe_approx_switch: ") + cudaGetErrorString(e));
         return GPUFHE_ECUDA;
     }
     return GPUFHE_OK;

@@ -64,7 +64,7 @@ _API: dict = {
     "gpufhe_ntt_batch": (I32, [VP, VP, U32, U32, U32, I32, VP, VP]),
     "gpufhe_ntt_job_bytes": (U64, []),
     "gpufhe_ntt_run_jobs": (I32, [VP, VP, U32, I32, VP]),
-    "gpufhe_approx_switch_tensor": (I32, [VP, VP, VP, VP, VP, VP, VP, VP, VP, U32, U32, U32, I32, VP]),
+    "gpufhe_approx_switch": (I32, [VP, VP, VP, VP, VP, VP, VP, VP, VP, U32, U32, U32, I32, VP]),
     "gpufhe_approx_switch_status": (I32, [VP]),
     "gpufhe_rns_mult_batch": (I32, [VP, VP, VP, VP, U32, U32, U32, VP]),
     "gpufhe_op_workspace_bytes": (U64, [VP, U32]),

@@ -233,22 +233,26 @@ int gpufhe_ntt_run_jobs(gpufhe_ctx* ctx, const uint64_t* d_jobs, uint32_t njobs,
  * launch. Buffers 16-byte aligned, n >= 2048; out may alias a or b. */
 int gpufhe_rns_mult_batch(gpufhe_ctx* ctx, const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_out,
                           uint32_t npolys, uint32_t towers, uint32_t first_tower, cudaStream_t stream);
-/* ApproxSwitchCRTBasis on the integer tensor cores: the arguments and the
- * result of LaunchApproxSwitchCRTBasis (reference kernels/basis_convert.cu:
- * 14-114), bit for bit. Every x_i and QHatModp[i][j] is split into bytes; the
- * fifteen byte-shift classes of the exact sum are unsigned 8-bit matrix
- * products with 32-bit sums (tcgen05.mma kind::i8 with the sums in tensor
- * memory, or the warp-level mma.sync m16n8k32), recombined into the exact
- * 128-bit sum before the same Barrett reduction. 1 <= sizeQ <= 12,
- * 1 <= sizeP <= 64; n (which may span several polynomials: the conversion is
- * per coefficient) a multiple of 128 for GPUFHE_CONVERT_TCGEN05, of 16 for
- * GPUFHE_CONVERT_MMA_SYNC. No counterpart in the reference. */
+/* ApproxSwitchCRTBasis in a chosen form: the arguments and the result of
+ * LaunchApproxSwitchCRTBasis (reference kernels/basis_convert.cu:14-114), bit
+ * for bit. The tensor-core forms split every x_i and QHatModp[i][j] into
+ * bytes; the fifteen byte-shift classes of the exact sum are unsigned 8-bit
+ * matrix products with 32-bit sums (tcgen05.mma kind::i8 with the sums in
+ * tensor memory, or the warp-level mma.sync m16n8k32), recombined into the
+ * exact 128-bit sum before the same Barrett reduction. The integer form is
+ * 128-bit multiply-adds on the integer pipes. LaunchApproxSwitchCRTBasis
+ * itself takes the tcgen05 form wherever its shape allows (sizeQ <= 12,
+ * sizeP <= 64, n a multiple of 128; n may span several polynomials, the
+ * conversion is per coefficient), else the integer form. The mma.sync form
+ * takes the same limits with n a multiple of 16. No counterpart in the
+ * reference. */
 #define GPUFHE_CONVERT_TCGEN05 0
 #define GPUFHE_CONVERT_MMA_SYNC 1
-int gpufhe_approx_switch_tensor(const uint64_t* d_src, uint64_t* d_dst, const uint64_t* d_QHatInvModq,
-                                const uint64_t* d_QHatInvModqPrecon, const uint64_t* d_q, const uint64_t* d_QHatModp,
-                                const uint64_t* d_p, const uint64_t* d_mu_lo, const uint64_t* d_mu_hi, uint32_t sizeQ,
-                                uint32_t sizeP, uint32_t n, int form, cudaStream_t stream);
+#define GPUFHE_CONVERT_INTEGER 2
+int gpufhe_approx_switch(const uint64_t* d_src, uint64_t* d_dst, const uint64_t* d_QHatInvModq,
+                         const uint64_t* d_QHatInvModqPrecon, const uint64_t* d_q, const uint64_t* d_QHatModp,
+                         const uint64_t* d_p, const uint64_t* d_mu_lo, const uint64_t* d_mu_hi, uint32_t sizeQ,
+                         uint32_t sizeP, uint32_t n, int form, cudaStream_t stream);
 /* Synchronizes the device and returns (then clears) the tensor-core
  * conversion's status word: 0, or 1 when a tcgen05 batch did not complete
  * within its bounded wait (its outputs are then not valid). */

@@ -1,7 +1,8 @@
-"""ApproxSwitchCRTBasis on the integer tensor cores (gpufhe_approx_switch_tensor:
+"""ApproxSwitchCRTBasis on the integer tensor cores (gpufhe_approx_switch:
 tcgen05.mma kind::i8 with tensor-memory sums, and the warp-level mma.sync
-form) against the integer-pipe form (LaunchApproxSwitchCRTBasis, the
-reference ABI kernel) and the oracle's restatement of
+form) against the integer-pipe form (form 2), the reference ABI entry
+LaunchApproxSwitchCRTBasis (which takes the tcgen05 form where it can) and
+the oracle's restatement of
 kernels/basis_convert.cu:14-114, bit for bit, at the widths the workloads use
 (ModUp alpha = 3 into 12 targets, alpha = 8 into 24, ModDown K = 8 into 24)
 and at ragged and maximal ones; two calls in a row; the bounded-wait status
@@ -42,10 +43,15 @@ def test_tensor_conversion_bit_exact(form, sizeQ, sizeP, bitsQ, bitsP):
     qhi, qhip, qmp, mulo, muhi = constants(Qm, Pm)
     bufs = [dev(x) for x in (src, qhi, qhip, Qm, qmp, Pm, mulo, muhi)]
     d_int, d_mma = empty(sizeP * n), empty(sizeP * n)
-    G.lib().LaunchApproxSwitchCRTBasis(ptr(bufs[0]), ptr(d_int), *[ptr(x) for x in bufs[1:]], sizeQ, sizeP, n, None)
+    G.check(G.lib().gpufhe_approx_switch(ptr(bufs[0]), ptr(d_int), *[ptr(x) for x in bufs[1:]], sizeQ, sizeP, n,
+                                         2, None))   # the integer form
+    d_abi = empty(sizeP * n)   # the reference ABI entry (tcgen05 where the shape allows)
+    G.lib().LaunchApproxSwitchCRTBasis(ptr(bufs[0]), ptr(d_abi), *[ptr(x) for x in bufs[1:]], sizeQ, sizeP, n, None)
+    sync()
+    assert np.array_equal(host(d_abi), host(d_int))
     for rep in range(2):   # the second call reuses nothing from the first
         d_mma.fill_(-1)
-        G.check(G.lib().gpufhe_approx_switch_tensor(ptr(bufs[0]), ptr(d_mma), *[ptr(x) for x in bufs[1:]], sizeQ,
+        G.check(G.lib().gpufhe_approx_switch(ptr(bufs[0]), ptr(d_mma), *[ptr(x) for x in bufs[1:]], sizeQ,
                                                     sizeP, n, form, None))
         sync()
         st = np.zeros(1, np.uint32)
@@ -61,9 +67,9 @@ def test_tensor_conversion_rejects_unsupported():
     import gpufhe_b200 as G
     x = empty(64)
     p = ptr(x)
-    f = G.lib().gpufhe_approx_switch_tensor
+    f = G.lib().gpufhe_approx_switch
     assert f(p, p, p, p, p, p, p, p, p, 13, 4, 128, 0, None) == -1    # sizeQ > 12
     assert f(p, p, p, p, p, p, p, p, p, 4, 65, 128, 0, None) == -1    # sizeP > 64
     assert f(p, p, p, p, p, p, p, p, p, 4, 4, 64, 0, None) == -1      # tcgen05 form needs n % 128 == 0
     assert f(p, p, p, p, p, p, p, p, p, 4, 4, 24, 1, None) == -1      # mma.sync form needs n % 16 == 0
-    assert f(p, p, p, p, p, p, p, p, p, 4, 4, 128, 2, None) == -1     # unknown form
+    assert f(p, p, p, p, p, p, p, p, p, 4, 4, 128, 3, None) == -1     # unknown form
