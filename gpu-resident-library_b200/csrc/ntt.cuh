@@ -177,6 +177,9 @@ struct FpArT {
     __device__ __forceinline__ double unbits(u64 b) const { return __longlong_as_double((long long)b); }
     __device__ __forceinline__ u64 stage_in(u64 x) const { return bits(in(x)); }
     __device__ __forceinline__ u64 final_out(u64 b) const { return out(unbits(b)); }
+    // final words already canonical: no lazy-range correction needed
+    __device__ __forceinline__ u64 final_canon(u64 b) const { return out(unbits(b)); }
+    __device__ __forceinline__ u64 final_2q(u64 b) const { return out(unbits(b)); }
     // pass-to-pass intermediates stay in the policy's own representation
     __device__ __forceinline__ double from_raw(u64 b) const { return unbits(b); }
     __device__ __forceinline__ u64 to_raw(double z) const { return bits(z); }
@@ -250,6 +253,9 @@ struct IntAr {
     __device__ __forceinline__ u64 unbits(u64 b) const { return b; }
     __device__ __forceinline__ u64 stage_in(u64 x) const { return x; }
     __device__ __forceinline__ u64 final_out(u64 b) const { return b; }
+    // lazy [0, 4q) -> canonical [0, q), or -> [0, 2q)
+    __device__ __forceinline__ u64 final_canon(u64 b) const { return csub(csub(b, two_q), q); }
+    __device__ __forceinline__ u64 final_2q(u64 b) const { return csub(b, two_q); }
     __device__ __forceinline__ u64 from_raw(u64 b) const { return b; }
     __device__ __forceinline__ u64 to_raw(u64 v) const { return v; }
     template <int K, class TW>

@@ -455,7 +455,7 @@ __device__ __forceinline__ void p4_modup_fwd_row_body(const DevCtx& D, const Pai
     const auto ar = ar_of<FP>(m);
     ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0, true>(sm, twf_of<FP>(D, qp, LOGN), R0, ar, ld);
     ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
-        Y[rl * 256 + c] = csub(ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)]), m.two_q);
+        Y[rl * 256 + c] = ar.final_2q(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)]);
     });
 }
 
@@ -1326,7 +1326,7 @@ __device__ __forceinline__ void p9_final_fwd_row_body(const DevCtx& D, const Pai
         [&](int rl, int cc) { return addend[rl * 256 + cc]; },
         [&](int rl, int cc, u64 a) {
             const int e = rl * 256 + cc;
-            const u64 v = csub(csub(ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)]), m.two_q), m.q);
+            const u64 v = ar.final_canon(sm[rl * G::ROW_STRIDE + ntt::rowpad(cc)]);
             u64 r;
             if (mode == RESCALE) {
                 r = csub(shoup(a, s1, s1p, m.q) + v, m.q);

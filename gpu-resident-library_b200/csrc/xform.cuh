@@ -75,14 +75,12 @@ k_fwd_row(const Job* __restrict__ arr, const Job one) {
     const int job = blockIdx.x / G::ROW_TILES;
     const u32 R0 = (blockIdx.x % G::ROW_TILES) * G::RB;
     const Job j = get_job<SINGLE>(arr, one, job);
-    const u64 q = j.q, two_q = 2 * q;
     u64* x = j.x + (size_t)R0 * 256;
     auto ld = [&](int rl, int c) { return x[rl * 256 + c]; };
     with_path(j, [&](const auto& ar, const auto& tw) {
         ntt::fwd_row_rounds<G::A, G::RB, G::ROW_THREADS, 4, 0, true>(sm, tw, R0, ar, ld);
         ntt::row_tile_walk<G::RB, G::ROW_THREADS>([&](int rl, int c) {
-            const u64 v = ar.final_out(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)]);
-            x[rl * 256 + c] = csub(csub(v, two_q), q);
+            x[rl * 256 + c] = ar.final_canon(sm[rl * G::ROW_STRIDE + ntt::rowpad(c)]);
         });
     });
 }
