@@ -78,7 +78,7 @@ uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan) {
     if (!plan) return 0;
     const pl::Plan& p = *plan->p;
     return (uint32_t)p.p5_form | ((p.mix & 0x1ffu) == 0x1ffu ? 4u : 0u) | ((uint32_t)p.p3_form << 3) |
-           (p.tuned ? 32u : 0u) | ((p.mix & 0x1ffu) << 8);
+           (p.tuned ? 32u : 0u) | (p.p5_fp ? 64u : 0u) | ((p.mix & 0x1ffu) << 8);
 }
 
 int gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule) {
@@ -93,6 +93,7 @@ int gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule) {
     p.mix = (schedule & 4) ? 0x1ffu : (schedule >> 8) & 0x1ffu;
     p.p3_form = (int)((schedule >> 3) & 3);
     if (p.p3_form > 2) { gfx::set_error("bad P3 form"); return GPUFHE_EINVAL; }
+    p.p5_fp = (schedule >> 6) & 1;
     p.tuned = true;
     return GPUFHE_OK;
 }
@@ -103,6 +104,11 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan) {
     const pl::Plan& p = *plan->p;
     for (int i = 0; i <= pl::NPHASE; ++i) {
         const int bit = i == pl::NPHASE ? 6 : i;   // the second P7 launch follows phase 7's choice
+        if (i == 4) {   // P5: the integer form, and the FP64 form for 50-bit Q rows when chosen
+            const uint32_t nfp = p.p5_fp ? p.job_cnt[4][1] : 0u;
+            k += (p.job_cnt[4][0] + p.job_cnt[4][1] - nfp ? 1 : 0) + (nfp ? 1 : 0);
+            continue;
+        }
         if ((p.mix >> bit & 1) && p.job_cnt[i][2]) k += 1;
         else k += (p.job_cnt[i][0] ? 1 : 0) + (p.job_cnt[i][1] ? 1 : 0);
     }

@@ -80,6 +80,7 @@ struct Launcher {
         cudaFuncSetAttribute(p5_mac<LOGN, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
         cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_ASYNC_SMEM_MAX);
         cudaFuncSetAttribute(p5_mac_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
+        cudaFuncSetAttribute(p5_mac_fp<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
     }
     // persistent warp-specialised P3 over job segment PATH: form 1 = 128
     // conversion threads, two CTAs per SM; form 2 = 256, one CTA per SM
@@ -115,10 +116,17 @@ struct Launcher {
         for (int k = 0; k < NPHASE; ++k) {
             if (!(mask >> k & 1)) continue;
             if (k == 4) {
-                if (!p.job_cnt[4][0]) continue;
-                const unsigned grid = p.job_cnt[4][0] * MAC_TILES;
+                // key rows: [integer rows | 50-bit Q rows]; the second segment goes to
+                // the FP64 kernel when p5_fp, else both to the integer form
+                const uint32_t nfp = p.p5_fp ? p.job_cnt[4][1] : 0u;
+                const uint32_t nint = p.job_cnt[4][0] + p.job_cnt[4][1] - nfp;
+                if (nfp)
+                    p5_mac_fp<LOGN><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), s>>>(
+                        D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
+                if (!nint) continue;
+                const unsigned grid = nint * MAC_TILES;
                 if (p.p5_form == P5_TMA && mac_tma_ok(D.dnum))
-                    p5_mac_tma<LOGN><<<p.job_cnt[4][0] * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum), s>>>(
+                    p5_mac_tma<LOGN><<<nint * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum), s>>>(
                         D, p.d_pairs, p.d_mac_jobs, p.d_plist);
                 else if (p.p5_form == P5_ASYNC && mac_async_ok(D.dnum))
                     p5_mac_async<LOGN><<<grid, MACA_NT, maca_smem((int)D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
@@ -255,14 +263,22 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
     }
     T.mac_jobs.clear();
     T.plist.clear();
+    // P5 jobs in two segments: key rows the integer forms must take (P rows,
+    // Q rows with q >= 2^50), then Q rows with q < 2^50, which the FP64 form
+    // may take instead
+    std::vector<uint4> mac_fp;
     for (auto& kv : rows) {
         const auto& v = kv.second;
+        const uint32_t r = kv.first.second;
+        const bool fp = r < c.fullQ() && fp_tower(c.Q()[r]);
         for (size_t g = 0; g < v.size(); g += MAC_GROUP) {
             const uint32_t cnt = (uint32_t)std::min<size_t>(MAC_GROUP, v.size() - g);
-            T.mac_jobs.push_back({kv.first.second, (uint32_t)T.plist.size(), cnt, 0});
+            (fp ? mac_fp : T.mac_jobs).push_back({r, (uint32_t)T.plist.size(), cnt, 0});
             T.plist.insert(T.plist.end(), v.begin() + g, v.begin() + g + cnt);
         }
     }
+    const uint32_t n_int_rows = (uint32_t)T.mac_jobs.size();
+    T.mac_jobs.insert(T.mac_jobs.end(), mac_fp.begin(), mac_fp.end());
     // Route the transform jobs of each NTT phase to the integer or the FP64
     // kernel by the modulus of the tower they transform (P7 stays integer:
     // one CTA there mixes P towers and tower L-1).
@@ -304,8 +320,10 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
         }
         T.job_cnt[k][2] = (uint32_t)(T.jobs.size() - T.job_off[k][2]);
     }
-    T.job_cnt[4][0] = (uint32_t)T.mac_jobs.size();
-    T.job_cnt[4][1] = T.job_cnt[4][2] = 0;
+    T.job_cnt[4][0] = n_int_rows;
+    T.job_off[4][1] = n_int_rows;                         // offset of the FP64 segment in mac_jobs
+    T.job_cnt[4][1] = (uint32_t)T.mac_jobs.size() - n_int_rows;
+    T.job_cnt[4][2] = 0;
 }
 
 Plan::Plan() : staging(std::make_unique<HostTables>()) {}
@@ -494,10 +512,12 @@ uint64_t tune_key(const Plan& p) {
     return ((uint64_t)p.logn << 40) | ((uint64_t)p.dc.dnum << 32) | cls;
 }
 // choice: bits 0-1 = P5 form, bits 3-4 = P3 form (0 plain, 1 and 2
-// warp-specialised), bits 8-16 = phases launched over their interleaved
-// integer / FP64 job list (else as two launches)
+// warp-specialised), bit 6 = P5 key rows of 50-bit Q towers on the FP64
+// pipe, bits 8-16 = phases launched over their interleaved integer / FP64
+// job list (else as two launches)
 void apply_choice(Plan& p, int choice) {
     p.p5_form = choice & 3;
+    p.p5_fp = (choice >> 6) & 1;
     if (p.p5_form == P5_ASYNC && !mac_async_ok(p.dc.dnum)) p.p5_form = P5_REG128;
     if (p.p5_form == P5_TMA && !mac_tma_ok(p.dc.dnum)) p.p5_form = P5_REG128;
     p.mix = ((unsigned)choice >> 8) & 0x1ffu;
@@ -516,7 +536,8 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         p.tuned = true;
         return;
     }
-    constexpr int DEFAULT = P5_REG128 | (0x1ff << 8);   // 4-word register P5, plain P3, interleaved paths
+    // 4-word register P5 with FP64 Q rows, plain P3, interleaved paths
+    constexpr int DEFAULT = P5_REG128 | 64 | (0x1ff << 8);
     apply_choice(p, DEFAULT);
     if (!measure) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -562,6 +583,7 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         cur = pick(1u << k, bit, {bit, 0}, cur);
     }
     cur = pick(1u << 2, 24, {0, 8, 16}, cur);                      // P3 form
+    if (p.job_cnt[4][1]) cur = pick(1u << 4, 64, {64, 0}, cur);     // P5 FP64 rows or integer rows
     std::vector<int> p5v = {P5_REG128, P5_REG256};
     if (mac_async_ok(p.dc.dnum)) p5v.push_back(P5_ASYNC);
     if (mac_tma_ok(p.dc.dnum)) p5v.push_back(P5_TMA);

@@ -665,6 +665,204 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
     }
 }
 
+// P5 on the FP64 pipe, for the key rows of Q towers with q < 2^50 (the
+// integer forms above take P rows and 60-bit Q rows). The integer forms keep
+// the FP64 pipe idle and are bound by integer issue; here every product
+// digit * key is an exact FP64 modular product (FpArS::mulq: h, l by
+// multiply and FMA, quotient by the magic-constant rounding, remainder by
+// FMA) and the inner product is a plain FP64 sum of those remainders.
+// Canonical quantities throughout, no Montgomery scale:
+//   key tile: key_p * P^-1 mod q for every digit (the own digit's stored key
+//     carries an extra R = 2^64 with DevCtx mont: one redc removes it on
+//     load), as signed doubles in (-q/2, q/2];
+//   own source: EvalMult a1 * b1, keyswitch input, rotation sigma_k(c1);
+//   res' = sum_p src_p * key'_p = res * P^-1 (mod q);
+//   EvalMult: W = (t + res') * s1 with t0 = a0 b0, t1 = a0 b1 + a1 b0; the
+//     dropped tower gets (t + res') times R^-1 (one redc) with mont, the
+//     scale the integer form writes for P7; keyswitch / rotation: W = res'.
+// Bounds (q < 2^50, digits and inputs in [0, 2q), keys and s1 signed):
+// every product |r| <= 0.75 q, the accumulator is normalised every eight
+// digits (|acc| < 6.1 q < 2^53), t0 and t1 stay below 1.25 q, t + res' below
+// 1.75 q + 1 before the final product, so every value is an exact integer
+// below 2^53 and the canonical outputs equal the integer form's word for
+// word.
+constexpr int MACF_NT = 128;
+
+template <int LOGN>
+__global__ void __launch_bounds__(MACF_NT, 4)
+p5_mac_fp(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
+          const u32* __restrict__ plist) {
+    constexpr int NT = MACF_NT;
+    constexpr int TILES = (1 << LOGN) / MAC_TILE;
+    constexpr int NV = MAC_TILE / (2 * NT);   // 16-byte vectors per thread
+    extern __shared__ __align__(16) u64 sm[];     // [dnum][2][MAC_TILE] signed doubles
+    double* smd = reinterpret_cast<double*>(sm);
+    const uint4 jb = jobs[blockIdx.x / TILES];
+    const u32 tile0 = (blockIdx.x % TILES) * MAC_TILE;
+    const u32 r = jb.x;                           // a Q row (r < fullQ), q < 2^50
+    const ModC m = D.mod[r];
+    const u32 dnum = D.dnum;
+    const double qd = ntt::u2d(m.q), hq = ntt::u2d(m.q >> 1);
+    const ntt::FpArS ar{qd, qinv_of(m)};
+    const u32 pin = r / D.alpha;                  // digit holding tower r
+    auto sgn = [&](u64 x) {                       // canonical -> signed double in (-q/2, q/2]
+        const double d = ntt::u2d(x);
+        return d > hq ? __dsub_rn(d, qd) : d;
+    };
+    const PairDesc& P0 = pairs[plist[jb.y]];
+    for (u32 k = threadIdx.x; k < dnum * MAC_TILE; k += NT) {
+        const u32 p = k / MAC_TILE, e = k % MAC_TILE;
+        const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0 + e;
+        u64 kb = P0.kbv[off], ka = P0.kav[off];
+        if (D.mont && p == pin) {
+            kb = redc(kb, 0, m);
+            ka = redc(ka, 0, m);
+        }
+        smd[(2 * p) * MAC_TILE + e] = sgn(kb);
+        smd[(2 * p + 1) * MAC_TILE + e] = sgn(ka);
+    }
+    __syncthreads();
+    const u64 q = m.q;
+    auto canon = [&](double z) { return ar.out(ar.norm(z)); };   // |z| < 2^52 -> [0, q)
+    for (u32 g = 0; g < jb.z; ++g) {
+        const PairDesc& P = pairs[plist[jb.y + g]];
+        const u32 L = P.L, K = D.K, QlP = L + K;
+        const u32 i = r;                          // QlP position of a Q row
+        const Level& lv = D.lvl[L];
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        const u32 nparts = lv.nparts;
+        const bool emr = P.mode == EMR;
+        const size_t o = ((size_t)i << LOGN) + tile0;
+        double s[2 * NV], t0[2 * NV], t1[2 * NV];
+        if (emr) {
+            ulonglong2 x0[NV], x1[NV], y0[NV], y1[NV];
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                const u32 e = 2 * (threadIdx.x + k * NT);
+                x0[k] = *reinterpret_cast<const ulonglong2*>(P.in[0] + o + e);
+                x1[k] = *reinterpret_cast<const ulonglong2*>(P.in[1] + o + e);
+                y0[k] = *reinterpret_cast<const ulonglong2*>(P.in[2] + o + e);
+                y1[k] = *reinterpret_cast<const ulonglong2*>(P.in[3] + o + e);
+            }
+#pragma unroll
+            for (int k = 0; k < NV; ++k)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const double a0 = ntt::u2d(v2get(x0[k], j)), a1 = ntt::u2d(v2get(x1[k], j));
+                    const double b0 = sgn(v2get(y0[k], j)), b1 = sgn(v2get(y1[k], j));
+                    s[2 * k + j] = ar.mulq<false>(a1, b1);
+                    t0[2 * k + j] = ar.mulq<false>(a0, b0);
+                    t1[2 * k + j] = __dadd_rn(ar.mulq<false>(a0, b1), ar.mulq<false>(a1, b0));
+                }
+        } else {
+#pragma unroll
+            for (int k = 0; k < NV; ++k)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const u32 e = tile0 + 2 * (threadIdx.x + k * NT) + j;
+                    const u64 x = (P.mode == ROT || P.mode == HROT)
+                                      ? P.in[1][((size_t)i << LOGN) + galois_slot<LOGN>(e, P.galois)]
+                                      : P.in[0][((size_t)i << LOGN) + e];
+                    s[2 * k + j] = ntt::u2d(x);
+                }
+        }
+        double acc_b[2 * NV], acc_a[2 * NV];
+#pragma unroll
+        for (int k = 0; k < 2 * NV; ++k) acc_b[k] = acc_a[k] = 0.0;
+        for (u32 p0 = 0; p0 < nparts; p0 += MAC_PCH) {
+            ulonglong2 v[MAC_PCH][NV];
+#pragma unroll
+            for (int pp = 0; pp < MAC_PCH; ++pp) {
+                const u32 p = p0 + pp;
+                if (p < nparts && p != pin) {
+                    const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN);
+                    if (P.mode == HROT) {   // sigma_k of the shared digit: eval-slot gather
+#pragma unroll
+                        for (int k = 0; k < NV; ++k)
+#pragma unroll
+                            for (int j = 0; j < 2; ++j)
+                                v2set(v[pp][k], j,
+                                      Yt[galois_slot<LOGN>(tile0 + 2 * (threadIdx.x + k * NT) + j, P.galois)]);
+                    } else {
+                        const ulonglong2* Y = reinterpret_cast<const ulonglong2*>(Yt + tile0);
+#pragma unroll
+                        for (int k = 0; k < NV; ++k) v[pp][k] = __ldcs(Y + threadIdx.x + k * NT);
+                    }
+                }
+            }
+#pragma unroll
+            for (int pp = 0; pp < MAC_PCH; ++pp) {
+                const u32 p = p0 + pp;
+                if (p >= nparts) break;
+                const double* kb = smd + (2 * p) * MAC_TILE;
+                const double* ka = smd + (2 * p + 1) * MAC_TILE;
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    const u32 e = 2 * (threadIdx.x + k * NT);
+                    const double2 kbv = *reinterpret_cast<const double2*>(kb + e);
+                    const double2 kav = *reinterpret_cast<const double2*>(ka + e);
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const double y = p == pin ? s[2 * k + j] : ntt::u2d(v2get(v[pp][k], j));
+                        acc_b[2 * k + j] = __dadd_rn(acc_b[2 * k + j], ar.mulq<false>(y, j ? kbv.y : kbv.x));
+                        acc_a[2 * k + j] = __dadd_rn(acc_a[2 * k + j], ar.mulq<false>(y, j ? kav.y : kav.x));
+                    }
+                }
+            }
+            if ((p0 & 7u) == 4u) {   // after every eighth digit: keep |acc| below 2^53
+#pragma unroll
+                for (int k = 0; k < 2 * NV; ++k) {
+                    acc_b[k] = ar.norm(acc_b[k]);
+                    acc_a[k] = ar.norm(acc_a[k]);
+                }
+            }
+        }
+        u64 *d0, *d1;
+        if (!emr) {   // keyswitch / rotation: W = res * P^-1
+            d0 = slot_ptr(P, w.W + i, LOGN) + tile0;
+            d1 = slot_ptr(P, w.W + L + i, LOGN) + tile0;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                const u32 e = 2 * (threadIdx.x + k * NT);
+                *reinterpret_cast<ulonglong2*>(d0 + e) = make_ulonglong2(canon(acc_b[2 * k]), canon(acc_b[2 * k + 1]));
+                *reinterpret_cast<ulonglong2*>(d1 + e) = make_ulonglong2(canon(acc_a[2 * k]), canon(acc_a[2 * k + 1]));
+            }
+            continue;
+        }
+        const bool drop = i == L - 1;
+        const double s1 = sgn(lv.s1[i]);
+        d0 = drop ? slot_ptr(P, w.U, LOGN) + tile0 : slot_ptr(P, w.W + i, LOGN) + tile0;
+        d1 = drop ? slot_ptr(P, w.U + 1, LOGN) + tile0 : slot_ptr(P, w.W + L + i, LOGN) + tile0;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const u32 e = 2 * (threadIdx.x + k * NT);
+            ulonglong2 o0, o1;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const double ua = __dadd_rn(t0[2 * k + j], ar.norm(acc_b[2 * k + j]));
+                const double ub = __dadd_rn(t1[2 * k + j], ar.norm(acc_a[2 * k + j]));
+                u64 wa, wb;
+                if (drop) {   // U: the integer form's scale, (t + res') * R^-1 with mont
+                    wa = canon(ua);
+                    wb = canon(ub);
+                    if (D.mont) {
+                        wa = redc(wa, 0, m);
+                        wb = redc(wb, 0, m);
+                    }
+                } else {
+                    wa = canon(ar.mulq<true>(ua, s1));
+                    wb = canon(ar.mulq<true>(ub, s1));
+                }
+                v2set(o0, j, wa);
+                v2set(o1, j, wb);
+            }
+            *reinterpret_cast<ulonglong2*>(d0 + e) = o0;
+            *reinterpret_cast<ulonglong2*>(d1 + e) = o1;
+        }
+    }
+    (void)q;
+}
+
 // P5, pipelined form (dnum small enough for the staging buffers): 256
 // threads, each owning one 16-byte pair of the 512-element tile. While a
 // pair is multiplied, the tiles of the next pair (the four tensor inputs or
