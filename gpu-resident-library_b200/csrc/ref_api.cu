@@ -17,6 +17,7 @@
 #include <stdexcept>
 #include <string>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "ckks_ops.h"
@@ -280,43 +281,56 @@ namespace gpufhe {
 bool g_ks_batched = true;
 
 // ---------------------------------------------------------------- DeviceCiphertext
+// Both components live in one device allocation: c0 at the start, c1 right
+// after the n x towers words of c0 (one cudaMalloc, one cudaFree). The
+// object owns that allocation through d_c0_; d_c1_ points into it.
+namespace {
+void release_components(uint64_t*& c0, uint64_t*& c1) {
+    if (c0) cudaFree(c0);
+    c0 = c1 = nullptr;
+}
+void check_words(const char* what, size_t have, size_t want) {
+    if (have != want)
+        throw std::runtime_error(std::string("gpufhe::DeviceCiphertext: ") + what + " has " + std::to_string(have) +
+                                 " words, the ciphertext holds " + std::to_string(want) + " per component");
+}
+}  // namespace
+
 DeviceCiphertext::DeviceCiphertext(Scheme scheme, uint32_t n, uint32_t num_towers)
     : scheme_(scheme), n_(n), towers_(num_towers) {
-    const size_t bytes = (size_t)n_ * towers_ * sizeof(uint64_t);
-    ck(cudaMalloc(&d_c0_, bytes), "DeviceCiphertext: cudaMalloc c0");
-    cudaError_t e = cudaMalloc(&d_c1_, bytes);
-    if (e != cudaSuccess) { cudaFree(d_c0_); d_c0_ = nullptr; ck(e, "DeviceCiphertext: cudaMalloc c1"); }
+    const size_t words = (size_t)n_ * towers_;
+    ck(cudaMalloc(&d_c0_, std::max<size_t>(2 * words, 1) * sizeof(uint64_t)), "DeviceCiphertext: device allocation");
+    d_c1_ = d_c0_ + words;
 }
-DeviceCiphertext::~DeviceCiphertext() {
-    if (d_c0_) cudaFree(d_c0_);
-    if (d_c1_) cudaFree(d_c1_);
-}
+DeviceCiphertext::~DeviceCiphertext() { release_components(d_c0_, d_c1_); }
 DeviceCiphertext::DeviceCiphertext(DeviceCiphertext&& o) noexcept
     : scheme_(o.scheme_), format_(o.format_), n_(o.n_), towers_(o.towers_), d_c0_(o.d_c0_), d_c1_(o.d_c1_) {
     o.d_c0_ = o.d_c1_ = nullptr;
 }
 DeviceCiphertext& DeviceCiphertext::operator=(DeviceCiphertext&& o) noexcept {
-    if (this != &o) {
-        if (d_c0_) cudaFree(d_c0_);
-        if (d_c1_) cudaFree(d_c1_);
-        scheme_ = o.scheme_; format_ = o.format_; n_ = o.n_; towers_ = o.towers_;
-        d_c0_ = o.d_c0_; d_c1_ = o.d_c1_;
-        o.d_c0_ = o.d_c1_ = nullptr;
-    }
+    if (this == &o) return *this;
+    release_components(d_c0_, d_c1_);
+    std::swap(scheme_, o.scheme_);
+    std::swap(format_, o.format_);
+    std::swap(n_, o.n_);
+    std::swap(towers_, o.towers_);
+    std::swap(d_c0_, o.d_c0_);
+    std::swap(d_c1_, o.d_c1_);
     return *this;
 }
 void DeviceCiphertext::upload(const std::vector<uint64_t>& c0, const std::vector<uint64_t>& c1) {
-    const size_t need = (size_t)n_ * towers_;
-    if (c0.size() != need || c1.size() != need) throw std::runtime_error("DeviceCiphertext::upload size mismatch");
-    ck(cudaMemcpy(d_c0_, c0.data(), need * 8, cudaMemcpyHostToDevice), "DeviceCiphertext: upload c0");
-    ck(cudaMemcpy(d_c1_, c1.data(), need * 8, cudaMemcpyHostToDevice), "DeviceCiphertext: upload c1");
+    const size_t words = (size_t)n_ * towers_;
+    check_words("upload: c0", c0.size(), words);
+    check_words("upload: c1", c1.size(), words);
+    ck(cudaMemcpy(d_c0_, c0.data(), words * sizeof(uint64_t), cudaMemcpyHostToDevice), "DeviceCiphertext: c0 to device");
+    ck(cudaMemcpy(d_c1_, c1.data(), words * sizeof(uint64_t), cudaMemcpyHostToDevice), "DeviceCiphertext: c1 to device");
 }
 void DeviceCiphertext::to_host(std::vector<uint64_t>& c0, std::vector<uint64_t>& c1) const {
-    const size_t need = (size_t)n_ * towers_;
-    c0.resize(need);
-    c1.resize(need);
-    ck(cudaMemcpy(c0.data(), d_c0_, need * 8, cudaMemcpyDeviceToHost), "DeviceCiphertext: to_host c0");
-    ck(cudaMemcpy(c1.data(), d_c1_, need * 8, cudaMemcpyDeviceToHost), "DeviceCiphertext: to_host c1");
+    const size_t words = (size_t)n_ * towers_;
+    c0.assign(words, 0);
+    c1.assign(words, 0);
+    ck(cudaMemcpy(c0.data(), d_c0_, words * sizeof(uint64_t), cudaMemcpyDeviceToHost), "DeviceCiphertext: c0 to host");
+    ck(cudaMemcpy(c1.data(), d_c1_, words * sizeof(uint64_t), cudaMemcpyDeviceToHost), "DeviceCiphertext: c1 to host");
 }
 
 // ---------------------------------------------------------------- DeviceTables

@@ -125,8 +125,8 @@ def test_budget_admission(G, setups, gctxs):
 
 
 def test_active_cap(G, setups, gctxs):
-    """max_active bounds the requests admitted at once (the bench's served
-    form runs with a cap); the results are the same bits as uncapped."""
+    """max_active bounds the requests admitted at once (an option beside the
+    HBM budget); the results are the same bits as uncapped."""
     reqs = make_trace(setups, 12, seed=21)
     for r in reqs:
         r["arrival"] = 0.0
