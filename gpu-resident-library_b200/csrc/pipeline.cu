@@ -80,7 +80,8 @@ struct Launcher {
         cudaFuncSetAttribute(p5_mac<LOGN, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
         cudaFuncSetAttribute(p5_mac_async<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_ASYNC_SMEM_MAX);
         cudaFuncSetAttribute(p5_mac_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
-        cudaFuncSetAttribute(p5_mac_fp<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
+        cudaFuncSetAttribute(p5_mac_fp<LOGN, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
+        cudaFuncSetAttribute(p5_mac_fp<LOGN, 2, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
     }
     // persistent warp-specialised P3 over job segment PATH: form 1 = 128
     // conversion threads, two CTAs per SM; form 2 = 256, one CTA per SM
@@ -120,8 +121,11 @@ struct Launcher {
                 // the FP64 kernel when p5_fp, else both to the integer form
                 const uint32_t nfp = p.p5_fp ? p.job_cnt[4][1] : 0u;
                 const uint32_t nint = p.job_cnt[4][0] + p.job_cnt[4][1] - nfp;
-                if (nfp)
-                    p5_mac_fp<LOGN><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), s>>>(
+                if (nfp && p.p5_fp_form == 1)
+                    p5_mac_fp<LOGN, 2, 5><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), s>>>(
+                        D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
+                else if (nfp)
+                    p5_mac_fp<LOGN, 4, 4><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), s>>>(
                         D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
                 if (!nint) continue;
                 const unsigned grid = nint * MAC_TILES;
@@ -513,11 +517,13 @@ uint64_t tune_key(const Plan& p) {
 }
 // choice: bits 0-1 = P5 form, bits 3-4 = P3 form (0 plain, 1 and 2
 // warp-specialised), bit 6 = P5 key rows of 50-bit Q towers on the FP64
-// pipe, bits 8-16 = phases launched over their interleaved integer / FP64
-// job list (else as two launches)
+// pipe, bit 7 = its occupancy form (0: 4 digits in flight, 4 CTAs per SM;
+// 1: 2 digits, 5 CTAs), bits 8-16 = phases launched over their interleaved
+// integer / FP64 job list (else as two launches)
 void apply_choice(Plan& p, int choice) {
     p.p5_form = choice & 3;
     p.p5_fp = (choice >> 6) & 1;
+    p.p5_fp_form = (choice >> 7) & 1;
     if (p.p5_form == P5_ASYNC && !mac_async_ok(p.dc.dnum)) p.p5_form = P5_REG128;
     if (p.p5_form == P5_TMA && !mac_tma_ok(p.dc.dnum)) p.p5_form = P5_REG128;
     p.mix = ((unsigned)choice >> 8) & 0x1ffu;
@@ -583,7 +589,7 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         cur = pick(1u << k, bit, {bit, 0}, cur);
     }
     cur = pick(1u << 2, 24, {0, 8, 16}, cur);                      // P3 form
-    if (p.job_cnt[4][1]) cur = pick(1u << 4, 64, {64, 0}, cur);     // P5 FP64 rows or integer rows
+    if (p.job_cnt[4][1]) cur = pick(1u << 4, 64 | 128, {64, 64 | 128, 0}, cur);   // P5 FP64 rows (two forms) or integer
     std::vector<int> p5v = {P5_REG128, P5_REG256};
     if (mac_async_ok(p.dc.dnum)) p5v.push_back(P5_ASYNC);
     if (mac_tma_ok(p.dc.dnum)) p5v.push_back(P5_TMA);

@@ -686,10 +686,12 @@ p5_mac(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restri
 // 1.75 q + 1 before the final product, so every value is an exact integer
 // below 2^53 and the canonical outputs equal the integer form's word for
 // word.
+// Two occupancy forms: PCH digits' loads in flight per batch and MINB CTAs
+// per SM (4 digits / 4 CTAs at 128 registers, or 2 digits / 5 CTAs at 94).
 constexpr int MACF_NT = 128;
 
-template <int LOGN>
-__global__ void __launch_bounds__(MACF_NT, 4)
+template <int LOGN, int PCH, int MINB>
+__global__ void __launch_bounds__(MACF_NT, MINB)
 p5_mac_fp(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
           const u32* __restrict__ plist) {
     constexpr int NT = MACF_NT;
@@ -769,10 +771,10 @@ p5_mac_fp(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __res
         double acc_b[2 * NV], acc_a[2 * NV];
 #pragma unroll
         for (int k = 0; k < 2 * NV; ++k) acc_b[k] = acc_a[k] = 0.0;
-        for (u32 p0 = 0; p0 < nparts; p0 += MAC_PCH) {
-            ulonglong2 v[MAC_PCH][NV];
+        for (u32 p0 = 0; p0 < nparts; p0 += PCH) {
+            ulonglong2 v[PCH][NV];
 #pragma unroll
-            for (int pp = 0; pp < MAC_PCH; ++pp) {
+            for (int pp = 0; pp < PCH; ++pp) {
                 const u32 p = p0 + pp;
                 if (p < nparts && p != pin) {
                     const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN);
@@ -791,7 +793,7 @@ p5_mac_fp(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __res
                 }
             }
 #pragma unroll
-            for (int pp = 0; pp < MAC_PCH; ++pp) {
+            for (int pp = 0; pp < PCH; ++pp) {
                 const u32 p = p0 + pp;
                 if (p >= nparts) break;
                 const double* kb = smd + (2 * p) * MAC_TILE;

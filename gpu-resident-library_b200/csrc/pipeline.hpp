@@ -39,6 +39,7 @@ struct Plan {
     // launch schedule (chosen by tune() or the context's tuning cache)
     int p5_form = 0;                   // P5_REG128, P5_ASYNC or P5_REG256
     bool p5_fp = false;                // P5 key rows of 50-bit Q towers on the FP64 pipe (p5_mac_fp)
+    int p5_fp_form = 0;                // 0: 4 digits in flight, 4 CTAs per SM; 1: 2 digits, 5 CTAs
     unsigned mix = 0x1ff;              // bit k: phase k+1 as one launch over its interleaved job list
     int p3_form = 0;                   // 0 plain P3; 1, 2 warp-specialised (128 x 2 CTAs, 256 x 1 CTA)
     bool tuned = false;

@@ -19,7 +19,7 @@ def S():
     return Setup(N, 6, K=2, alpha=2, rot_ks=(5, O.galois_element(3, N)))
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 8, 16, 7, 64, 67, 71])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 8, 16, 7, 64, 67, 71, 192])
 def test_mixed_batch_small_ring(S, schedule):
     import gpufhe_b200 as G
     g = S.gpu_context()
@@ -96,7 +96,7 @@ def test_forms_after_a_larger_dnum():
         g.set_key(0, key[0], key[1])
         x = [dev(np.concatenate([rng.integers(0, int(q), N, dtype=np.uint64) for q in Q[:tw]])) for _ in range(4)]
         got = []
-        for sched in (0, 1, 2, 3, 64, 67):
+        for sched in (0, 1, 2, 3, 64, 67, 192):
             o0, o1 = empty((tw - 1) * N), empty((tw - 1) * N)
             plan = G.Plan(g, [dict(level=tw, inp=[ptr(t) for t in x], out=[ptr(o0), ptr(o1)])])
             plan.set_schedule(sched)
