@@ -105,3 +105,35 @@ def test_forms_after_a_larger_dnum():
             got.append((host(o0), host(o1)))
         for k in range(1, len(got)):
             assert np.array_equal(got[k][0], got[0][0]) and np.array_equal(got[k][1], got[0][1]), (tw, k)
+
+
+@pytest.mark.parametrize("schedule", [64, 192, 0])
+def test_many_digits_fp64_key_product(schedule):
+    """Twelve digits (alpha = 1): the FP64 key inner product normalises its
+    accumulators after every eighth digit; EvalMult+Rescale and keyswitch at
+    every digit count up to twelve equal the oracle in the FP64 forms and in
+    the integer form."""
+    import gpufhe_b200 as G
+    S = Setup(N, 12, K=2, alpha=1, seed=33)
+    g = S.gpu_context()
+    rng = np.random.default_rng(77 + schedule)
+    keep, specs, want = [], [], []
+    for L in (2, 9, 12):
+        c0a, c1a = S.rand_ct(rng, L)
+        c0b, c1b = S.rand_ct(rng, L)
+        ins = [dev(x) for x in (c0a, c1a, c0b, c1b)]
+        outs = [empty((L - 1) * N), empty((L - 1) * N)]
+        keep += ins + outs
+        specs.append(dict(level=L, inp=[ptr(x) for x in ins], out=[ptr(x) for x in outs]))
+        want.append((outs, S.octx.evalmult_rescale(L, c0a, c1a, c0b, c1b)))
+        k0, k1 = empty(L * N), empty(L * N)
+        keep += [k0, k1]
+        specs.append(dict(level=L, mode=G.KEYSWITCH, inp=[ptr(ins[0])], out=[ptr(k0), ptr(k1)]))
+        want.append(([k0, k1], S.octx.keyswitch(L, c0a)))
+    plan = G.Plan(g, specs)
+    plan.set_schedule(schedule)
+    plan.launch()
+    sync()
+    assert plan.schedule()["p5_fp64_rows"] == bool(schedule & 64)
+    for j, (outs, (e0, e1)) in enumerate(want):
+        assert np.array_equal(host(outs[0]), e0) and np.array_equal(host(outs[1]), e1), j
