@@ -18,6 +18,8 @@ namespace {
 
 int sm_count() { return gfx::current_sm_count(); }
 
+
+
 // PATH 0 / 1: the integer / FP64 job segment of a phase; PATH 2: the mixed
 // segment (both kinds interleaved, one launch).
 template <int LOGN, int PATH>
@@ -109,6 +111,23 @@ struct Launcher {
                 p.dc, p.d_pairs, J, ntiles);
         }
     }
+    // The integer forms of P5 over the first nint key-row jobs.
+    static void launch_p5_int(const Plan& p, cudaStream_t s, uint32_t nint) {
+        constexpr int MAC_TILES = (1 << LOGN) / MAC_TILE;
+        const DevCtx& D = p.dc;
+        const unsigned grid = nint * MAC_TILES;
+        if (p.p5_form == P5_TMA && mac_tma_ok(D.dnum))
+            p5_mac_tma<LOGN><<<nint * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum), s>>>(
+                D, p.d_pairs, p.d_mac_jobs, p.d_plist);
+        else if (p.p5_form == P5_ASYNC && mac_async_ok(D.dnum))
+            p5_mac_async<LOGN><<<grid, MACA_NT, maca_smem((int)D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
+                                                                             p.d_plist);
+        else if (p.p5_form == P5_REG256)
+            p5_mac<LOGN, 256><<<grid, 256, mac_smem(D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs, p.d_plist);
+        else
+            p5_mac<LOGN, MAC_NT><<<grid, MAC_NT, mac_smem(D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
+                                                                       p.d_plist);
+    }
     static void launch(const Plan& p, cudaStream_t s, unsigned mask) {
         using G = ntt::Geo<LOGN>;
         constexpr int MAC_TILES = (1 << LOGN) / MAC_TILE;
@@ -121,25 +140,29 @@ struct Launcher {
                 // the FP64 kernel when p5_fp, else both to the integer form
                 const uint32_t nfp = p.p5_fp ? p.job_cnt[4][1] : 0u;
                 const uint32_t nint = p.job_cnt[4][0] + p.job_cnt[4][1] - nfp;
+                // with p5_split the FP64 rows run on a second stream beside the integer
+                // rows (different pipes, disjoint outputs), joined before P6
+                cudaStream_t sf = s;
+                const bool split = p.p5_split && nfp && nint && ensure_side(p);
+                if (split) {
+                    cudaEventRecord(p.ev_fork, s);
+                    cudaStreamWaitEvent(p.side, p.ev_fork, 0);
+                    sf = p.side;
+                }
                 if (nfp && p.p5_fp_form == 1)
-                    p5_mac_fp<LOGN, 2, 5><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), s>>>(
+                    p5_mac_fp<LOGN, 2, 5><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), sf>>>(
                         D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
                 else if (nfp)
-                    p5_mac_fp<LOGN, 4, 4><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), s>>>(
+                    p5_mac_fp<LOGN, 4, 4><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), sf>>>(
                         D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
+                if (split) {
+                    launch_p5_int(p, s, nint);
+                    cudaEventRecord(p.ev_join, p.side);
+                    cudaStreamWaitEvent(s, p.ev_join, 0);
+                    continue;
+                }
                 if (!nint) continue;
-                const unsigned grid = nint * MAC_TILES;
-                if (p.p5_form == P5_TMA && mac_tma_ok(D.dnum))
-                    p5_mac_tma<LOGN><<<nint * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum), s>>>(
-                        D, p.d_pairs, p.d_mac_jobs, p.d_plist);
-                else if (p.p5_form == P5_ASYNC && mac_async_ok(D.dnum))
-                    p5_mac_async<LOGN><<<grid, MACA_NT, maca_smem((int)D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
-                                                                                     p.d_plist);
-                else if (p.p5_form == P5_REG256)
-                    p5_mac<LOGN, 256><<<grid, 256, mac_smem(D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs, p.d_plist);
-                else
-                    p5_mac<LOGN, MAC_NT><<<grid, MAC_NT, mac_smem(D.dnum), s>>>(D, p.d_pairs, p.d_mac_jobs,
-                                                                               p.d_plist);
+                launch_p5_int(p, s, nint);
             } else if (k == 6) {   // P7a then P7b (U and r_l need the P towers)
                 for (int kk : {6, (int)NPHASE}) {
                     if ((p.mix >> 6 & 1) && p.job_cnt[kk][0] && p.job_cnt[kk][1]) {
@@ -330,6 +353,25 @@ static void fill_tables(const gfx::Context& c, const std::vector<Op>& ops, const
     T.job_cnt[4][2] = 0;
 }
 
+// The plan's second stream and fork / join events (made on the current device
+// at first use); false if they cannot be made, and P5 then runs on one stream.
+bool ensure_side(const Plan& p) {
+    if (p.side) return true;
+    cudaStream_t st = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return false;
+    if (cudaEventCreateWithFlags(&a, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b, cudaEventDisableTiming) != cudaSuccess) {
+        if (a) cudaEventDestroy(a);
+        cudaStreamDestroy(st);
+        return false;
+    }
+    p.side = st;
+    p.ev_fork = a;
+    p.ev_join = b;
+    return true;
+}
+
 Plan::Plan() : staging(std::make_unique<HostTables>()) {}
 
 Plan::~Plan() {
@@ -340,6 +382,9 @@ Plan::~Plan() {
     if (d_blob) cudaFree(d_blob);
     if (h_blob) cudaFreeHost(h_blob);
     for (void* h : old_h_blobs) cudaFreeHost(h);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (own_ws && ws) cudaFree(ws);
 }
 
@@ -519,11 +564,14 @@ uint64_t tune_key(const Plan& p) {
 // warp-specialised), bit 6 = P5 key rows of 50-bit Q towers on the FP64
 // pipe, bit 7 = its occupancy form (0: 4 digits in flight, 4 CTAs per SM;
 // 1: 2 digits, 5 CTAs), bits 8-16 = phases launched over their interleaved
-// integer / FP64 job list (else as two launches)
+// integer / FP64 job list (else as two launches), bit 17 = P5's FP64 and
+// integer rows on two streams at once
 void apply_choice(Plan& p, int choice) {
     p.p5_form = choice & 3;
     p.p5_fp = (choice >> 6) & 1;
     p.p5_fp_form = (choice >> 7) & 1;
+    p.p5_split = (choice >> 17) & 1;
+    if (p.p5_split) ensure_side(p);   // outside any graph capture where possible
     if (p.p5_form == P5_ASYNC && !mac_async_ok(p.dc.dnum)) p.p5_form = P5_REG128;
     if (p.p5_form == P5_TMA && !mac_tma_ok(p.dc.dnum)) p.p5_form = P5_REG128;
     p.mix = ((unsigned)choice >> 8) & 0x1ffu;
@@ -589,7 +637,10 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         cur = pick(1u << k, bit, {bit, 0}, cur);
     }
     cur = pick(1u << 2, 24, {0, 8, 16}, cur);                      // P3 form
-    if (p.job_cnt[4][1]) cur = pick(1u << 4, 64 | 128, {64, 64 | 128, 0}, cur);   // P5 FP64 rows (two forms) or integer
+    if (p.job_cnt[4][1]) {
+        cur = pick(1u << 4, 64 | 128, {64, 64 | 128, 0}, cur);   // P5 FP64 rows (two forms) or integer
+        if (cur & 64) cur = pick(1u << 4, 1 << 17, {0, 1 << 17}, cur);   // FP64 and integer rows concurrent
+    }
     std::vector<int> p5v = {P5_REG128, P5_REG256};
     if (mac_async_ok(p.dc.dnum)) p5v.push_back(P5_ASYNC);
     if (mac_tma_ok(p.dc.dnum)) p5v.push_back(P5_TMA);

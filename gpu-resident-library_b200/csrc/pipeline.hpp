@@ -40,6 +40,10 @@ struct Plan {
     int p5_form = 0;                   // P5_REG128, P5_ASYNC or P5_REG256
     bool p5_fp = false;                // P5 key rows of 50-bit Q towers on the FP64 pipe (p5_mac_fp)
     int p5_fp_form = 0;                // 0: 4 digits in flight, 4 CTAs per SM; 1: 2 digits, 5 CTAs
+    bool p5_split = false;             // FP64 and integer P5 rows on two streams at once (fork / join)
+    // the second stream and its fork / join events, made on first use
+    mutable cudaStream_t side = nullptr;
+    mutable cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     unsigned mix = 0x1ff;              // bit k: phase k+1 as one launch over its interleaved job list
     int p3_form = 0;                   // 0 plain P3; 1, 2 warp-specialised (128 x 2 CTAs, 256 x 1 CTA)
     bool tuned = false;
@@ -59,6 +63,9 @@ struct Plan {
 };
 
 bool supported_logn(int logn);
+// Makes the plan's second stream and fork / join events on the current
+// device (once); false when they cannot be made.
+bool ensure_side(const Plan& p);
 size_t op_workspace_words(const gfx::Context& c, uint32_t L);
 void validate(const gfx::Context& c, const Op& op);
 // ws == nullptr: the plan allocates (and owns) its workspace.

@@ -325,11 +325,13 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
  * product (P5) of Q towers with q < 2^50 on the FP64 pipe (exact FP64 modular
  * products) beside the chosen integer form for the other rows, bit 7 = that
  * FP64 form's occupancy (0: four digits' loads in flight, four CTAs per SM;
- * 1: two digits, five CTAs), bits 8-16 = the
+ * 1: two digits, five CTAs), bit 17 = those FP64 rows on a second stream
+ * beside the integer rows (forked and joined inside the launch, graph-
+ * capturable), bits 8-16 = the
  * phases (bit 8 + k for phase k+1) launched interleaved (the others as two
  * launches). */
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan);
-/* Fixes the schedule (bits 0-4, 6-7 and 8-16 as above; bit 2 sets every phase
+/* Fixes the schedule (bits 0-4, 6-7 and 8-17 as above; bit 2 sets every phase
  * interleaved) and skips the autotuner; every schedule computes the same bits. */
 int      gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule);
 /* Host-buffer form: copies h_in[4*i+k] (host, level*n words) into op i's
