@@ -636,6 +636,62 @@ def ntt_isolation(G, torch, dev, local, cur, gen):
     return ntt
 
 
+def conversion_isolation(G, torch, dev, gen, coeffs=1 << 22, reps=10):
+    """ApproxSwitchCRTBasis over `coeffs` coefficients in its three forms
+    (integer pipes; tensor cores by byte limbs: tcgen05.mma kind::i8 and the
+    warp-level mma.sync) at ModUp widths 8 -> 24 (the serving contexts,
+    alpha = 8) and 3 -> 12 (the step, alpha = 3); 50-bit sources, 60-bit
+    targets. Milliseconds per launch by CUDA events (best of three x reps)
+    and the input + output bytes per launch over that time; the three forms'
+    outputs are compared word for word."""
+    out = {"coefficients_per_launch": coeffs}
+    for sizeQ, sizeP in ((8, 24), (3, 12)):
+        Qm = G.native_primes(sizeQ, 50, 1 << N_LOG)
+        Pm = G.native_primes(sizeP, 60, 1 << N_LOG, avoid=list(Qm))
+        prod = 1
+        for q in Qm:
+            prod *= int(q)
+        qhi = [pow((prod // int(q)) % int(q), -1, int(q)) for q in Qm]
+        consts = [np.array(qhi, np.uint64),
+                  np.array([(h << 64) // int(q) for h, q in zip(qhi, Qm)], np.uint64),
+                  np.array(Qm, np.uint64),
+                  np.array([[(prod // int(q)) % int(pp) for pp in Pm] for q in Qm], np.uint64).ravel(),
+                  np.array(Pm, np.uint64),
+                  np.array([(((1 << 128) - 1) // int(pp)) & (2 ** 64 - 1) for pp in Pm], np.uint64),
+                  np.array([((1 << 128) - 1) // int(pp) >> 64 for pp in Pm], np.uint64)]
+        dc = [torch.from_numpy(c.view(np.int64).copy()).to(dev) for c in consts]
+        src = torch.empty(sizeQ * coeffs, dtype=torch.int64, device=dev)
+        for i in range(sizeQ):
+            src[i * coeffs:(i + 1) * coeffs].random_(0, int(Qm[i]), generator=gen)
+        dsts = {f: torch.empty(sizeP * coeffs, dtype=torch.int64, device=dev) for f in ("tcgen05", "mma_sync", "integer")}
+        form_id = {"tcgen05": 0, "mma_sync": 1, "integer": 2}
+        res = {}
+        for f, dst in dsts.items():
+            run = lambda: G.check(G.lib().gpufhe_approx_switch(src.data_ptr(), dst.data_ptr(), *[c.data_ptr() for c in dc],
+                                                              sizeQ, sizeP, coeffs, form_id[f], None))
+            for _ in range(3):
+                run()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            best = 1e30
+            for _ in range(3):
+                a.record()
+                for _ in range(reps):
+                    run()
+                b.record()
+                torch.cuda.synchronize()
+                best = min(best, a.elapsed_time(b) / reps)
+            res[f] = {"ms": best, "gbs": 8 * coeffs * (sizeQ + sizeP) / (best * 1e-3) / 1e9}
+        st = np.zeros(1, np.uint32)
+        G.check(G.lib().gpufhe_approx_switch_status(st.ctypes.data))
+        res["same_bits"] = bool(torch.equal(dsts["tcgen05"], dsts["integer"]) and torch.equal(dsts["mma_sync"], dsts["integer"]))
+        res["tcgen05_status"] = int(st[0])
+        res["tcgen05_speedup"] = res["integer"]["ms"] / res["tcgen05"]["ms"]
+        out[f"{sizeQ}to{sizeP}"] = res
+        del src, dsts, dc
+    return out
+
+
 # ---------------------------------------------------------------- rotation batch
 ROT_TOWERS, ROT_COUNT, ROT_HOIST = 10, 256, 16
 ENC_COUNT = 16
@@ -896,6 +952,12 @@ def run_gpu(args):
         res = ntt_isolation(G, torch, dev, local, torch.cuda.current_stream().cuda_stream, gen)
         print(json.dumps({"section": "ntt", "ntt_kernel_isolation": res}), flush=True)
         return 0
+    if args.section == "convert":
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SEED)
+        res = conversion_isolation(G, torch, dev, gen)
+        print(json.dumps({"section": "convert", "basis_conversion": res}), flush=True)
+        return 0
     if args.section == "rot":
         gen = torch.Generator(device=dev)
         gen.manual_seed(SEED)
@@ -1099,6 +1161,7 @@ def run_gpu(args):
 
     # kernel isolation: 64 polys x 12 towers x 2^16
     ntt = None if args.no_ntt else ntt_isolation(G, torch, dev, local, cur, gen)
+    conv = None if args.no_ntt else conversion_isolation(G, torch, dev, gen)
 
     # rotation batch (plain and hoisted)
     rotation = None
@@ -1170,6 +1233,7 @@ def run_gpu(args):
         "latency_ms": (dict(serving["served"]["latency_ms"], source="serving trace, served form") if serving
                        else {"p50": ms_step, "p99": ms_step, "source": "whole batch per step"}),
         "ntt_kernel_isolation": ntt,
+        "basis_conversion_isolation": conv,
         "rotation_batch": rotation,
         "bootstrap_steps": rotation.pop("bootstrap_steps") if rotation else None,
         "serving": serving,
@@ -1194,8 +1258,9 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-rot", action="store_true")
     ap.add_argument("--pairs", type=int, default=PAIRS, help="pairs per step (smaller only for profiling)")
-    ap.add_argument("--section", default="all", choices=["all", "ntt", "rot"],
-                    help="ntt / rot: only the kernel isolation or the rotation batch (prints its own line)")
+    ap.add_argument("--section", default="all", choices=["all", "ntt", "rot", "convert"],
+                    help="ntt / rot / convert: only the transform isolation, the rotation batch or the basis-"
+                         "conversion isolation (prints its own line)")
     ap.add_argument("--serve-requests", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:

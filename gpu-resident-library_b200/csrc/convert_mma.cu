@@ -45,6 +45,12 @@ __device__ __forceinline__ void mma_u8(int (&c)[4], const uint32_t (&a)[4], uint
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// acc += a * b with a, b 32-bit (one wide multiply-add): folds a 32-bit
+// partial sum into a 64-bit word at a byte shift b = 2^(8k).
+__device__ __forceinline__ void mad_wide(u64& acc, uint32_t a, uint32_t b) {
+    asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc) : "r"(a), "r"(b));
+}
+
 __device__ __forceinline__ u64 bswap64(u64 v) {
     return ((u64)__byte_perm((uint32_t)v, 0, 0x0123) << 32) | __byte_perm((uint32_t)(v >> 32), 0, 0x0123);
 }
@@ -254,7 +260,7 @@ __device__ __forceinline__ u32 canon_off(int r, int h) { return (u32)((r & 7) * 
 __device__ __forceinline__ u64 tc_reduce(const uint32_t (&cs)[16], const ModC& m) {
     u64 acc4[4] = {0, 0, 0, 0};
 #pragma unroll
-    for (int sft = 0; sft < 15; ++sft) acc4[sft >> 2] += (u64)cs[sft] << (8 * (sft & 3));
+    for (int sft = 0; sft < 15; ++sft) mad_wide(acc4[sft >> 2], cs[sft], 1u << (8 * (sft & 3)));
     u64 lo = acc4[0], hi = acc4[2] + (acc4[3] << 32);
     add_wide(lo, hi, acc4[1] << 32, acc4[1] >> 32);
     return barrett(lo, hi, m);
