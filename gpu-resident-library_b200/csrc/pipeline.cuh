@@ -1103,92 +1103,121 @@ __device__ __forceinline__ void bulk_load(u32 dst, const void* src, u32 bytes, u
                  : "memory");
 }
 
+// Ring of the TMA forms: mbarriers at the start of dynamic shared memory
+// (key, full[S], empty[S]), then the key tile [dnum][2][P5T_TILE], then
+// P5T_STAGES stages of maca_slots(dnum) rows.
+struct P5Ring {
+    u64* keys;
+    u64* stage;
+    u32 kbar;
+    __device__ __forceinline__ u32 full(u32 b) const { return kbar + 8 * (1 + b); }
+    __device__ __forceinline__ u32 empty(u32 b) const { return kbar + 8 * (1 + P5T_STAGES + b); }
+};
+
+// Thread 0 initialises the mbarriers; every thread learns whether an earlier
+// CTA's wait expired (then the CTA leaves before issuing anything).
+__device__ __forceinline__ bool p5t_setup(const DevCtx& D, u64* sm, P5Ring& R) {
+    __shared__ u32 failed;
+    R.keys = sm + P5T_BAR_WORDS;
+    R.stage = R.keys + 2 * D.dnum * P5T_TILE;
+    R.kbar = smem_addr(sm);
+    if (threadIdx.x == 0) {
+        failed = *reinterpret_cast<volatile u32*>(D.err);
+        mbar_init(R.kbar, 1);
+        for (u32 b = 0; b < P5T_STAGES; ++b) {
+            mbar_init(R.full(b), 1);
+            mbar_init(R.empty(b), P5T_NC);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();                            // the only CTA-wide barrier
+    return failed == 0;
+}
+
+// The producer (one thread): the key tile of row r once, then per listed
+// pair the tensor inputs (EvalMult+Rescale, slots 0-3) or the keyswitch input
+// (slot 1) of a Q row and every other digit of its tower (slot MACA_IN + p),
+// into stage g % S after the consumers have released it; finally it waits
+// (bounded) for every copy in flight.
+template <int LOGN>
+__device__ __forceinline__ void p5t_produce(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
+                                            const u32* __restrict__ plist, const u32 tile0, const P5Ring& R) {
+    constexpr u32 ROW = P5T_TILE * 8;           // bytes of one staged row
+    constexpr int S = P5T_STAGES;
+    const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum), K = D.K;
+    const bool is_p = r >= D.fullQ;
+    const PairDesc& P0 = pairs[plist[jb.y]];
+    mbar_arrive_expect_tx(R.kbar, 2 * dnum * ROW);
+    for (u32 p = 0; p < dnum; ++p) {
+        const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0;
+        bulk_load(smem_addr(R.keys + (2 * p) * P5T_TILE), P0.kbv + off, ROW, R.kbar);
+        bulk_load(smem_addr(R.keys + (2 * p + 1) * P5T_TILE), P0.kav + off, ROW, R.kbar);
+    }
+    u32 issued = 0;
+    for (u32 g = 0; g < jb.z; ++g) {
+        const u32 b = g % S;
+        if (g >= S && !mbar_wait(R.empty(b), (g / S - 1) & 1)) {
+            atomicOr(D.err, 4u);
+            break;
+        }
+        const PairDesc& P = pairs[plist[jb.y + g]];
+        const u32 L = P.L, QlP = L + K;
+        const u32 i = is_p ? L + (r - D.fullQ) : r;
+        const u32 pin = is_p ? 0xffffffffu : i / D.alpha;
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        const u32 nparts = D.lvl[L].nparts;
+        const u32 nin = is_p ? 0u : (P.mode == EMR ? 4u : (P.mode == KS ? 1u : 0u));
+        const u32 ndig = P.mode == HROT ? 0u : nparts - (pin < nparts ? 1u : 0u);
+        u64* sb = R.stage + (size_t)b * slots * P5T_TILE;
+        const size_t o = ((size_t)i << LOGN) + tile0;
+        mbar_arrive_expect_tx(R.full(b), (nin + ndig) * ROW);
+        if (nin == 4) {
+            for (u32 k = 0; k < 4; ++k) bulk_load(smem_addr(sb + k * P5T_TILE), P.in[k] + o, ROW, R.full(b));
+        } else if (nin == 1) {
+            bulk_load(smem_addr(sb + P5T_TILE), P.in[0] + o, ROW, R.full(b));
+        }
+        if (ndig)
+            for (u32 p = 0; p < nparts; ++p) {
+                if (p == pin) continue;
+                const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN) + tile0;
+                bulk_load(smem_addr(sb + (MACA_IN + p) * P5T_TILE), Yt, ROW, R.full(b));
+            }
+        issued = g + 1;
+    }
+    // every issued stage's copies must land before this thread leaves
+    const u32 first = issued > (u32)S ? issued - S : 0u;
+    for (u32 g = first; g < issued; ++g)
+        if (!mbar_wait(R.full(g % S), (g / S) & 1)) atomicOr(D.err, 4u);
+    if (!mbar_wait(R.kbar, 0)) atomicOr(D.err, 1u);
+}
+
 template <int LOGN>
 __global__ void __launch_bounds__(P5T_NT)
 p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
            const u32* __restrict__ plist) {
     constexpr int TILES = (1 << LOGN) / P5T_TILE;
-    constexpr u32 ROW = P5T_TILE * 8;           // bytes of one staged row
     constexpr int S = P5T_STAGES;
     extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
     const uint4 jb = jobs[blockIdx.x / TILES];
     const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
-    const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum);
-    u64* keys = sm + P5T_BAR_WORDS;
-    u64* stage = keys + 2 * dnum * P5T_TILE;
-    const u32 kbar = smem_addr(sm);
-    auto full = [&](u32 b) { return kbar + 8 * (1 + b); };
-    auto empty = [&](u32 b) { return kbar + 8 * (1 + S + b); };
-    __shared__ u32 failed;                      // a wait of an earlier CTA expired: skip the tile
-    if (threadIdx.x == 0) {
-        failed = *reinterpret_cast<volatile u32*>(D.err);
-        mbar_init(kbar, 1);
-        for (u32 b = 0; b < S; ++b) {
-            mbar_init(full(b), 1);
-            mbar_init(empty(b), P5T_NC);
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();                            // the only CTA-wide barrier
-    if (failed) return;
+    const u32 r = jb.x, slots = maca_slots((int)D.dnum);
+    P5Ring R;
+    if (!p5t_setup(D, sm, R)) return;
     const bool is_p = r >= D.fullQ;
     const u32 K = D.K;
     if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
-        if (threadIdx.x != P5T_NC) return;
-        const PairDesc& P0 = pairs[plist[jb.y]];
-        mbar_arrive_expect_tx(kbar, 2 * dnum * ROW);
-        for (u32 p = 0; p < dnum; ++p) {
-            const size_t off = (((size_t)p * D.QP + r) << LOGN) + tile0;
-            bulk_load(smem_addr(keys + (2 * p) * P5T_TILE), P0.kbv + off, ROW, kbar);
-            bulk_load(smem_addr(keys + (2 * p + 1) * P5T_TILE), P0.kav + off, ROW, kbar);
-        }
-        u32 issued = 0;
-        for (u32 g = 0; g < jb.z; ++g) {
-            const u32 b = g % S;
-            if (g >= S && !mbar_wait(empty(b), (g / S - 1) & 1)) {
-                atomicOr(D.err, 4u);
-                break;
-            }
-            const PairDesc& P = pairs[plist[jb.y + g]];
-            const u32 L = P.L, QlP = L + K;
-            const u32 i = is_p ? L + (r - D.fullQ) : r;
-            const u32 pin = is_p ? 0xffffffffu : i / D.alpha;
-            const WsLayout w = ws_layout(L, K, D.alpha);
-            const u32 nparts = D.lvl[L].nparts;
-            const u32 nin = is_p ? 0u : (P.mode == EMR ? 4u : (P.mode == KS ? 1u : 0u));
-            const u32 ndig = P.mode == HROT ? 0u : nparts - (pin < nparts ? 1u : 0u);
-            u64* sb = stage + (size_t)b * slots * P5T_TILE;
-            const size_t o = ((size_t)i << LOGN) + tile0;
-            mbar_arrive_expect_tx(full(b), (nin + ndig) * ROW);
-            if (nin == 4) {
-                for (u32 k = 0; k < 4; ++k) bulk_load(smem_addr(sb + k * P5T_TILE), P.in[k] + o, ROW, full(b));
-            } else if (nin == 1) {
-                bulk_load(smem_addr(sb + P5T_TILE), P.in[0] + o, ROW, full(b));
-            }
-            if (ndig)
-                for (u32 p = 0; p < nparts; ++p) {
-                    if (p == pin) continue;
-                    const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN) + tile0;
-                    bulk_load(smem_addr(sb + (MACA_IN + p) * P5T_TILE), Yt, ROW, full(b));
-                }
-            issued = g + 1;
-        }
-        // every issued stage's copies must land before this thread leaves
-        const u32 first = issued > (u32)S ? issued - S : 0u;
-        for (u32 g = first; g < issued; ++g)
-            if (!mbar_wait(full(g % S), (g / S) & 1)) atomicOr(D.err, 4u);
-        if (!mbar_wait(kbar, 0)) atomicOr(D.err, 1u);
+        if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
         return;
     }
     const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
     const ModC m = D.mod[r];
-    if (!mbar_wait(kbar, 0)) {
+    if (!mbar_wait(R.kbar, 0)) {
         atomicOr(D.err, 1u);
         return;
     }
     for (u32 g = 0; g < jb.z; ++g) {
         const u32 b = g % S;
-        if (!mbar_wait(full(b), (g / S) & 1)) {
+        if (!mbar_wait(R.full(b), (g / S) & 1)) {
             atomicOr(D.err, 2u);
             return;
         }
@@ -1200,7 +1229,7 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
         const u32 nparts = lv.nparts;
         const u32 pin = is_p ? 0xffffffffu : i / D.alpha;
         const bool emr = P.mode == EMR;
-        const u64* sb = stage + (size_t)b * slots * P5T_TILE + e;
+        const u64* sb = R.stage + (size_t)b * slots * P5T_TILE + e;
         ulonglong2 s{0, 0}, t0{0, 0}, t1{0, 0};
         if (!is_p) {
             if (emr) {
@@ -1244,14 +1273,14 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
             } else {
                 dv = ld2(sb + (MACA_IN + p) * P5T_TILE);
             }
-            const ulonglong2 kbv = ld2(keys + (2 * p) * P5T_TILE + e);
-            const ulonglong2 kav = ld2(keys + (2 * p + 1) * P5T_TILE + e);
+            const ulonglong2 kbv = ld2(R.keys + (2 * p) * P5T_TILE + e);
+            const ulonglong2 kav = ld2(R.keys + (2 * p + 1) * P5T_TILE + e);
             mac_wide(a0l[0], a0h[0], dv.x, kbv.x);
             mac_wide(a0l[1], a0h[1], dv.y, kbv.y);
             mac_wide(a1l[0], a1h[0], dv.x, kav.x);
             mac_wide(a1l[1], a1h[1], dv.y, kav.y);
         }
-        mbar_arrive(empty(b));                  // every word of stage b is in registers
+        mbar_arrive(R.empty(b));                  // every word of stage b is in registers
         const u32 use_redc = D.mont && (is_p || emr);
         ulonglong2 r0, r1;
 #pragma unroll
@@ -1283,6 +1312,158 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
                 const u64 ub = csub(v2get(t1, j) + v2get(r1, j), q);
                 v2set(o0, j, drop ? ua : shoup(ua, s1, s1p, q));
                 v2set(o1, j, drop ? ub : shoup(ub, s1, s1p, q));
+            }
+        }
+        *reinterpret_cast<ulonglong2*>(d0 + tile0 + e) = o0;
+        *reinterpret_cast<ulonglong2*>(d1 + tile0 + e) = o1;
+    }
+}
+
+// P5 on the FP64 pipe, TMA form: p5_mac_tma's ring (the same producer,
+// bounded waits and error codes) with p5_mac_fp's arithmetic in the
+// consumers, for the key rows of Q towers with q < 2^50. The key tile lands
+// as stored words; each consumer turns its own two words of every key row
+// into signed doubles in place (a Montgomery reduction first for the own
+// digit's key under DevCtx mont), so no barrier is needed. The bounds are
+// p5_mac_fp's: products |r| <= 0.75 q, the sums normalised after every
+// eighth digit, every value an exact integer below 2^53. Results equal
+// p5_mac's word for word.
+template <int LOGN>
+__global__ void __launch_bounds__(P5T_NT, 3)
+p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
+              const u32* __restrict__ plist) {
+    constexpr int TILES = (1 << LOGN) / P5T_TILE;
+    constexpr int S = P5T_STAGES;
+    extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
+    const uint4 jb = jobs[blockIdx.x / TILES];
+    const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
+    const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum);   // a Q row, q < 2^50
+    P5Ring R;
+    if (!p5t_setup(D, sm, R)) return;
+    if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
+        if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
+        return;
+    }
+    const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
+    const u32 K = D.K, pin = r / D.alpha;       // digit holding tower r
+    const ModC m = D.mod[r];
+    const double qd = ntt::u2d(m.q), hq = ntt::u2d(m.q >> 1);
+    const ntt::FpArS ar{qd, qinv_of(m)};
+    auto sgn = [&](u64 x) {                     // canonical -> signed double in (-q/2, q/2]
+        const double d = ntt::u2d(x);
+        return d > hq ? __dsub_rn(d, qd) : d;
+    };
+    auto canon = [&](double z) { return ar.out(ar.norm(z)); };   // |z| < 2^52 -> [0, q)
+    if (!mbar_wait(R.kbar, 0)) {
+        atomicOr(D.err, 1u);
+        return;
+    }
+    for (u32 p = 0; p < 2 * dnum; ++p) {        // own words of key row p / 2 (b, then a) -> doubles
+        u64* kw = R.keys + p * P5T_TILE + e;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            u64 k = kw[j];
+            if (D.mont && p / 2 == pin) k = redc(k, 0, m);
+            kw[j] = (u64)__double_as_longlong(sgn(k));
+        }
+    }
+    const double* kd = reinterpret_cast<const double*>(R.keys);
+    for (u32 g = 0; g < jb.z; ++g) {
+        const u32 b = g % S;
+        if (!mbar_wait(R.full(b), (g / S) & 1)) {
+            atomicOr(D.err, 2u);
+            return;
+        }
+        const PairDesc& P = pairs[plist[jb.y + g]];
+        const u32 L = P.L, QlP = L + K;
+        const u32 i = r;                        // QlP position of a Q row
+        const Level& lv = D.lvl[L];
+        const WsLayout w = ws_layout(L, K, D.alpha);
+        const u32 nparts = lv.nparts;
+        const bool emr = P.mode == EMR;
+        const u64* sb = R.stage + (size_t)b * slots * P5T_TILE + e;
+        double s[2], t0[2] = {0.0, 0.0}, t1[2] = {0.0, 0.0};
+        if (emr) {
+            const ulonglong2 x0 = ld2(sb), x1 = ld2(sb + P5T_TILE);
+            const ulonglong2 y0 = ld2(sb + 2 * P5T_TILE), y1 = ld2(sb + 3 * P5T_TILE);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const double a0 = ntt::u2d(v2get(x0, j)), a1 = ntt::u2d(v2get(x1, j));
+                const double b0 = sgn(v2get(y0, j)), b1 = sgn(v2get(y1, j));
+                s[j] = ar.mulq<false>(a1, b1);
+                t0[j] = ar.mulq<false>(a0, b0);
+                t1[j] = __dadd_rn(ar.mulq<false>(a0, b1), ar.mulq<false>(a1, b0));
+            }
+        } else if (P.mode == ROT || P.mode == HROT) {
+            const u64* src = P.in[1] + ((size_t)i << LOGN);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) s[j] = ntt::u2d(src[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
+        } else {
+            const ulonglong2 x = ld2(sb + P5T_TILE);
+            s[0] = ntt::u2d(x.x);
+            s[1] = ntt::u2d(x.y);
+        }
+        double acc_b[2] = {0.0, 0.0}, acc_a[2] = {0.0, 0.0};
+        for (u32 p = 0; p < nparts; ++p) {
+            double y[2];
+            if (p == pin) {
+                y[0] = s[0];
+                y[1] = s[1];
+            } else if (P.mode == HROT) {        // sigma_k of the shared digit: eval-slot gather
+                const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) y[j] = ntt::u2d(Yt[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
+            } else {
+                const ulonglong2 dv = ld2(sb + (MACA_IN + p) * P5T_TILE);
+                y[0] = ntt::u2d(dv.x);
+                y[1] = ntt::u2d(dv.y);
+            }
+            const double2 kbv = *reinterpret_cast<const double2*>(kd + (2 * p) * P5T_TILE + e);
+            const double2 kav = *reinterpret_cast<const double2*>(kd + (2 * p + 1) * P5T_TILE + e);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                acc_b[j] = __dadd_rn(acc_b[j], ar.mulq<false>(y[j], j ? kbv.y : kbv.x));
+                acc_a[j] = __dadd_rn(acc_a[j], ar.mulq<false>(y[j], j ? kav.y : kav.x));
+            }
+            if ((p & 7u) == 7u) {               // after every eighth digit: keep |acc| below 2^53
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    acc_b[j] = ar.norm(acc_b[j]);
+                    acc_a[j] = ar.norm(acc_a[j]);
+                }
+            }
+        }
+        mbar_arrive(R.empty(b));                // every word of stage b is in registers
+        ulonglong2 o0, o1;
+        u64 *d0, *d1;
+        if (!emr) {   // keyswitch / rotation: W = res * P^-1
+            d0 = slot_ptr(P, w.W + i, LOGN);
+            d1 = slot_ptr(P, w.W + L + i, LOGN);
+            o0 = make_ulonglong2(canon(acc_b[0]), canon(acc_b[1]));
+            o1 = make_ulonglong2(canon(acc_a[0]), canon(acc_a[1]));
+        } else {
+            const bool drop = i == L - 1;
+            const double s1 = sgn(lv.s1[i]);
+            d0 = drop ? slot_ptr(P, w.U, LOGN) : slot_ptr(P, w.W + i, LOGN);
+            d1 = drop ? slot_ptr(P, w.U + 1, LOGN) : slot_ptr(P, w.W + L + i, LOGN);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const double ua = __dadd_rn(t0[j], ar.norm(acc_b[j]));
+                const double ub = __dadd_rn(t1[j], ar.norm(acc_a[j]));
+                u64 wa, wb;
+                if (drop) {   // U: the integer form's scale, (t + res') * R^-1 with mont
+                    wa = canon(ua);
+                    wb = canon(ub);
+                    if (D.mont) {
+                        wa = redc(wa, 0, m);
+                        wb = redc(wb, 0, m);
+                    }
+                } else {
+                    wa = canon(ar.mulq<true>(ua, s1));
+                    wb = canon(ar.mulq<true>(ub, s1));
+                }
+                v2set(o0, j, wa);
+                v2set(o1, j, wb);
             }
         }
         *reinterpret_cast<ulonglong2*>(d0 + tile0 + e) = o0;

@@ -39,7 +39,7 @@ struct Plan {
     // launch schedule (chosen by tune() or the context's tuning cache)
     int p5_form = 0;                   // P5_REG128, P5_ASYNC or P5_REG256
     bool p5_fp = false;                // P5 key rows of 50-bit Q towers on the FP64 pipe (p5_mac_fp)
-    int p5_fp_form = 0;                // 0: 4 digits in flight, 4 CTAs per SM; 1: 2 digits, 5 CTAs
+    int p5_fp_form = 0;                // 0: 4 digits in flight, 4 CTAs per SM; 1: 2 digits, 5 CTAs; 2: TMA ring
     bool p5_split = false;             // FP64 and integer P5 rows on two streams at once (fork / join)
     // the second stream and its fork / join events, made on first use
     mutable cudaStream_t side = nullptr;
@@ -47,6 +47,12 @@ struct Plan {
     unsigned mix = 0x1ff;              // bit k: phase k+1 as one launch over its interleaved job list
     int p3_form = 0;                   // 0 plain P3; 1, 2 warp-specialised (128 x 2 CTAs, 256 x 1 CTA)
     bool tuned = false;
+    // The plan's launches share the GPU with other streams' steps (the
+    // server's rings run side by side): the autotuner, which times each
+    // candidate alone, then leaves out the TMA form of the FP64 P5 rows,
+    // whose ring holds about 197 KB of shared memory per SM and keeps the
+    // other streams' kernels off those SMs.
+    bool concurrent = false;
     const gfx::Context* ctx = nullptr;
     std::vector<uint64_t> key_pins;    // keys this plan holds resident (Context::acquire)
     void* d_blob = nullptr;            // device tables (pairs, jobs, P5 groups, pair lists)

@@ -119,7 +119,10 @@ Server::Server(const std::vector<gfx::Context*>& ctxs, size_t budget_bytes, uint
     st_.arena_bytes = arena_->capacity();
     streams_.resize(ctxs_.size());
     for (auto& s : streams_) ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
-    for (size_t i = 0; i < 2 * ctxs_.size(); ++i) plans_.push_back(std::make_unique<pl::Plan>());
+    for (size_t i = 0; i < 2 * ctxs_.size(); ++i) {
+        plans_.push_back(std::make_unique<pl::Plan>());
+        plans_.back()->concurrent = true;   // the rings' steps run side by side on their streams
+    }
     ck(cudaEventCreate(&epoch_ev_), "cudaEventCreate");
     epoch_ = std::chrono::steady_clock::now();
     for (auto* c : ctxs_) c->hold();       // the contexts outlive the server

@@ -327,11 +327,12 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
  * FP64 form's occupancy (0: four digits' loads in flight, four CTAs per SM;
  * 1: two digits, five CTAs), bit 17 = those FP64 rows on a second stream
  * beside the integer rows (forked and joined inside the launch, graph-
- * capturable), bits 8-16 = the
+ * capturable), bit 18 = those FP64 rows through the bulk-copy (TMA) stage
+ * ring of form 3 instead (overrides bit 7), bits 8-16 = the
  * phases (bit 8 + k for phase k+1) launched interleaved (the others as two
  * launches). */
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan);
-/* Fixes the schedule (bits 0-4, 6-7 and 8-17 as above; bit 2 sets every phase
+/* Fixes the schedule (bits 0-4, 6-7 and 8-18 as above; bit 2 sets every phase
  * interleaved) and skips the autotuner; every schedule computes the same bits. */
 int      gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule);
 /* Host-buffer form: copies h_in[4*i+k] (host, level*n words) into op i's

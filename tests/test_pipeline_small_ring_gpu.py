@@ -19,7 +19,8 @@ def S():
     return Setup(N, 6, K=2, alpha=2, rot_ks=(5, O.galois_element(3, N)))
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 8, 16, 7, 64, 67, 71, 192, 64 | 1 << 17])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 3, 8, 16, 7, 64, 67, 71, 192, 64 | 1 << 17, 64 | 1 << 18,
+                                      64 | 1 << 17 | 1 << 18])
 def test_mixed_batch_small_ring(S, schedule):
     import gpufhe_b200 as G
     g = S.gpu_context()
@@ -107,12 +108,12 @@ def test_forms_after_a_larger_dnum():
             assert np.array_equal(got[k][0], got[0][0]) and np.array_equal(got[k][1], got[0][1]), (tw, k)
 
 
-@pytest.mark.parametrize("schedule", [64, 192, 0, 64 | 1 << 17])
+@pytest.mark.parametrize("schedule", [64, 192, 0, 64 | 1 << 17, 64 | 1 << 18])
 def test_many_digits_fp64_key_product(schedule):
     """Twelve digits (alpha = 1): the FP64 key inner product normalises its
     accumulators after every eighth digit; EvalMult+Rescale and keyswitch at
-    every digit count up to twelve equal the oracle in the FP64 forms and in
-    the integer form."""
+    every digit count up to twelve equal the oracle in the FP64 forms (the
+    TMA ring's among them) and in the integer form."""
     import gpufhe_b200 as G
     S = Setup(N, 12, K=2, alpha=1, seed=33)
     g = S.gpu_context()
