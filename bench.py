@@ -999,9 +999,12 @@ def run_gpu(args):
 
     stream = torch.cuda.Stream(device=dev)
     graph = torch.cuda.CUDAGraph()
+    if args.schedule is not None:     # a fixed schedule (profiling: the one the autotuner picks unprofiled)
+        plan.set_schedule(args.schedule)
     plan.launch(stream.cuda_stream)   # first launch outside capture: kernel attributes, autotuner
     torch.cuda.synchronize()
     schedule = plan.schedule()
+    schedule["bits"] = hex(int(G.lib().gpufhe_plan_schedule(plan.h)))
     kernels_per_step = plan.kernel_count()
     with torch.cuda.graph(graph, stream=stream):
         plan.launch(torch.cuda.current_stream().cuda_stream)
@@ -1262,6 +1265,9 @@ def main():
                     help="ntt / rot / convert: only the transform isolation, the rotation batch or the basis-"
                          "conversion isolation (prints its own line)")
     ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--schedule", type=lambda x: int(x, 0), default=None,
+                    help="fix the step's launch schedule (gpufhe_plan_schedule bits) instead of autotuning it; "
+                         "for profiling runs, whose serialised launches mislead the autotuner")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -1191,24 +1191,15 @@ __device__ __forceinline__ void p5t_produce(const DevCtx& D, const PairDesc* __r
     if (!mbar_wait(R.kbar, 0)) atomicOr(D.err, 1u);
 }
 
+// Consumer of the TMA forms for an integer key row (a P row, or a Q row of
+// any width): p5_mac's arithmetic on one 16-byte pair of the tile per thread.
 template <int LOGN>
-__global__ void __launch_bounds__(P5T_NT)
-p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
-           const u32* __restrict__ plist) {
-    constexpr int TILES = (1 << LOGN) / P5T_TILE;
+__device__ __forceinline__ void p5t_consume_int(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
+                                                const u32* __restrict__ plist, const u32 tile0, const P5Ring& R) {
     constexpr int S = P5T_STAGES;
-    extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
-    const uint4 jb = jobs[blockIdx.x / TILES];
-    const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
     const u32 r = jb.x, slots = maca_slots((int)D.dnum);
-    P5Ring R;
-    if (!p5t_setup(D, sm, R)) return;
     const bool is_p = r >= D.fullQ;
     const u32 K = D.K;
-    if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
-        if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
-        return;
-    }
     const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
     const ModC m = D.mod[r];
     if (!mbar_wait(R.kbar, 0)) {
@@ -1319,7 +1310,25 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
     }
 }
 
-// P5 on the FP64 pipe, TMA form: p5_mac_tma's ring (the same producer,
+template <int LOGN>
+__global__ void __launch_bounds__(P5T_NT)
+p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
+           const u32* __restrict__ plist) {
+    constexpr int TILES = (1 << LOGN) / P5T_TILE;
+    extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
+    const uint4 jb = jobs[blockIdx.x / TILES];
+    const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
+    P5Ring R;
+    if (!p5t_setup(D, sm, R)) return;
+    if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
+        if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
+        return;
+    }
+    p5t_consume_int<LOGN>(D, pairs, jb, plist, tile0, R);
+}
+
+// Consumer of the TMA forms for an FP64 key row (P5 on the FP64 pipe, TMA
+// form, the kernel below): p5_mac_tma's ring (the same producer,
 // bounded waits and error codes) with p5_mac_fp's arithmetic in the
 // consumers, for the key rows of Q towers with q < 2^50. The key tile lands
 // as stored words; each consumer turns its own two words of every key row
@@ -1329,21 +1338,10 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
 // eighth digit, every value an exact integer below 2^53. Results equal
 // p5_mac's word for word.
 template <int LOGN>
-__global__ void __launch_bounds__(P5T_NT, 3)
-p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
-              const u32* __restrict__ plist) {
-    constexpr int TILES = (1 << LOGN) / P5T_TILE;
+__device__ __forceinline__ void p5t_consume_fp(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
+                                               const u32* __restrict__ plist, const u32 tile0, const P5Ring& R) {
     constexpr int S = P5T_STAGES;
-    extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
-    const uint4 jb = jobs[blockIdx.x / TILES];
-    const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
     const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum);   // a Q row, q < 2^50
-    P5Ring R;
-    if (!p5t_setup(D, sm, R)) return;
-    if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
-        if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
-        return;
-    }
     const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
     const u32 K = D.K, pin = r / D.alpha;       // digit holding tower r
     const ModC m = D.mod[r];
@@ -1469,6 +1467,23 @@ p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* _
         *reinterpret_cast<ulonglong2*>(d0 + tile0 + e) = o0;
         *reinterpret_cast<ulonglong2*>(d1 + tile0 + e) = o1;
     }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(P5T_NT, 3)
+p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
+              const u32* __restrict__ plist) {
+    constexpr int TILES = (1 << LOGN) / P5T_TILE;
+    extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
+    const uint4 jb = jobs[blockIdx.x / TILES];
+    const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
+    P5Ring R;
+    if (!p5t_setup(D, sm, R)) return;
+    if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
+        if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
+        return;
+    }
+    p5t_consume_fp<LOGN>(D, pairs, jb, plist, tile0, R);
 }
 
 // ------------------------------------------------------------------ P6
