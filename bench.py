@@ -101,12 +101,14 @@ def p5_algorithmic_bytes(levels, n):
 
 
 # DRAM traffic per algorithmic byte, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum) of the 16-pair case of this workload: P5 moved 773.2 MB
-# against its 827.3 MB of algorithmic bytes, the whole step 2571 MB against
-# 489.7 MB. Both are scaled to the bench's launch by its algorithmic bytes and
-# reported with that label; they are not measured in this run.
-P5_TRAFFIC_PER_ALG = 0.935
-STEP_TRAFFIC_PER_ALG = 5.25
+# dram__bytes_write.sum) of the 16-pair case of this workload under the
+# 128-pair step's tuned schedule: P5 (its FP64 TMA-ring and integer kernels)
+# moved 756.3 MB against its 827.3 MB of algorithmic bytes, the whole step
+# 2559 MB against 489.7 MB. Both are scaled to the bench's launch by its
+# algorithmic bytes and reported with that label; they are not measured in
+# this run.
+P5_TRAFFIC_PER_ALG = 0.914
+STEP_TRAFFIC_PER_ALG = 5.23
 TRAFFIC_SOURCE = "ncu DRAM bytes of the 16-pair case of this workload, scaled to this launch by algorithmic bytes"
 
 
@@ -1205,8 +1207,9 @@ def run_gpu(args):
                    "mean_level": float(np.mean(levels)), "l2": "inputs larger than L2 (no flush)",
                    "graph": f"{kernels_per_step} kernels per step, one CUDA graph",
                    "schedule": schedule},
-        "roofline": {"bound": "hbm", "kernel": "p5_mac (keyswitch inner product + EvalMult/Rescale epilogue), "
-                                               "the step's largest kernel",
+        "roofline": {"bound": "hbm", "kernel": "P5: key-switch inner product + EvalMult/Rescale epilogue "
+                                               "(p5_mac_fp_tma for the 50-bit Q rows and p5_mac for the others "
+                                               "under the tuned schedule), the step's largest phase by bytes",
                      "achieved": p5_alg / (phases[4] * 1e-3) / 1e9, "peak": pk["hbm_gbs"],
                      "peak_source": pk["source"] + " (burst copy)", "unit": "GB/s",
                      "frac": p5_alg / (phases[4] * 1e-3) / 1e9 / pk["hbm_gbs"],
@@ -1218,7 +1221,7 @@ def run_gpu(args):
                           "algorithmic_bytes_per_launch": alg,
                           "traffic": STEP_TRAFFIC_PER_ALG * alg, "traffic_source": TRAFFIC_SOURCE,
                           "note": "the step's intermediates (ModUp digits, ModDown inputs) cross HBM between phases "
-                                  "(traffic 5.25x the algorithmic bytes), yet DRAM stays about a third busy: the "
+                                  "(traffic 5.23x the algorithmic bytes), yet DRAM stays about a third busy: the "
                                   "step is bound by integer / FP64 issue in the transforms and the key inner "
                                   "product, not by HBM"},
         "phases_ms": {f"P{k + 1}": p for k, p in enumerate(phases)},
