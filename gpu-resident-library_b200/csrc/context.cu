@@ -70,6 +70,8 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
         ninv[i] = hm::invmod(n, q);
         ninvp[i] = hm::precon(ninv[i], q);
     }
+    ninv_h_ = ninv;
+    ninvp_h_ = ninvp;
 
     // Montgomery form of the keys when the key-switch sums stay below q * 2^64 (Key)
     {

@@ -92,6 +92,9 @@ public:
     const std::vector<u64>& Q() const { return Q_; }
     const std::vector<u64>& P() const { return P_; }
     const std::vector<u64>& roots() const { return roots_; }
+    // n^-1 mod each QP modulus and its Shoup precomputation (host copies)
+    const std::vector<u64>& ninv_host() const { return ninv_h_; }
+    const std::vector<u64>& ninvp_host() const { return ninvp_h_; }
     const Level& level_host(uint32_t L) const { return lv_host_[L]; }
     int device() const { return device_; }
 
@@ -139,6 +142,7 @@ private:
     uint32_t n_, logn_, alpha_, dnum_;
     int device_;
     std::vector<u64> Q_, P_, roots_;
+    std::vector<u64> ninv_h_, ninvp_h_;
     std::vector<Level> lv_host_;
     u64* d_key_scale_ = nullptr;                 // [2][dnum * QP] row scale and Shoup precon (Key)
     DevCtx dc_{};

@@ -271,36 +271,6 @@ __global__ void k_gather_tower0(const u64* const* __restrict__ in, u64* __restri
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) dst[k] = src[k];
 }
 
-// ModRaise, third step: out[p][t][k] = centre(x[p][k]) mod q_t, where
-// centre(v) = v - q0 for v > q0 / 2 (the reference's decrypt_host centring,
-// src/encdec.cpp:79) and the embedding is ((v % q) + q) % q
-// (src/rotate.cpp:108-110). blockIdx.y = component, blockIdx.z = tower.
-__global__ void k_raise(const u64* __restrict__ x, u64* const* __restrict__ out, const ModC* __restrict__ mod,
-                        uint32_t n) {
-    const uint32_t p = blockIdx.y, t = blockIdx.z;
-    const u64 q0 = mod[0].q;
-    const ModC m = mod[t];
-    const u64* src = x + (size_t)p * n;
-    u64* dst = out[p] + (size_t)t * n;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const u64 v = src[k];
-        const long long c = v > q0 / 2 ? (long long)v - (long long)q0 : (long long)v;
-        dst[k] = emb(c, m);
-    }
-}
-
-// out[p][t][k] = m[p][k] mod q_t (blockIdx.y = message, blockIdx.z = tower),
-// the reference's plaintext embedding ((v % q) + q) % q (src/rotate.cpp:108-110).
-__global__ void k_embed_ptrs(const int64_t* __restrict__ m, u64* const* __restrict__ out,
-                             const ModC* __restrict__ mod, uint32_t n) {
-    const uint32_t p = blockIdx.y, t = blockIdx.z;
-    const ModC md = mod[t];
-    const int64_t* src = m + (size_t)p * n;
-    u64* dst = out[p] + (size_t)t * n;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-        dst[k] = emb(src[k], md);
-}
-
 struct Scratch {
     cudaStream_t s;
     std::vector<void*> ptrs;
@@ -331,8 +301,8 @@ xf::Job xjob(const Context& c, const std::vector<u64>& qp, u64* x, uint32_t qi, 
     j.x = x;
     j.tw = (inverse ? D.twi : D.twf) + (size_t)qi * n;
     j.q = qp[qi];
-    j.scale = hm::invmod(n, j.q);
-    j.scale_p = hm::precon(j.scale, j.q);
+    j.scale = c.ninv_host()[qi];   // n^-1 (inverse transforms), kept by the context
+    j.scale_p = c.ninvp_host()[qi];
     j.fp = fp_tower(j.q) ? 1u : 0u;
     j.twd = j.fp ? (inverse ? D.twid : D.twfd) + (size_t)qi * n : nullptr;
     return j;
@@ -609,15 +579,18 @@ int gpufhe_pt_to_eval_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, cons
         for (u64* o : out)
             if (!o) throw std::invalid_argument("pt_to_eval: null output pointer");
         Scratch S(stream);
-        u64* const* dout = upload(S, out);
-        k_embed_ptrs<<<dim3((n + KNT - 1) / KNT, count, towers), KNT, 0, stream>>>(d_m, dout, c->dev().mod, n);
-        ck(cudaGetLastError(), "pt_to_eval embed");
+        // each tower's forward transform reads the message and embeds it on load
         std::vector<xf::Job> jobs((size_t)count * towers);
         for (uint32_t p = 0; p < count; ++p)
-            for (uint32_t t = 0; t < towers; ++t)
-                jobs[(size_t)p * towers + t] = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
+            for (uint32_t t = 0; t < towers; ++t) {
+                xf::Job& j = jobs[(size_t)p * towers + t];
+                j = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
+                j.lift = reinterpret_cast<const u64*>(d_m) + (size_t)p * n;
+                j.lift_q0 = 0;                 // signed 64-bit coefficients
+                j.lift_r64 = ~0ull / qp[t];
+            }
         xf::Job* dj = upload(S, jobs);
-        ck(xf_launch_ntt(dj, nullptr, (int)jobs.size(), (int)c->logn(), false, stream), "pt_to_eval transform");
+        ck(xf_launch_ntt_lift(dj, (int)jobs.size(), (int)c->logn(), stream), "pt_to_eval transform");
         return GPUFHE_OK;
     })
 }
@@ -646,19 +619,23 @@ int gpufhe_modraise_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, const 
         Scratch S(stream);
         u64* x = S.get<u64>((size_t)comps * n);
         const u64* const* din = upload(S, in);
-        u64* const* dout = upload(S, out);
         const unsigned gx = (n + KNT - 1) / KNT;
         k_gather_tower0<<<dim3(gx, comps), KNT, 0, stream>>>(din, x, n);
         ck(cudaGetLastError(), "modraise gather");
         transform(*c, qp, S, x, comps, 1, true);                        // tower 0 -> coefficients
-        k_raise<<<dim3(gx, comps, towers), KNT, 0, stream>>>(x, dout, c->dev().mod, n);
-        ck(cudaGetLastError(), "modraise embed");
-        std::vector<xf::Job> jobs((size_t)comps * towers);           // every tower -> eval form
+        // every tower -> eval form, its column pass lifting tower 0 (centred
+        // mod q0) into the tower's modulus on load
+        std::vector<xf::Job> jobs((size_t)comps * towers);
         for (uint32_t p = 0; p < comps; ++p)
-            for (uint32_t t = 0; t < towers; ++t)
-                jobs[(size_t)p * towers + t] = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
+            for (uint32_t t = 0; t < towers; ++t) {
+                xf::Job& j = jobs[(size_t)p * towers + t];
+                j = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
+                j.lift = x + (size_t)p * n;
+                j.lift_q0 = qp[0];
+                j.lift_r64 = ~0ull / qp[t];
+            }
         xf::Job* dj = upload(S, jobs);
-        ck(xf_launch_ntt(dj, nullptr, (int)jobs.size(), (int)c->logn(), false, stream), "modraise transform");
+        ck(xf_launch_ntt_lift(dj, (int)jobs.size(), (int)c->logn(), stream), "modraise transform");
         return GPUFHE_OK;
     })
 }
