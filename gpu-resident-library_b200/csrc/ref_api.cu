@@ -443,6 +443,99 @@ void compute_keyswitch_constants(KeySwitchConstants& K, const std::vector<uint64
 }
 
 // ---------------------------------------------------------------- resident keyswitch
+namespace {
+// Root tables in the reference's split layout (psi^bitrev(i), its Shoup
+// precomputation, and the same from psi^-1), shared by every context of a
+// device for the process: DeviceKSContext publishes them and never frees them.
+struct SplitTab { u64 *fr, *fp, *ir, *ip; u64 ninv, ninvp; };
+std::mutex g_split_mu;
+std::map<std::tuple<int, uint32_t, u64, u64>, SplitTab> g_split;
+
+u64* upload_words(const std::vector<u64>& h) {
+    u64* d = nullptr;
+    ck(cudaMalloc(&d, std::max<size_t>(h.size(), 1) * 8), "ks_context_create: table");
+    if (!h.empty()) ck(cudaMemcpy(d, h.data(), h.size() * 8, cudaMemcpyHostToDevice), "ks_context_create: upload");
+    return d;
+}
+
+SplitTab split_tables_for(uint32_t n, u64 q, u64 root) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(g_split_mu);
+    const auto key = std::make_tuple(dev, n, q, root);
+    auto it = g_split.find(key);
+    if (it != g_split.end()) return it->second;
+    std::vector<Tw> f, iv;
+    hm::twiddles(n, q, root, f, iv);
+    std::vector<u64> a(n), b(n), c(n), d(n);
+    for (uint32_t i = 0; i < n; ++i) { a[i] = f[i].w; b[i] = f[i].wp; c[i] = iv[i].w; d[i] = iv[i].wp; }
+    const u64 ni = hm::invmod(n, q);
+    const SplitTab t{upload_words(a), upload_words(b), upload_words(c), upload_words(d), ni, hm::precon(ni, q)};
+    g_split.emplace(key, t);
+    return t;
+}
+
+// The reference's public tables of a context (its ks_context_create,
+// src/keyswitch_resident.cpp:32-107): the same values under the same names.
+void publish_tables(DeviceKSContext& C, const KeySwitchConstants& K) {
+    auto root_of = [&](u64 q) {
+        for (size_t r = 0; r < K.rootModList.size(); ++r) if (K.rootModList[r] == q) return K.rootValList[r];
+        throw std::runtime_error("no root table for modulus");
+    };
+    for (u64 q : C.modList) {
+        const SplitTab t = split_tables_for(C.n, q, root_of(q));
+        C.d_fr.push_back(t.fr); C.d_fp.push_back(t.fp); C.d_ir.push_back(t.ir); C.d_ip.push_back(t.ip);
+        C.ninv.push_back(t.ninv); C.ninv_p.push_back(t.ninvp);
+    }
+    for (uint32_t p = 0; p < K.numPart; ++p) {
+        C.complModHost.push_back(K.partComplMod[p]);
+        C.d_qhi.push_back(upload_words(K.partQHatInv[p]));
+        C.d_qhip.push_back(upload_words(K.partQHatInvPrec[p]));
+        C.d_srcMod.push_back(upload_words(K.partSrcMod[p]));
+        C.d_qmp.push_back(upload_words(K.partQHatModp[p]));
+        C.d_complMod.push_back(upload_words(K.partComplMod[p]));
+        C.d_mlo.push_back(upload_words(K.partBMuLo[p]));
+        C.d_mhi.push_back(upload_words(K.partBMuHi[p]));
+        if (p < K.av.size() && p < K.bv.size()) {
+            C.d_av.push_back(upload_words(K.av[p]));
+            C.d_bv.push_back(upload_words(K.bv[p]));
+        }
+    }
+    C.d_pHatInv = upload_words(K.pHatInv);
+    C.d_pHatInvPrec = upload_words(K.pHatInvPrec);
+    C.d_pMod = upload_words(K.pMod);
+    C.d_pHatModq = upload_words(K.pHatModq);
+    C.d_qMod = upload_words(K.qMod);
+    C.d_mdMuLo = upload_words(K.mdBMuLo);
+    C.d_mdMuHi = upload_words(K.mdBMuHi);
+    // per QlP tower: modulus, and the eval-key row (P rows sit after all fullQ rows)
+    std::vector<u64> mq(C.sizeQlP);
+    std::vector<uint32_t> kr(C.sizeQlP);
+    for (uint32_t i = 0; i < C.sizeQlP; ++i) {
+        mq[i] = i < C.sizeQl ? K.qMod[i] : K.pMod[i - C.sizeQl];
+        kr[i] = i < C.sizeQl ? i : i + (C.fullQ - C.sizeQl);
+    }
+    C.d_modsQlP = upload_words(mq);
+    ck(cudaMalloc(&C.d_keyRow, std::max<size_t>(kr.size(), 1) * 4), "ks_context_create: key rows");
+    ck(cudaMemcpy(C.d_keyRow, kr.data(), kr.size() * 4, cudaMemcpyHostToDevice), "ks_context_create: key rows");
+}
+
+void free_published(DeviceKSContext& C) {
+    for (auto* v : {&C.d_qhi, &C.d_qhip, &C.d_srcMod, &C.d_qmp, &C.d_complMod, &C.d_mlo, &C.d_mhi, &C.d_av, &C.d_bv}) {
+        for (u64* p : *v) cudaFree(p);
+        v->clear();
+    }
+    for (u64** p : {&C.d_pHatInv, &C.d_pHatInvPrec, &C.d_pMod, &C.d_pHatModq, &C.d_qMod, &C.d_mdMuLo, &C.d_mdMuHi,
+                    &C.d_modsQlP}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (C.d_keyRow) cudaFree(C.d_keyRow);
+    C.d_keyRow = nullptr;
+    C.d_fr.clear(); C.d_fp.clear(); C.d_ir.clear(); C.d_ip.clear();   // shared root tables stay
+}
+}  // namespace
+
 DeviceKSContext ks_context_create(const KeySwitchConstants& K) {
     DeviceKSContext C;
     C.n = K.n; C.sizeQl = K.sizeQl; C.sizeP = K.sizeP; C.sizeQlP = K.sizeQl + K.sizeP;
@@ -479,10 +572,18 @@ DeviceKSContext ks_context_create(const KeySwitchConstants& K) {
             }
         ctx->set_key(0, av.data(), bv.data());
     }
+    try {
+        publish_tables(C, K);
+    } catch (...) {
+        free_published(C);
+        gfx::Context::retire(ctx);
+        throw;
+    }
     return C;
 }
 
 void ks_context_destroy(DeviceKSContext& C) {
+    free_published(C);
     gfx::Context::retire(static_cast<gfx::Context*>(C.impl));
     C.impl = nullptr;
 }
@@ -494,6 +595,18 @@ DeviceKSWork ks_work_create(const DeviceKSContext& C) {
     const uint32_t L = C.sizeQl;
     const size_t words = pl::op_workspace_words(*ctx, L);
     ck(cudaMalloc(&W.d_ws, words * 8), "ks_work_create: workspace");
+    // the reference's scratch buffers, at its sizes (keyswitch_resident.cpp:109-120)
+    const size_t n = C.n;
+    uint32_t max_part = 0;
+    for (uint32_t sp : C.sizePart) max_part = std::max(max_part, sp);
+    ck(cudaMalloc(&W.d_part, std::max<size_t>(max_part, 1) * n * 8), "ks_work_create: scratch");
+    ck(cudaMalloc(&W.d_compl, (size_t)C.sizeQlP * n * 8), "ks_work_create: scratch");
+    ck(cudaMalloc(&W.d_res0, (size_t)C.sizeQlP * n * 8), "ks_work_create: scratch");
+    ck(cudaMalloc(&W.d_res1, (size_t)C.sizeQlP * n * 8), "ks_work_create: scratch");
+    ck(cudaMalloc(&W.d_pwork, std::max<size_t>(C.sizeP, 1) * n * 8), "ks_work_create: scratch");
+    ck(cudaMalloc(&W.d_qsw, (size_t)C.sizeQl * n * 8), "ks_work_create: scratch");
+    ck(cudaMalloc(reinterpret_cast<void**>(&W.d_digPtrs), std::max<size_t>(C.sizeQlP, 1) * sizeof(uint64_t*)),
+       "ks_work_create: scratch");
     auto* wi = new WorkImpl();
     wi->ctx = ctx;
     if (ctx->key(0)) {
@@ -512,8 +625,12 @@ DeviceKSWork ks_work_create(const DeviceKSContext& C) {
 void ks_work_destroy(DeviceKSWork& W) {
     delete static_cast<WorkImpl*>(W.impl);
     W.impl = nullptr;
-    if (W.d_ws) cudaFree(W.d_ws);
-    W.d_ws = nullptr;
+    for (uint64_t** p : {&W.d_ws, &W.d_part, &W.d_compl, &W.d_res0, &W.d_res1, &W.d_pwork, &W.d_qsw}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (W.d_digPtrs) cudaFree(const_cast<uint64_t**>(W.d_digPtrs));
+    W.d_digPtrs = nullptr;
 }
 
 void keyswitch_resident(const uint64_t* d_a, uint64_t* d_ba0, uint64_t* d_ba1, const DeviceKSContext& C,

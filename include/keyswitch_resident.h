@@ -18,19 +18,46 @@ extern bool g_ks_batched;
 /* Shared read-only device state for one level: constants, eval key, root
  * tables (reference include/keyswitch_resident.h:11-29). Built once by
  * ks_context_create; any number of streams may use it concurrently, each
- * with its own DeviceKSWork. `impl` owns the device data. */
+ * with its own DeviceKSWork. `impl` owns the fused pipeline's context, which
+ * keyswitch_resident runs on. The public fields carry the reference's device
+ * tables under its names and layouts, for callers that compose the Launch*
+ * entry points themselves:
+ *   d_fr, d_fp, d_ir, d_ip  per modulus of modList: psi^bitrev(i) and its
+ *                           Shoup precomputation, the same from psi^-1
+ *                           (shared by every context, never freed);
+ *   ninv, ninv_p            per modulus: n^-1 and its precomputation (host);
+ *   d_qhi ... d_mhi, complModHost   per digit: the ApproxSwitchCRTBasis
+ *                           constants of KeySwitchConstants (device; host);
+ *   d_av, d_bv              per digit: the eval key rows as given (device);
+ *   d_pHatInv ... d_mdMuHi  the ModDown constants (device);
+ *   d_modsQlP, d_keyRow     per QlP tower: modulus and eval-key row. */
 struct DeviceKSContext {
     uint32_t n = 0, sizeQl = 0, sizeP = 0, sizeQlP = 0, numPart = 0, fullQ = 0;
     std::vector<uint64_t> modList;
+    std::vector<uint64_t*> d_fr, d_fp, d_ir, d_ip;
+    std::vector<uint64_t> ninv, ninv_p;
     std::vector<uint32_t> sizePart, sizeCompl, startIdx;
+    std::vector<std::vector<uint64_t>> complModHost;
+    std::vector<uint64_t*> d_qhi, d_qhip, d_srcMod, d_qmp, d_complMod, d_mlo, d_mhi;
+    std::vector<uint64_t*> d_av, d_bv;
+    uint64_t *d_pHatInv = nullptr, *d_pHatInvPrec = nullptr, *d_pMod = nullptr, *d_pHatModq = nullptr,
+             *d_qMod = nullptr, *d_mdMuLo = nullptr, *d_mdMuHi = nullptr;
     std::vector<uint64_t> pInvModqHost, qModHost, pModHost;
+    uint64_t* d_modsQlP = nullptr;
+    uint32_t* d_keyRow = nullptr;
     void* impl = nullptr;
 };
 
 /* Per-stream work buffers for one keyswitch in flight (reference
- * keyswitch_resident.h:32-39): the pipeline workspace, its job tables and a
- * device operation descriptor. */
+ * keyswitch_resident.h:32-39). keyswitch_resident uses d_ws (the pipeline
+ * workspace) and impl (its plan); the reference's scratch buffers are
+ * allocated at its sizes for callers that compose their own sequence:
+ * d_part (largest digit x n), d_compl, d_res0, d_res1 (sizeQlP x n),
+ * d_pwork (sizeP x n), d_qsw (sizeQl x n), d_digPtrs (sizeQlP pointers). */
 struct DeviceKSWork {
+    uint64_t *d_part = nullptr, *d_compl = nullptr, *d_res0 = nullptr, *d_res1 = nullptr;
+    uint64_t *d_pwork = nullptr, *d_qsw = nullptr;
+    const uint64_t** d_digPtrs = nullptr;
     uint64_t* d_ws = nullptr;
     void* impl = nullptr;
 };

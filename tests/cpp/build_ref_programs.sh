@@ -24,7 +24,8 @@ fi
 mkdir -p "$OUT"
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
 for p in test_rot_resident test_keyreuse test_chain test_stage_acc test_boot; do
-    if [ ! -f "$OUT/$p" ] || [ "$REF/tests/$p.cpp" -nt "$OUT/$p" ] || [ "$LIBDIR/libgpufhe_b200.so" -nt "$OUT/$p" ]; then
+    if [ ! -f "$OUT/$p" ] || [ "$REF/tests/$p.cpp" -nt "$OUT/$p" ] || [ "$LIBDIR/libgpufhe_b200.so" -nt "$OUT/$p" ] ||
+       [ -n "$(find "$ROOT/include" -newer "$OUT/$p" -name '*.h')" ]; then
         "$NVCC" -std=c++17 -O2 -ccbin /usr/bin/g++ -Wno-deprecated-gpu-targets -I"$ROOT/include" \
             "$REF/tests/$p.cpp" -o "$OUT/$p" -L"$LIBDIR" -lgpufhe_b200 \
             -Xlinker -rpath -Xlinker '$ORIGIN/../../../../gpu-resident-library_b200/gpufhe_b200'

@@ -22,6 +22,9 @@
 #include "keygen.h"
 #include "keyswitch.h"
 #include "keyswitch_resident.h"
+#include "basis_convert.h"
+#include "intt.h"
+#include "ntt.h"
 #include "params.h"
 #include "tensor.h"
 
@@ -134,6 +137,76 @@ int main(int argc, char** argv) {
         ok = ok && g0 == ks0 && g1 == ks1;
         gate(ok, "keyswitch_resident graph replay bit-exact vs direct");
         cudaGraphExecDestroy(ge); cudaGraphDestroy(g); cudaStreamDestroy(s);
+    }
+
+    {   // the context's public tables (the reference's names and layouts), used
+        // the way a caller composing the Launch* entry points uses them
+        bool ok = C.d_av.size() == numPart && C.d_bv.size() == numPart && C.d_qhi.size() == numPart;
+        for (uint32_t p = 0; ok && p < numPart; ++p) {   // eval key rows as given
+            std::vector<u64> av(K.av[p].size()), bv(K.bv[p].size());
+            cudaMemcpy(av.data(), C.d_av[p], av.size() * 8, cudaMemcpyDeviceToHost);
+            cudaMemcpy(bv.data(), C.d_bv[p], bv.size() * 8, cudaMemcpyDeviceToHost);
+            ok = av == K.av[p] && bv == K.bv[p];
+        }
+        gate(ok, "DeviceKSContext d_av / d_bv hold the eval key rows");
+        // NTT with d_fr / d_fp, inverse with d_ir / d_ip / ninv: a round trip
+        // on one 60-bit, one 50-bit and one P tower
+        ok = C.modList.size() == sizeQlP && C.d_fr.size() == sizeQlP && C.ninv.size() == sizeQlP;
+        u64* dx; cudaMalloc(&dx, (size_t)n * 8);
+        for (uint32_t r : {0u, 2u, sizeQ + 1}) {
+            if (!ok) break;
+            std::vector<u64> x(n), y(n);
+            std::mt19937_64 g(77 + r);
+            for (auto& v : x) v = g() % C.modList[r];
+            cudaMemcpy(dx, x.data(), (size_t)n * 8, cudaMemcpyHostToDevice);
+            LaunchNTT_CT(dx, C.d_fr[r], C.d_fp[r], n, C.modList[r], 0);
+            cudaMemcpy(y.data(), dx, (size_t)n * 8, cudaMemcpyDeviceToHost);
+            LaunchINTT_GS(dx, C.d_ir[r], C.d_ip[r], n, C.modList[r], C.ninv[r], C.ninv_p[r], 0);
+            std::vector<u64> z(n);
+            cudaMemcpy(z.data(), dx, (size_t)n * 8, cudaMemcpyDeviceToHost);
+            ok = y != x && z == x;
+        }
+        gate(ok, "DeviceKSContext d_fr / d_fp / d_ir / d_ip / ninv: NTT round trip");
+        // ApproxSwitchCRTBasis of digit 1 with d_qhi ... d_mhi against the
+        // formula on the host: y_i = x_i * QHatInv_i mod q_i, out_j = sum_i
+        // y_i * QHatModp[i][j] mod p_j
+        {
+            const uint32_t p = 1, sp = C.sizePart[p], sc = C.sizeCompl[p], st = C.startIdx[p];
+            std::vector<u64> src((size_t)sp * n), dst((size_t)sc * n);
+            std::mt19937_64 g(91);
+            for (uint32_t i = 0; i < sp; ++i)
+                for (uint32_t k = 0; k < n; ++k) src[(size_t)i * n + k] = g() % mod[st + i];
+            u64 *dsrc, *ddst;
+            cudaMalloc(&dsrc, src.size() * 8); cudaMalloc(&ddst, dst.size() * 8);
+            cudaMemcpy(dsrc, src.data(), src.size() * 8, cudaMemcpyHostToDevice);
+            LaunchApproxSwitchCRTBasis(dsrc, ddst, C.d_qhi[p], C.d_qhip[p], C.d_srcMod[p], C.d_qmp[p],
+                                       C.d_complMod[p], C.d_mlo[p], C.d_mhi[p], sp, sc, n, 0);
+            cudaMemcpy(dst.data(), ddst, dst.size() * 8, cudaMemcpyDeviceToHost);
+            bool cv = C.complModHost[p] == K.partComplMod[p];
+            for (uint32_t j = 0; cv && j < sc; ++j) {
+                const u64 pj = K.partComplMod[p][j];
+                for (uint32_t k = 0; cv && k < n; ++k) {
+                    unsigned __int128 acc = 0;
+                    for (uint32_t i = 0; i < sp; ++i) {
+                        const u64 qi = mod[st + i], y = mm(src[(size_t)i * n + k], K.partQHatInv[p][i], qi);
+                        acc += (unsigned __int128)y * K.partQHatModp[p][(size_t)i * sc + j];
+                    }
+                    cv = dst[(size_t)j * n + k] == (u64)(acc % pj);
+                }
+            }
+            gate(cv, "DeviceKSContext d_qhi ... d_mhi drive LaunchApproxSwitchCRTBasis");
+            cudaFree(dsrc); cudaFree(ddst);
+        }
+        cudaFree(dx);
+        std::vector<u64> mq(sizeQlP), md(sizeQ), pm(sizeP);
+        std::vector<uint32_t> kr(sizeQlP);
+        cudaMemcpy(mq.data(), C.d_modsQlP, sizeQlP * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(kr.data(), C.d_keyRow, sizeQlP * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(md.data(), C.d_qMod, sizeQ * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(pm.data(), C.d_pMod, sizeP * 8, cudaMemcpyDeviceToHost);
+        ok = mq == modQP && md == mod && pm == modP && W.d_res0 && W.d_res1 && W.d_part && W.d_digPtrs;
+        for (uint32_t i = 0; i < sizeQlP; ++i) ok = ok && kr[i] == i;   // full level: rows in place
+        gate(ok, "DeviceKSContext d_modsQlP / d_keyRow / d_qMod / d_pMod and DeviceKSWork scratch");
     }
 
     {   // keyswitch_core_resident (host vectors) == keyswitch_resident

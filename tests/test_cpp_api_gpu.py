@@ -19,7 +19,10 @@ LIBDIR = os.path.join(ROOT, "gpu-resident-library_b200", "gpufhe_b200")
 
 
 def _build():
-    if os.path.exists(BIN) and os.path.getmtime(BIN) >= os.path.getmtime(SRC):
+    # rebuilt when the program, a header it compiles against or the library changed
+    deps = [SRC, os.path.join(LIBDIR, "libgpufhe_b200.so")] + \
+        [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
+    if os.path.exists(BIN) and os.path.getmtime(BIN) >= max(os.path.getmtime(d) for d in deps):
         return
     os.makedirs(os.path.dirname(BIN), exist_ok=True)
     subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-O2", "-ccbin", "/usr/bin/g++",
