@@ -78,8 +78,8 @@ uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan) {
     if (!plan) return 0;
     const pl::Plan& p = *plan->p;
     return (uint32_t)p.p5_form | ((p.mix & 0x1ffu) == 0x1ffu ? 4u : 0u) | ((uint32_t)p.p3_form << 3) |
-           (p.tuned ? 32u : 0u) | (p.p5_fp ? 64u : 0u) | (p.p5_fp_form == 1 ? 128u : 0u) | ((p.mix & 0x1ffu) << 8) |
-           (p.p5_split ? (1u << 17) : 0u) | (p.p5_fp_form == 2 ? (1u << 18) : 0u);
+           (p.tuned ? 32u : 0u) | (p.p5_fp ? 64u : 0u) | ((p.p5_fp_form & 1) ? 128u : 0u) | ((p.mix & 0x1ffu) << 8) |
+           (p.p5_split ? (1u << 17) : 0u) | (p.p5_fp_form >= 2 ? (1u << 18) : 0u);
 }
 
 int gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule) {
@@ -95,8 +95,8 @@ int gpufhe_plan_set_schedule(gpufhe_plan* plan, uint32_t schedule) {
     p.p3_form = (int)((schedule >> 3) & 3);
     if (p.p3_form > 2) { gfx::set_error("bad P3 form"); return GPUFHE_EINVAL; }
     p.p5_fp = (schedule >> 6) & 1;
-    p.p5_fp_form = (schedule >> 18) & 1 ? 2 : (int)((schedule >> 7) & 1);
-    if (p.p5_fp_form == 2 && !pl::mac_tma_ok(p.dc.dnum)) p.p5_fp_form = 0;
+    p.p5_fp_form = ((schedule >> 18) & 1 ? 2 : 0) + (int)((schedule >> 7) & 1);
+    if (p.p5_fp_form >= 2 && !pl::mac_tma_ok(p.dc.dnum)) p.p5_fp_form = 0;
     p.p5_split = (schedule >> 17) & 1;
     if (p.p5_split && !pl::ensure_side(p)) {
         gfx::set_error("gpufhe_plan_set_schedule: cannot create the second P5 stream");

@@ -84,7 +84,8 @@ struct Launcher {
         cudaFuncSetAttribute(p5_mac_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
         cudaFuncSetAttribute(p5_mac_fp<LOGN, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
         cudaFuncSetAttribute(p5_mac_fp<LOGN, 2, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, mac_smem(MAC_MAX_DNUM));
-        cudaFuncSetAttribute(p5_mac_fp_tma<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
+        cudaFuncSetAttribute(p5_mac_fp_tma<LOGN, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
+        cudaFuncSetAttribute(p5_mac_fp_tma<LOGN, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, MAC_TMA_SMEM_MAX);
     }
     // persistent warp-specialised P3 over job segment PATH: form 1 = 128
     // conversion threads, two CTAs per SM; form 2 = 256, one CTA per SM
@@ -151,7 +152,10 @@ struct Launcher {
                     sf = p.side;
                 }
                 if (nfp && p.p5_fp_form == 2 && mac_tma_ok(D.dnum))
-                    p5_mac_fp_tma<LOGN><<<nfp * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum), sf>>>(
+                    p5_mac_fp_tma<LOGN, 3><<<nfp * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum, 3), sf>>>(
+                        D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
+                else if (nfp && p.p5_fp_form == 3 && mac_tma_ok(D.dnum))
+                    p5_mac_fp_tma<LOGN, 2><<<nfp * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum, 2), sf>>>(
                         D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
                 else if (nfp && p.p5_fp_form == 1)
                     p5_mac_fp<LOGN, 2, 5><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), sf>>>(
@@ -570,12 +574,12 @@ uint64_t tune_key(const Plan& p) {
 // 1: 2 digits, 5 CTAs), bits 8-16 = phases launched over their interleaved
 // integer / FP64 job list (else as two launches), bit 17 = P5's FP64 and
 // integer rows on two streams at once, bit 18 = the FP64 rows in the TMA
-// form (p5_mac_fp_tma; takes precedence over bit 7)
+// form (p5_mac_fp_tma, three stages; with bit 7, two)
 void apply_choice(Plan& p, int choice) {
     p.p5_form = choice & 3;
     p.p5_fp = (choice >> 6) & 1;
-    p.p5_fp_form = (choice >> 18) & 1 ? 2 : (choice >> 7) & 1;
-    if (p.p5_fp_form == 2 && !mac_tma_ok(p.dc.dnum)) p.p5_fp_form = 0;
+    p.p5_fp_form = ((choice >> 18) & 1 ? 2 : 0) + ((choice >> 7) & 1);
+    if (p.p5_fp_form >= 2 && !mac_tma_ok(p.dc.dnum)) p.p5_fp_form = 0;
     p.p5_split = (choice >> 17) & 1;
     if (p.p5_split) ensure_side(p);   // outside any graph capture where possible
     if (p.p5_form == P5_ASYNC && !mac_async_ok(p.dc.dnum)) p.p5_form = P5_REG128;
@@ -647,8 +651,9 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         // P5 FP64 rows (register form 0, then the TMA form where its ring fits,
         // else register form 1) or integer; the TMA form wins the large
         // batches, form 0 the small ones (its ring's set-up is not amortised)
-        const std::vector<int> fpv = mac_tma_ok(p.dc.dnum) && !p.concurrent ? std::vector<int>{64, 64 | 1 << 18, 0}
-                                                           : std::vector<int>{64, 64 | 128, 0};
+        const std::vector<int> fpv = mac_tma_ok(p.dc.dnum) && !p.concurrent
+                                         ? std::vector<int>{64, 64 | 1 << 18, 64 | 128 | 1 << 18, 0}
+                                         : std::vector<int>{64, 64 | 128, 0};
         cur = pick(1u << 4, 64 | 128 | 1 << 18, fpv, cur);
         if (cur & 64) cur = pick(1u << 4, 1 << 17, {0, 1 << 17}, cur);   // FP64 and integer rows concurrent
     }

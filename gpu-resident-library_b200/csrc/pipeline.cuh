@@ -1057,8 +1057,8 @@ constexpr int P5T_NT = P5T_NC + 32;         // + one producer warp
 constexpr int P5T_STAGES = 3;
 constexpr int P5T_BAR_WORDS = 16;           // mbarriers: key, full[S], empty[S] (padded)
 static_assert(1 + 2 * P5T_STAGES <= P5T_BAR_WORDS, "mbarrier area");
-__host__ __device__ constexpr int p5t_smem(int dnum) {
-    return (P5T_BAR_WORDS + (2 * dnum + P5T_STAGES * maca_slots(dnum)) * P5T_TILE) * 8;
+__host__ __device__ constexpr int p5t_smem(int dnum, int stages = P5T_STAGES) {
+    return (P5T_BAR_WORDS + (2 * dnum + stages * maca_slots(dnum)) * P5T_TILE) * 8;
 }
 
 __device__ __forceinline__ u32 smem_addr(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -1105,18 +1105,21 @@ __device__ __forceinline__ void bulk_load(u32 dst, const void* src, u32 bytes, u
 
 // Ring of the TMA forms: mbarriers at the start of dynamic shared memory
 // (key, full[S], empty[S]), then the key tile [dnum][2][P5T_TILE], then
-// P5T_STAGES stages of maca_slots(dnum) rows.
+// S stages of maca_slots(dnum) rows.
+template <int S>
 struct P5Ring {
     u64* keys;
     u64* stage;
     u32 kbar;
     __device__ __forceinline__ u32 full(u32 b) const { return kbar + 8 * (1 + b); }
-    __device__ __forceinline__ u32 empty(u32 b) const { return kbar + 8 * (1 + P5T_STAGES + b); }
+    __device__ __forceinline__ u32 empty(u32 b) const { return kbar + 8 * (1 + S + b); }
 };
 
 // Thread 0 initialises the mbarriers; every thread learns whether an earlier
 // CTA's wait expired (then the CTA leaves before issuing anything).
-__device__ __forceinline__ bool p5t_setup(const DevCtx& D, u64* sm, P5Ring& R) {
+template <int S>
+__device__ __forceinline__ bool p5t_setup(const DevCtx& D, u64* sm, P5Ring<S>& R) {
+    static_assert(1 + 2 * S <= P5T_BAR_WORDS, "mbarrier area");
     __shared__ u32 failed;
     R.keys = sm + P5T_BAR_WORDS;
     R.stage = R.keys + 2 * D.dnum * P5T_TILE;
@@ -1124,7 +1127,7 @@ __device__ __forceinline__ bool p5t_setup(const DevCtx& D, u64* sm, P5Ring& R) {
     if (threadIdx.x == 0) {
         failed = *reinterpret_cast<volatile u32*>(D.err);
         mbar_init(R.kbar, 1);
-        for (u32 b = 0; b < P5T_STAGES; ++b) {
+        for (u32 b = 0; b < (u32)S; ++b) {
             mbar_init(R.full(b), 1);
             mbar_init(R.empty(b), P5T_NC);
         }
@@ -1139,11 +1142,10 @@ __device__ __forceinline__ bool p5t_setup(const DevCtx& D, u64* sm, P5Ring& R) {
 // (slot 1) of a Q row and every other digit of its tower (slot MACA_IN + p),
 // into stage g % S after the consumers have released it; finally it waits
 // (bounded) for every copy in flight.
-template <int LOGN>
+template <int LOGN, int S>
 __device__ __forceinline__ void p5t_produce(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
-                                            const u32* __restrict__ plist, const u32 tile0, const P5Ring& R) {
+                                            const u32* __restrict__ plist, const u32 tile0, const P5Ring<S>& R) {
     constexpr u32 ROW = P5T_TILE * 8;           // bytes of one staged row
-    constexpr int S = P5T_STAGES;
     const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum), K = D.K;
     const bool is_p = r >= D.fullQ;
     const PairDesc& P0 = pairs[plist[jb.y]];
@@ -1193,10 +1195,9 @@ __device__ __forceinline__ void p5t_produce(const DevCtx& D, const PairDesc* __r
 
 // Consumer of the TMA forms for an integer key row (a P row, or a Q row of
 // any width): p5_mac's arithmetic on one 16-byte pair of the tile per thread.
-template <int LOGN>
+template <int LOGN, int S>
 __device__ __forceinline__ void p5t_consume_int(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
-                                                const u32* __restrict__ plist, const u32 tile0, const P5Ring& R) {
-    constexpr int S = P5T_STAGES;
+                                                const u32* __restrict__ plist, const u32 tile0, const P5Ring<S>& R) {
     const u32 r = jb.x, slots = maca_slots((int)D.dnum);
     const bool is_p = r >= D.fullQ;
     const u32 K = D.K;
@@ -1318,7 +1319,7 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
     extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
     const uint4 jb = jobs[blockIdx.x / TILES];
     const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
-    P5Ring R;
+    P5Ring<P5T_STAGES> R;
     if (!p5t_setup(D, sm, R)) return;
     if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
         if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
@@ -1337,10 +1338,9 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
 // p5_mac_fp's: products |r| <= 0.75 q, the sums normalised after every
 // eighth digit, every value an exact integer below 2^53. Results equal
 // p5_mac's word for word.
-template <int LOGN>
+template <int LOGN, int S>
 __device__ __forceinline__ void p5t_consume_fp(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
-                                               const u32* __restrict__ plist, const u32 tile0, const P5Ring& R) {
-    constexpr int S = P5T_STAGES;
+                                               const u32* __restrict__ plist, const u32 tile0, const P5Ring<S>& R) {
     const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum);   // a Q row, q < 2^50
     const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
     const u32 K = D.K, pin = r / D.alpha;       // digit holding tower r
@@ -1469,7 +1469,9 @@ __device__ __forceinline__ void p5t_consume_fp(const DevCtx& D, const PairDesc* 
     }
 }
 
-template <int LOGN>
+// S = 3 stages (65.7 KB at dnum 4, three CTAs per SM) or 2 (49.3 KB, four,
+// or three beside an integer P5 CTA on a second stream).
+template <int LOGN, int S>
 __global__ void __launch_bounds__(P5T_NT, 3)
 p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
               const u32* __restrict__ plist) {
@@ -1477,7 +1479,7 @@ p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* _
     extern __shared__ __align__(128) u64 sm[];  // mbarriers | key [dnum][2][TILE] | stage [S][slots][TILE]
     const uint4 jb = jobs[blockIdx.x / TILES];
     const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
-    P5Ring R;
+    P5Ring<S> R;
     if (!p5t_setup(D, sm, R)) return;
     if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
         if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);

@@ -39,7 +39,8 @@ struct Plan {
     // launch schedule (chosen by tune() or the context's tuning cache)
     int p5_form = 0;                   // P5_REG128, P5_ASYNC or P5_REG256
     bool p5_fp = false;                // P5 key rows of 50-bit Q towers on the FP64 pipe (p5_mac_fp)
-    int p5_fp_form = 0;                // 0: 4 digits in flight, 4 CTAs per SM; 1: 2 digits, 5 CTAs; 2: TMA ring
+    int p5_fp_form = 0;                // 0: 4 digits in flight, 4 CTAs per SM; 1: 2 digits, 5 CTAs;
+                                       // 2, 3: TMA ring of three or two stages
     bool p5_split = false;             // FP64 and integer P5 rows on two streams at once (fork / join)
     // the second stream and its fork / join events, made on first use
     mutable cudaStream_t side = nullptr;

@@ -303,7 +303,7 @@ class Plan:
         form = {0: "register-128x4", 1: "cp.async", 2: "register-256x2", 3: "tma"}.get(b & 3, "?")
         p3 = {0: "plain", 1: "warp-specialised-128x2", 2: "warp-specialised-256x1"}.get((b >> 3) & 3, "?")
         mixed = [k + 1 for k in range(9) if b >> (8 + k) & 1]
-        return {"p5": form, "p5_fp64_rows": bool(b & 64), "p5_fp64_form": 2 if b >> 18 & 1 else (b >> 7) & 1, "p5_split": bool(b >> 17 & 1), "mixed_paths": bool(b & 4), "mixed_phases": mixed,
+        return {"p5": form, "p5_fp64_rows": bool(b & 64), "p5_fp64_form": (2 if b >> 18 & 1 else 0) + ((b >> 7) & 1), "p5_split": bool(b >> 17 & 1), "mixed_paths": bool(b & 4), "mixed_phases": mixed,
                 "p3": p3, "tuned": bool(b & 32)}
 
     def launch_host(self, h_in, h_out, stream=None, sync=True):

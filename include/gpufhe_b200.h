@@ -328,7 +328,8 @@ uint32_t gpufhe_plan_kernel_count(const gpufhe_plan* plan);
  * 1: two digits, five CTAs), bit 17 = those FP64 rows on a second stream
  * beside the integer rows (forked and joined inside the launch, graph-
  * capturable), bit 18 = those FP64 rows through the bulk-copy (TMA) stage
- * ring of form 3 instead (overrides bit 7), bits 8-16 = the
+ * ring of form 3 instead, of three stages (bit 7 clear) or two (bit 7 set),
+ * bits 8-16 = the
  * phases (bit 8 + k for phase k+1) launched interleaved (the others as two
  * launches). */
 uint32_t gpufhe_plan_schedule(const gpufhe_plan* plan);

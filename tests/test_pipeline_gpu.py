@@ -146,7 +146,7 @@ def test_rotate_hoisted_groups(G, S, gctx):
 
 
 @pytest.mark.parametrize("schedule", [0, 1, 2, 3, 4, 5, 6, 7, 8, 11, 12, 13, 16, 19, 20, 64, 65, 66, 67, 68, 72, 84, 192, 195, 196, 64 | 1 << 17, 195 | 1 << 17,
-                                      64 | 1 << 18, 67 | 1 << 17 | 1 << 18, 196 | 1 << 18])
+                                      64 | 1 << 18, 67 | 1 << 17 | 1 << 18, 196 | 1 << 18, 192 | 1 << 18, 195 | 1 << 17 | 1 << 18])
 def test_every_schedule_same_bits(G, S, gctx, schedule):
     """Each launch schedule the autotuner can pick (P5 form, P5 50-bit Q rows
     on the FP64 pipe or not and in which of its three forms, P3 form, interleaved or separate integer / FP64
@@ -180,7 +180,7 @@ def test_every_schedule_same_bits(G, S, gctx, schedule):
     assert got["tuned"] and got["mixed_paths"] == bool(schedule & 4)
     assert got["p3"] == ("plain", "warp-specialised-128x2", "warp-specialised-256x1")[(schedule >> 3) & 3]
     assert got["p5_fp64_rows"] == bool(schedule & 64)
-    assert got["p5_fp64_form"] == (2 if schedule >> 18 & 1 else (schedule >> 7) & 1)
+    assert got["p5_fp64_form"] == (2 if schedule >> 18 & 1 else 0) + ((schedule >> 7) & 1)
     assert got["p5_split"] == bool(schedule >> 17 & 1)
     for outs, (e0, e1) in want:
         assert np.array_equal(host(outs[0]), e0) and np.array_equal(host(outs[1]), e1)

@@ -20,7 +20,7 @@ def S():
 
 
 @pytest.mark.parametrize("schedule", [0, 1, 2, 3, 8, 16, 7, 64, 67, 71, 192, 64 | 1 << 17, 64 | 1 << 18,
-                                      64 | 1 << 17 | 1 << 18])
+                                      64 | 1 << 17 | 1 << 18, 192 | 1 << 18])
 def test_mixed_batch_small_ring(S, schedule):
     import gpufhe_b200 as G
     g = S.gpu_context()
@@ -108,7 +108,7 @@ def test_forms_after_a_larger_dnum():
             assert np.array_equal(got[k][0], got[0][0]) and np.array_equal(got[k][1], got[0][1]), (tw, k)
 
 
-@pytest.mark.parametrize("schedule", [64, 192, 0, 64 | 1 << 17, 64 | 1 << 18])
+@pytest.mark.parametrize("schedule", [64, 192, 0, 64 | 1 << 17, 64 | 1 << 18, 192 | 1 << 18])
 def test_many_digits_fp64_key_product(schedule):
     """Twelve digits (alpha = 1): the FP64 key inner product normalises its
     accumulators after every eighth digit; EvalMult+Rescale and keyswitch at
