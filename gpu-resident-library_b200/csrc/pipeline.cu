@@ -155,7 +155,7 @@ struct Launcher {
                     p5_mac_fp_tma<LOGN, 3><<<nfp * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum, 3), sf>>>(
                         D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
                 else if (nfp && p.p5_fp_form == 3 && mac_tma_ok(D.dnum))
-                    p5_mac_fp_tma<LOGN, 2><<<nfp * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum, 2), sf>>>(
+                    p5_mac_fp_tma<LOGN, 2><<<nfp * ((1u << LOGN) / P5T_TILE), P5T_NT, p5t_smem((int)D.dnum, 2, true), sf>>>(
                         D, p.d_pairs, p.d_mac_jobs + p.job_off[4][1], p.d_plist);
                 else if (nfp && p.p5_fp_form == 1)
                     p5_mac_fp<LOGN, 2, 5><<<nfp * MAC_TILES, MACF_NT, mac_smem(D.dnum), sf>>>(

@@ -1057,8 +1057,8 @@ constexpr int P5T_NT = P5T_NC + 32;         // + one producer warp
 constexpr int P5T_STAGES = 3;
 constexpr int P5T_BAR_WORDS = 16;           // mbarriers: key, full[S], empty[S] (padded)
 static_assert(1 + 2 * P5T_STAGES <= P5T_BAR_WORDS, "mbarrier area");
-__host__ __device__ constexpr int p5t_smem(int dnum, int stages = P5T_STAGES) {
-    return (P5T_BAR_WORDS + (2 * dnum + stages * maca_slots(dnum)) * P5T_TILE) * 8;
+__host__ __device__ constexpr int p5t_smem(int dnum, int stages = P5T_STAGES, bool compact = false) {
+    return (P5T_BAR_WORDS + (2 * dnum + stages * (maca_slots(dnum) - (compact ? 1 : 0))) * P5T_TILE) * 8;
 }
 
 __device__ __forceinline__ u32 smem_addr(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -1105,12 +1105,17 @@ __device__ __forceinline__ void bulk_load(u32 dst, const void* src, u32 bytes, u
 
 // Ring of the TMA forms: mbarriers at the start of dynamic shared memory
 // (key, full[S], empty[S]), then the key tile [dnum][2][P5T_TILE], then
-// S stages of maca_slots(dnum) rows.
+// S stages of `slots` rows: MACA_IN input rows, then a row per digit. A
+// compact ring (Q rows only) leaves out the row of the digit that holds the
+// tower itself, which is never copied.
 template <int S>
 struct P5Ring {
     u64* keys;
     u64* stage;
     u32 kbar;
+    u32 slots;
+    bool compact;
+    __device__ __forceinline__ u32 slot(u32 p, u32 pin) const { return MACA_IN + p - (compact && p > pin ? 1u : 0u); }
     __device__ __forceinline__ u32 full(u32 b) const { return kbar + 8 * (1 + b); }
     __device__ __forceinline__ u32 empty(u32 b) const { return kbar + 8 * (1 + S + b); }
 };
@@ -1118,9 +1123,11 @@ struct P5Ring {
 // Thread 0 initialises the mbarriers; every thread learns whether an earlier
 // CTA's wait expired (then the CTA leaves before issuing anything).
 template <int S>
-__device__ __forceinline__ bool p5t_setup(const DevCtx& D, u64* sm, P5Ring<S>& R) {
+__device__ __forceinline__ bool p5t_setup(const DevCtx& D, u64* sm, P5Ring<S>& R, bool compact = false) {
     static_assert(1 + 2 * S <= P5T_BAR_WORDS, "mbarrier area");
     __shared__ u32 failed;
+    R.compact = compact;
+    R.slots = (u32)maca_slots((int)D.dnum) - (compact ? 1u : 0u);
     R.keys = sm + P5T_BAR_WORDS;
     R.stage = R.keys + 2 * D.dnum * P5T_TILE;
     R.kbar = smem_addr(sm);
@@ -1146,7 +1153,7 @@ template <int LOGN, int S>
 __device__ __forceinline__ void p5t_produce(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
                                             const u32* __restrict__ plist, const u32 tile0, const P5Ring<S>& R) {
     constexpr u32 ROW = P5T_TILE * 8;           // bytes of one staged row
-    const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum), K = D.K;
+    const u32 r = jb.x, dnum = D.dnum, slots = R.slots, K = D.K;
     const bool is_p = r >= D.fullQ;
     const PairDesc& P0 = pairs[plist[jb.y]];
     mbar_arrive_expect_tx(R.kbar, 2 * dnum * ROW);
@@ -1182,7 +1189,7 @@ __device__ __forceinline__ void p5t_produce(const DevCtx& D, const PairDesc* __r
             for (u32 p = 0; p < nparts; ++p) {
                 if (p == pin) continue;
                 const u64* Yt = P.ysrc + ((size_t)(w.Y + p * QlP + i) << LOGN) + tile0;
-                bulk_load(smem_addr(sb + (MACA_IN + p) * P5T_TILE), Yt, ROW, R.full(b));
+                bulk_load(smem_addr(sb + R.slot(p, pin) * P5T_TILE), Yt, ROW, R.full(b));
             }
         issued = g + 1;
     }
@@ -1198,7 +1205,7 @@ __device__ __forceinline__ void p5t_produce(const DevCtx& D, const PairDesc* __r
 template <int LOGN, int S>
 __device__ __forceinline__ void p5t_consume_int(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
                                                 const u32* __restrict__ plist, const u32 tile0, const P5Ring<S>& R) {
-    const u32 r = jb.x, slots = maca_slots((int)D.dnum);
+    const u32 r = jb.x, slots = R.slots;
     const bool is_p = r >= D.fullQ;
     const u32 K = D.K;
     const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
@@ -1263,7 +1270,7 @@ __device__ __forceinline__ void p5t_consume_int(const DevCtx& D, const PairDesc*
 #pragma unroll
                 for (int j = 0; j < 2; ++j) v2set(dv, j, Yt[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
             } else {
-                dv = ld2(sb + (MACA_IN + p) * P5T_TILE);
+                dv = ld2(sb + R.slot(p, pin) * P5T_TILE);
             }
             const ulonglong2 kbv = ld2(R.keys + (2 * p) * P5T_TILE + e);
             const ulonglong2 kav = ld2(R.keys + (2 * p + 1) * P5T_TILE + e);
@@ -1341,7 +1348,7 @@ p5_mac_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __re
 template <int LOGN, int S>
 __device__ __forceinline__ void p5t_consume_fp(const DevCtx& D, const PairDesc* __restrict__ pairs, const uint4 jb,
                                                const u32* __restrict__ plist, const u32 tile0, const P5Ring<S>& R) {
-    const u32 r = jb.x, dnum = D.dnum, slots = maca_slots((int)dnum);   // a Q row, q < 2^50
+    const u32 r = jb.x, dnum = D.dnum, slots = R.slots;   // a Q row, q < 2^50
     const u32 e = 2 * threadIdx.x;              // this thread's pair within the tile
     const u32 K = D.K, pin = r / D.alpha;       // digit holding tower r
     const ModC m = D.mod[r];
@@ -1412,7 +1419,7 @@ __device__ __forceinline__ void p5t_consume_fp(const DevCtx& D, const PairDesc* 
 #pragma unroll
                 for (int j = 0; j < 2; ++j) y[j] = ntt::u2d(Yt[galois_slot<LOGN>(tile0 + e + j, P.galois)]);
             } else {
-                const ulonglong2 dv = ld2(sb + (MACA_IN + p) * P5T_TILE);
+                const ulonglong2 dv = ld2(sb + R.slot(p, pin) * P5T_TILE);
                 y[0] = ntt::u2d(dv.x);
                 y[1] = ntt::u2d(dv.y);
             }
@@ -1469,10 +1476,10 @@ __device__ __forceinline__ void p5t_consume_fp(const DevCtx& D, const PairDesc* 
     }
 }
 
-// S = 3 stages (65.7 KB at dnum 4, three CTAs per SM) or 2 (49.3 KB, four,
-// or three beside an integer P5 CTA on a second stream).
+// S = 3 stages (65.7 KB at dnum 4, three CTAs per SM), or 2 stages in the
+// compact ring (44.1 KB, five CTAs per SM at up to 81 registers).
 template <int LOGN, int S>
-__global__ void __launch_bounds__(P5T_NT, 3)
+__global__ void __launch_bounds__(P5T_NT, S == 2 ? 5 : 3)
 p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* __restrict__ jobs,
               const u32* __restrict__ plist) {
     constexpr int TILES = (1 << LOGN) / P5T_TILE;
@@ -1480,7 +1487,7 @@ p5_mac_fp_tma(const DevCtx D, const PairDesc* __restrict__ pairs, const uint4* _
     const uint4 jb = jobs[blockIdx.x / TILES];
     const u32 tile0 = (blockIdx.x % TILES) * P5T_TILE;
     P5Ring<S> R;
-    if (!p5t_setup(D, sm, R)) return;
+    if (!p5t_setup(D, sm, R, S == 2)) return;
     if (threadIdx.x >= P5T_NC) {                // producer warp: lane 0 issues every copy
         if (threadIdx.x == P5T_NC) p5t_produce<LOGN>(D, pairs, jb, plist, tile0, R);
         return;
