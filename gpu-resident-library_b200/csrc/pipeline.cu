@@ -566,7 +566,12 @@ namespace {
 uint64_t tune_key(const Plan& p) {
     uint32_t cls = 0;
     while ((1u << (cls + 1)) <= p.nops) ++cls;   // batch-size class: floor(log2(nops))
-    return (p.concurrent ? 1ull << 48 : 0ull) | ((uint64_t)p.logn << 40) | ((uint64_t)p.dc.dnum << 32) | cls;
+    // hoisted rotations read their shared digits by an eval-slot gather, which
+    // favours other P5 forms than batches whose digits stream in order
+    bool hoisted = false;
+    for (const Op& op : p.ops) hoisted = hoisted || op.mode == HROT;
+    return (p.concurrent ? 1ull << 48 : 0ull) | ((uint64_t)p.logn << 40) | ((uint64_t)p.dc.dnum << 32) |
+           (hoisted ? 1ull << 16 : 0ull) | cls;
 }
 // choice: bits 0-1 = P5 form, bits 3-4 = P3 form (0 plain, 1 and 2
 // warp-specialised), bit 6 = P5 key rows of 50-bit Q towers on the FP64
@@ -652,7 +657,7 @@ void tune(Plan& p, cudaStream_t s, bool measure) {
         // else register form 1) or integer; the TMA form wins the large
         // batches, form 0 the small ones (its ring's set-up is not amortised)
         const std::vector<int> fpv = mac_tma_ok(p.dc.dnum) && !p.concurrent
-                                         ? std::vector<int>{64, 64 | 1 << 18, 64 | 128 | 1 << 18, 0}
+                                         ? std::vector<int>{64, 64 | 128, 64 | 1 << 18, 64 | 128 | 1 << 18, 0}
                                          : std::vector<int>{64, 64 | 128, 0};
         cur = pick(1u << 4, 64 | 128 | 1 << 18, fpv, cur);
         if (cur & 64) cur = pick(1u << 4, 1 << 17, {0, 1 << 17}, cur);   // FP64 and integer rows concurrent
