@@ -308,26 +308,55 @@ xf::Job xjob(const Context& c, const std::vector<u64>& qp, u64* x, uint32_t qi, 
     return j;
 }
 
-// Transforms polys x towers tower-polys at base ([poly][tower][n], tower t
-// uses QP modulus t) in one launch pair.
-void transform(const Context& c, const std::vector<u64>& qp, Scratch& S, u64* base, uint32_t polys,
-               uint32_t towers, bool inverse) {
-    const uint32_t n = c.n();
-    std::vector<xf::Job> jobs((size_t)polys * towers);
-    for (uint32_t p = 0; p < polys; ++p)
-        for (uint32_t t = 0; t < towers; ++t)
-            jobs[(size_t)p * towers + t] = xjob(c, qp, base + ((size_t)p * towers + t) * n, t, inverse);
-    xf::Job* dj = S.get<xf::Job>(jobs.size());
-    ck(cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(xf::Job), cudaMemcpyHostToDevice, S.s), "job upload");
-    // (a copy from pageable memory has read the job list when it returns)
-    ck(xf_launch_ntt(dj, nullptr, (int)jobs.size(), (int)c.logn(), inverse, S.s), "transform");
-}
-
 template <class T>
 T* upload(Scratch& S, const std::vector<T>& h) {
     T* d = S.get<T>(h.size());
     ck(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, S.s), "upload");
+    // (a copy from pageable memory has read `h` when it returns)
     return d;
+}
+
+// Job p * towers + t of a batch: the template of tower t on x = xs[p] + t n
+// (xs given) or base + (p * towers + t) n, lifting from lift + p n when lift
+// is set. Built on the device, so a batch of thousands of tower transforms
+// costs the host one template per tower.
+__global__ void k_tower_jobs(xf::Job* __restrict__ jobs, const xf::Job* __restrict__ tmpl, u64* const* __restrict__ xs,
+                             u64* base, const u64* lift, uint32_t polys, uint32_t towers, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= polys * towers) return;
+    const uint32_t p = i / towers, t = i % towers;
+    xf::Job j = tmpl[t];
+    j.x = xs ? xs[p] + (size_t)t * n : base + (size_t)i * n;
+    if (lift) j.lift = lift + (size_t)p * n;
+    jobs[i] = j;
+}
+
+// Device job table for polys x towers transforms (see k_tower_jobs); with
+// `lift`, every job's column pass lifts from it (lift_q0 as in xf::Job).
+xf::Job* tower_jobs(const Context& c, const std::vector<u64>& qp, Scratch& S, uint32_t polys, uint32_t towers,
+                    bool inverse, u64* const* xs, u64* base, const u64* lift = nullptr, u64 lift_q0 = 0) {
+    std::vector<xf::Job> tmpl(towers);
+    for (uint32_t t = 0; t < towers; ++t) {
+        tmpl[t] = xjob(c, qp, nullptr, t, inverse);
+        if (lift) {
+            tmpl[t].lift_q0 = lift_q0;
+            tmpl[t].lift_r64 = ~0ull / qp[t];
+        }
+    }
+    const xf::Job* dt = upload(S, tmpl);
+    xf::Job* dj = S.get<xf::Job>((size_t)polys * towers);
+    const uint32_t total = polys * towers;
+    k_tower_jobs<<<(total + 255) / 256, 256, 0, S.s>>>(dj, dt, xs, base, lift, polys, towers, c.n());
+    ck(cudaGetLastError(), "job table");
+    return dj;
+}
+
+// Transforms polys x towers tower-polys at base ([poly][tower][n], tower t
+// uses QP modulus t) in one launch pair.
+void transform(const Context& c, const std::vector<u64>& qp, Scratch& S, u64* base, uint32_t polys,
+               uint32_t towers, bool inverse) {
+    xf::Job* dj = tower_jobs(c, qp, S, polys, towers, inverse, nullptr, base);
+    ck(xf_launch_ntt(dj, nullptr, (int)(polys * towers), (int)c.logn(), inverse, S.s), "transform");
 }
 
 #define KEYS_TRY(...)                                                          \
@@ -579,18 +608,11 @@ int gpufhe_pt_to_eval_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, cons
         for (u64* o : out)
             if (!o) throw std::invalid_argument("pt_to_eval: null output pointer");
         Scratch S(stream);
-        // each tower's forward transform reads the message and embeds it on load
-        std::vector<xf::Job> jobs((size_t)count * towers);
-        for (uint32_t p = 0; p < count; ++p)
-            for (uint32_t t = 0; t < towers; ++t) {
-                xf::Job& j = jobs[(size_t)p * towers + t];
-                j = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
-                j.lift = reinterpret_cast<const u64*>(d_m) + (size_t)p * n;
-                j.lift_q0 = 0;                 // signed 64-bit coefficients
-                j.lift_r64 = ~0ull / qp[t];
-            }
-        xf::Job* dj = upload(S, jobs);
-        ck(xf_launch_ntt_lift(dj, (int)jobs.size(), (int)c->logn(), stream), "pt_to_eval transform");
+        // each tower's forward transform reads the message and embeds it on
+        // load (lift_q0 = 0: signed 64-bit coefficients)
+        u64* const* dout = upload(S, out);
+        xf::Job* dj = tower_jobs(*c, qp, S, count, towers, false, dout, nullptr, reinterpret_cast<const u64*>(d_m), 0);
+        ck(xf_launch_ntt_lift(dj, (int)(count * towers), (int)c->logn(), stream), "pt_to_eval transform");
         return GPUFHE_OK;
     })
 }
@@ -625,17 +647,9 @@ int gpufhe_modraise_batch(gpufhe_ctx* h, uint32_t count, uint32_t towers, const 
         transform(*c, qp, S, x, comps, 1, true);                        // tower 0 -> coefficients
         // every tower -> eval form, its column pass lifting tower 0 (centred
         // mod q0) into the tower's modulus on load
-        std::vector<xf::Job> jobs((size_t)comps * towers);
-        for (uint32_t p = 0; p < comps; ++p)
-            for (uint32_t t = 0; t < towers; ++t) {
-                xf::Job& j = jobs[(size_t)p * towers + t];
-                j = xjob(*c, qp, out[p] + (size_t)t * n, t, false);
-                j.lift = x + (size_t)p * n;
-                j.lift_q0 = qp[0];
-                j.lift_r64 = ~0ull / qp[t];
-            }
-        xf::Job* dj = upload(S, jobs);
-        ck(xf_launch_ntt_lift(dj, (int)jobs.size(), (int)c->logn(), stream), "modraise transform");
+        u64* const* dout = upload(S, out);
+        xf::Job* dj = tower_jobs(*c, qp, S, comps, towers, false, dout, nullptr, x, qp[0]);
+        ck(xf_launch_ntt_lift(dj, (int)(comps * towers), (int)c->logn(), stream), "modraise transform");
         return GPUFHE_OK;
     })
 }
