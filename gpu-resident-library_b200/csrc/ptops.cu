@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "context.hpp"
+#include "ntt.cuh"
 #include "gpufhe_b200.h"
 
 gfx::Context* gpufhe_impl(gpufhe_ctx* h);
@@ -27,9 +28,17 @@ __device__ __forceinline__ u64 pw_add(u64 a, u64 b, u64 q) {
     return s >= q ? s - q : s;
 }
 __device__ __forceinline__ u64 pw_sub(u64 a, u64 b, u64 q) { return a >= b ? a - b : a + q - b; }
-// (a * b) mod q for any 64-bit a, b: operands reduced first, then one product
+// (a * b) mod q for any 64-bit a, b: operands reduced first, then one
+// product. Canonical operands (the usual case) skip the two reductions, and
+// for q < 2^50 their product runs on the FP64 pipe: an exact FP64 modular
+// product of unsigned operands below q (|r| <= 2q), normalised to [0, q).
 __device__ __forceinline__ u64 pw_mul(u64 a, u64 b, const ModC& m) {
-    return mulmod(reduce64(a, m), reduce64(b, m), m);
+    if (a >= m.q || b >= m.q) return mulmod(reduce64(a, m), reduce64(b, m), m);
+    if (fp_tower(m.q)) {
+        const ntt::FpAr ar{ntt::u2d(m.q), qinv_of(m)};
+        return ar.out(ar.norm(ar.mulq<true>(ntt::u2d(a), ntt::u2d(b))));
+    }
+    return mulmod(a, b, m);
 }
 
 // blockIdx.y = operation, blockIdx.z = tower (towers beyond an operation's
