@@ -225,7 +225,20 @@ __device__ __forceinline__ void p1_inv_row_body(const DevCtx& D, const PairDesc*
         ntt::row_tile_stage2<G::RB, G::ROW_THREADS>(
             [&](int rl, int c) { return P.in[1][o + rl * 256 + c]; },
             [&](int rl, int c) { return P.in[3][o + rl * 256 + c]; },
-            [&](int rl, int c, u64 a, u64 b) { sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = ar.stage_in(mulmod(a, b, m)); });
+            [&](int rl, int c, u64 a, u64 b) {
+                u64 v;
+                if constexpr (FP) {   // canonical operands: the product exactly on the FP64 pipe
+                    if (a < m.q && b < m.q) {
+                        const ntt::FpAr ua{ntt::u2d(m.q), qinv_of(m)};
+                        v = ar.bits(ua.norm(ua.mulq<true>(ntt::u2d(a), ntt::u2d(b))));
+                    } else {
+                        v = ar.stage_in(mulmod(a, b, m));
+                    }
+                } else {
+                    v = ar.stage_in(mulmod(a, b, m));
+                }
+                sm[rl * G::ROW_STRIDE + ntt::rowpad(c)] = v;
+            });
     } else {
         ntt::row_tile_stage<G::RB, G::ROW_THREADS>(
             [&](int rl, int c) { return digit_src<LOGN>(P, i, (R0 + rl) * 256 + c, m); },
