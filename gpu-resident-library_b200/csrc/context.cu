@@ -129,6 +129,17 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
                 pool.push_back(dc_.mont_up ? hm::mulmod(v, r64mod(m), m) : v);
             }
         }
+        lv.qmpp_off = lv.qmp_off;
+        if (dc_.mont_up) {   // plain copies for the FP64 conversion of P3
+            lv.qmpp_off = (u32)pool.size();
+            for (uint32_t i = 0; i < L; ++i) {
+                const uint32_t p = i / alpha, st = lv.part_st[p], sp = lv.part_sp[p];
+                for (uint32_t j = 0; j < QlP; ++j) {
+                    const u64 m = j < L ? Q[j] : P[j - L];
+                    pool.push_back(hm::prod_mod(Q.data() + st, sp, m, (int)(i - st)));
+                }
+            }
+        }
         if (L >= 2) {
             // s1 = ql^-1 mod q_i and s2 = floor(Ql*u/ql) mod q_i (params.cpp:54-75),
             // which equals q_i - s1 (the derivation is at native_rescale_consts)

@@ -26,7 +26,8 @@ constexpr int MAXD = 48;     // digits
 struct Level {
     u32 L, nparts;
     u32 part_st[MAXD], part_sp[MAXD];
-    u32 qmp_off;                       // pool offset of qhatmodp [L][L+K]
+    u32 qmp_off;                       // pool offset of qhatmodp [L][L+K] (times 2^64 with mont_up)
+    u32 qmpp_off;                      // the same entries without the 2^64 factor (FP64 conversions)
     u64 up_scale[MAXQ], up_scale_p[MAXQ];    // n^-1 * QHatInv_i (i's digit) mod q_i
     // rescale of tower L-1 onto i < L-1
     u64 s1[MAXQ], s1p[MAXQ];           // q_l^-1 mod q_i

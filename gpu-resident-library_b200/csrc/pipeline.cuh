@@ -304,9 +304,60 @@ __device__ __forceinline__ void p3_modup_fwd_col_body(const DevCtx& D, const Pai
     const WsLayout w = ws_layout(L, K, D.alpha);
     const u64* X = slot_ptr(P, w.X + st0, LOGN) + c0;
     u64* Y = slot_ptr(P, w.Y + p * QlP + i, LOGN) + c0;
-    const u64* pool = D.pool + lv.qmp_off + (size_t)st0 * QlP + i;
-    if (threadIdx.x < sp) cst[threadIdx.x] = pool[(size_t)threadIdx.x * QlP];
+    // A 50-bit target whose digit has at most three sources, all below 2^50,
+    // converts on the FP64 pipe: every term x_s * QHatModp[s][i] is an exact
+    // FP64 modular product of unsigned operands (|r| <= 2q), their sum stays
+    // below 6q < 2^53, and one normalisation gives the canonical residue.
+    bool fpc = false;
+    if constexpr (FP) {
+        fpc = sp <= 3;
+        for (u32 s = 0; s < sp; ++s) fpc = fpc && fp_tower(D.mod[st0 + s].q);
+    }
+    const u64* pool = D.pool + (fpc ? lv.qmpp_off : lv.qmp_off) + (size_t)st0 * QlP + i;
+    if (threadIdx.x < sp) {
+        const u64 c = pool[(size_t)threadIdx.x * QlP];
+        cst[threadIdx.x] = fpc ? (u64)__double_as_longlong(ntt::u2d(c)) : c;
+    }
     __syncthreads();
+    if (fpc) {
+        const ntt::FpAr ua{ntt::u2d(m.q), qinv_of(m)};
+#pragma unroll 1
+        for (int k0 = 0; k0 < CS::PER; k0 += CS_VB) {
+            int r[CS_VB], cl[CS_VB];
+            size_t e[CS_VB];
+            ulonglong2 xv[3][CS_VB];
+#pragma unroll
+            for (int b = 0; b < CS_VB; ++b) {
+                CS::pos(k0 + b, r[b], cl[b]);
+                e[b] = (size_t)r[b] * 256 + cl[b];
+            }
+#pragma unroll
+            for (int t = 0; t < 3; ++t)
+                if ((u32)t < sp)
+#pragma unroll
+                    for (int b = 0; b < CS_VB; ++b) xv[t][b] = ld2(X + ((size_t)t << LOGN) + e[b]);
+#pragma unroll
+            for (int b = 0; b < CS_VB; ++b) {
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int t = 0; t < 3; ++t)
+                    if ((u32)t < sp) {
+                        const double c = __longlong_as_double((long long)cst[t]);
+                        a0 = __dadd_rn(a0, ua.mulq<true>(ntt::u2d(xv[t][b].x), c));
+                        a1 = __dadd_rn(a1, ua.mulq<true>(ntt::u2d(xv[t][b].y), c));
+                    }
+                ulonglong2 v;
+                v.x = ua.out(ua.norm(a0));
+                v.y = ua.out(ua.norm(a1));
+                *reinterpret_cast<ulonglong2*>(sm + r[b] * G::C + cl[b]) = v;
+            }
+        }
+        __syncthreads();
+        auto ld = [&](int r, int cl) { return sm[r * G::C + cl]; };
+        auto stf = [&](int r, int cl, u64 v) { Y[r * 256 + cl] = v; };
+        ntt::fwd_col_rounds<G::A, G::C, G::COL_THREADS, 0, true>(sm, twf_of<FP>(D, qp, LOGN), ar_of<FP>(m), ld, stf);
+        return;
+    }
     // conv_i = sum_s x_s * QHatModp[s][i] (ApproxSwitchCRTBasis), lazy in [0, 4q)
 #pragma unroll 1
     for (int k0 = 0; k0 < CS::PER; k0 += CS_VB) {
