@@ -964,6 +964,7 @@ def run_gpu(args):
         gen = torch.Generator(device=dev)
         gen.manual_seed(SEED)
         res = rotation_batch(G, torch, dev, local, gen, max(3, min(args.steps, 10)))
+        res.pop("_check", None)   # outputs kept for the full run's CPU check
         print(json.dumps({"section": "rot", "rotation_batch": res}), flush=True)
         return 0
     n = 1 << N_LOG
