@@ -3,6 +3,7 @@
 #include <cstring>
 #include <stdexcept>
 
+#include "devonce.hpp"
 #include "hostmath.hpp"
 #include "params.h"
 
@@ -35,6 +36,25 @@ T* Context::upload(const std::vector<T>& h) {
     return d;
 }
 
+namespace {
+// The batched key, encryption, ModRaise and embedding entry points take their
+// scratch (up to a few hundred MB per call) from the device's default
+// stream-ordered pool. With the pool's default release threshold of zero,
+// every synchronisation hands that memory back, and the next call maps and
+// clears it again; keeping up to 4 GiB in the pool makes repeated calls
+// reuse it. Raised only, once per device, never lowered.
+void keep_scratch_pool(int device) {
+    static gfx::DeviceOnce once;
+    once([device] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return;
+        uint64_t cur = 0, want = 4ull << 30;
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < want)
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &want);
+    });
+}
+}  // namespace
+
 Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& P, uint32_t alpha,
                  const std::vector<u64>& roots, int device)
     : n_(n), alpha_(alpha), device_(device), Q_(Q), P_(P) {
@@ -56,6 +76,7 @@ Context::Context(uint32_t n, const std::vector<u64>& Q, const std::vector<u64>& 
     roots_.resize(QP);
     for (uint32_t i = 0; i < QP; ++i) roots_[i] = roots.empty() ? native_root(n, QPm[i]) : roots[i];
     cudaSetDevice(device);
+    keep_scratch_pool(device);
 
     // per-modulus constants and twiddles
     std::vector<ModC> mc(QP);
