@@ -154,6 +154,17 @@ k_inv_col(const Job* __restrict__ arr, const Job one) {
     u64* x = j.x;
     auto ld = [&](int r, int cl) { return x[r * 256 + c0 + cl]; };
     const u64 sc = j.scale, scp = j.scale_p;
+    if (j.fp && sc < q) {   // n^-1 as an exact FP64 product (both operands below q < 2^50)
+        const ntt::FpAr ua{ntt::u2d(q), __ddiv_rn(1.0, ntt::u2d(q))};
+        const double scd = ntt::u2d(sc);
+        auto st = [&](int r, int cl, u64 v) {
+            x[r * 256 + c0 + cl] = ua.out(ua.norm(ua.mulq<true>(ntt::u2d(v), scd)));
+        };
+        with_path(j, [&](const auto& ar, const auto& tw) {
+            ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, tw, ar, ld, st);
+        });
+        return;
+    }
     auto st = [&](int r, int cl, u64 v) { x[r * 256 + c0 + cl] = shoup(v, sc, scp, q); };
     with_path(j, [&](const auto& ar, const auto& tw) {
         ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, tw, ar, ld, st);
