@@ -273,8 +273,15 @@ __device__ __forceinline__ void p2_inv_col_body(const DevCtx& D, const PairDesc*
     const WsLayout w = ws_layout(P.L, D.K, D.alpha);
     u64* X = slot_ptr(P, w.X + i, LOGN) + c0;
     auto ld = [&](int r, int cl) { return X[r * 256 + cl]; };
-    auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
-    ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, twi_of<FP>(D, i, LOGN), ar_of<FP>(m), ld, st);
+    if constexpr (FP) {   // the scale as an exact FP64 product (v, sc < q < 2^50), canonical
+        const ntt::FpAr ua{ntt::u2d(m.q), qinv_of(m)};
+        const double scd = ntt::u2d(sc);
+        auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = ua.out(ua.norm(ua.mulq<true>(ntt::u2d(v), scd))); };
+        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, twi_of<FP>(D, i, LOGN), ar_of<FP>(m), ld, st);
+    } else {
+        auto st = [&](int r, int cl, u64 v) { X[r * 256 + cl] = shoup(v, sc, scp, m.q); };
+        ntt::inv_col_rounds<G::A, G::C, G::COL_THREADS, G::A, true>(sm, twi_of<FP>(D, i, LOGN), ar_of<FP>(m), ld, st);
+    }
 }
 
 template <int LOGN, int PATH>
