@@ -81,6 +81,14 @@ def algorithmic_bytes(levels, n):
     return ct + 8 * n * 2 * beta * (Lm + K_SPECIAL)
 
 
+def p3_algorithmic_bytes(levels, n):
+    """Bytes one P3 launch (ModUp conversion + first forward NTT stages) must
+    move: per pair at level L with beta = ceil(L/alpha) digits, each digit's
+    source towers read once and its L + K - sp target towers written once,
+    beta (L + K) towers in all."""
+    return sum(8 * n * (-(-L // ALPHA)) * (L + K_SPECIAL) for L in levels)
+
+
 def p5_algorithmic_bytes(levels, n):
     """Bytes one P5 launch (keyswitch inner product + EvalMult/Rescale epilogue)
     must move over the batch: per pair at level L with beta = ceil(L/alpha)
@@ -103,11 +111,13 @@ def p5_algorithmic_bytes(levels, n):
 # DRAM traffic per algorithmic byte, from one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum) of the 16-pair case of this workload under the
 # 128-pair step's tuned schedule: P5 (its FP64 TMA-ring and integer kernels)
-# moved 755.3 MB against its 827.3 MB of algorithmic bytes, the whole step
-# 2543 MB against 489.7 MB. Both are scaled to the bench's launch by its
+# moved 755.3 MB against its 827.3 MB of algorithmic bytes, P3 302.2 MB
+# against 344.5 MB (part of its last writes still in L2 when it ends), the
+# whole step 2543 MB against 489.7 MB. All are scaled to the bench's launch by its
 # algorithmic bytes and reported with that label; they are not measured in
 # this run.
 P5_TRAFFIC_PER_ALG = 0.913
+P3_TRAFFIC_PER_ALG = 0.877
 STEP_TRAFFIC_PER_ALG = 5.19
 TRAFFIC_SOURCE = "ncu DRAM bytes of the 16-pair case of this workload, scaled to this launch by algorithmic bytes"
 
@@ -1198,6 +1208,7 @@ def run_gpu(args):
     pk = peaks()
     alg = algorithmic_bytes(levels, n)
     p5_alg = p5_algorithmic_bytes(levels, n)
+    p3_alg = p3_algorithmic_bytes(levels, n)
     achieved = alg / (ms_step * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "ops/s", "n_gpus": world, "steps": args.steps,
@@ -1208,9 +1219,18 @@ def run_gpu(args):
                    "mean_level": float(np.mean(levels)), "l2": "inputs larger than L2 (no flush)",
                    "graph": f"{kernels_per_step} kernels per step, one CUDA graph",
                    "schedule": schedule},
-        "roofline": {"bound": "hbm", "kernel": "P5: key-switch inner product + EvalMult/Rescale epilogue "
+        "roofline": {"bound": "hbm", "kernel": "P3: ModUp conversion + first 8 forward NTT stages "
+                                               "(p3_modup_fwd_col), the step's longest kernel",
+                     "achieved": p3_alg / (phases[2] * 1e-3) / 1e9, "peak": pk["hbm_gbs"],
+                     "peak_source": pk["source"] + " (burst copy)", "unit": "GB/s",
+                     "frac": p3_alg / (phases[2] * 1e-3) / 1e9 / pk["hbm_gbs"],
+                     "traffic": P3_TRAFFIC_PER_ALG * p3_alg, "traffic_source": TRAFFIC_SOURCE,
+                     "algorithmic_bytes_per_launch": p3_alg, "launch_ms": phases[2],
+                     "note": "bound by instruction issue, not HBM: ncu shows DRAM 15% busy and issue 60% "
+                             "(integer and FP64 pipes shared)"},
+        "roofline_p5": {"bound": "hbm", "kernel": "P5: key-switch inner product + EvalMult/Rescale epilogue "
                                                "(p5_mac_fp_tma for the 50-bit Q rows and p5_mac for the others "
-                                               "under the tuned schedule), the step's largest phase by bytes",
+                                               "under the tuned schedule), the step's HBM-heaviest phase",
                      "achieved": p5_alg / (phases[4] * 1e-3) / 1e9, "peak": pk["hbm_gbs"],
                      "peak_source": pk["source"] + " (burst copy)", "unit": "GB/s",
                      "frac": p5_alg / (phases[4] * 1e-3) / 1e9 / pk["hbm_gbs"],
